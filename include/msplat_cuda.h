@@ -1,0 +1,117 @@
+/*
+ * msplat_cuda.h -- C-ABI of the B200 (sm_100a) backend for msplat's splatting path.
+ *
+ * Each entry point replaces one function of the reference's backend contract,
+ * core/metal/bindings.h, cited beside it. Differences from that C++ interface:
+ *  - buffers are raw pointers with explicit sizes instead of MTensor;
+ *  - every call takes a context (msplat_cuda_ctx) holding the CUDA stream and the
+ *    per-frame cache that the reference keeps in a process global
+ *    (core/cpu/msplat_cpu.cpp:436, core/metal/msplat_metal.mm:585);
+ *  - every call returns a status code; msplat_cuda_last_error() gives the message
+ *    (the reference throws std::runtime_error / std::invalid_argument).
+ *
+ * Pointer kinds. "device" pointers must be readable by the GPU (cudaMalloc, torch
+ * CUDA tensors, or msplat_cuda_alloc's managed memory). "host" pointers (the 4x4
+ * matrices, camera position, background, Adam scalars) are read before the call
+ * returns. Work is enqueued on the context's stream and runs asynchronously unless
+ * a function says it synchronises.
+ *
+ * Layouts (bindings.h): means (N,3), log-scales (N,3), quats (N,4) as (w,x,y,z),
+ * features_dc (N,3), features_rest (N,B-1,3), opacity logits (N,1); viewmat and
+ * projmat row-major 4x4; images (H,W,3) float32; tile grid ceil(W/16) x ceil(H/16).
+ */
+#ifndef MSPLAT_CUDA_H
+#define MSPLAT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MSPLAT_CUDA_OK = 0,
+    MSPLAT_CUDA_EINVAL = 1,       /* bad argument (reference: std::invalid_argument) */
+    MSPLAT_CUDA_ECUDA = 2,        /* CUDA runtime error */
+    MSPLAT_CUDA_ECAPACITY = 3,    /* capacity exceeded (reference: core/cpu/msplat_cpu.cpp:1347) */
+    MSPLAT_CUDA_EOVERFLOW = 4,    /* more than 2^31 tile intersections (msplat_cpu.cpp:546-547) */
+    MSPLAT_CUDA_EUNSUPPORTED = 5  /* feature outside this backend (e.g. PriorStep extras) */
+};
+
+typedef struct msplat_cuda_ctx msplat_cuda_ctx;
+
+/* Message of the last failed call on this thread. */
+const char *msplat_cuda_last_error(void);
+/* Library ABI version (major * 100 + minor). */
+int msplat_cuda_version(void);
+
+/* Context: stream + frame cache. bindings.h keeps one global; see msplat_cuda_default_ctx. */
+int msplat_cuda_ctx_create(msplat_cuda_ctx **out);
+void msplat_cuda_ctx_destroy(msplat_cuda_ctx *ctx);
+msplat_cuda_ctx *msplat_cuda_default_ctx(void);
+/* Stream for all later work of this context (a cudaStream_t; NULL = legacy default). */
+int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
+/* Options: "keep_grads" (1 = keep per-Gaussian gradients for msplat_cuda_frame). */
+int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
+
+/* bindings.h:8 cleanup_msplat_metal -- release the context's cached buffers. */
+int msplat_cuda_cleanup(msplat_cuda_ctx *ctx);
+/* bindings.h:22 msplat_commit -- work is already submitted; kept for symmetry. */
+int msplat_cuda_commit(msplat_cuda_ctx *ctx);
+/* bindings.h:25 msplat_gpu_sync -- wait for the context's stream. */
+int msplat_cuda_sync(msplat_cuda_ctx *ctx);
+/* bindings.h:18-19 gpu_zeros / gpu_empty -- managed (host- and device-visible) memory. */
+int msplat_cuda_alloc(size_t bytes, int zero, void **out);
+int msplat_cuda_free(void *ptr);
+
+/* bindings.h:143 msplat_copy_buffer -- copy `bytes` from src to dst, ordered on the
+ * context's stream (any mix of device, managed and host memory). */
+int msplat_cuda_copy_buffer(msplat_cuda_ctx *ctx, void *dst, const void *src, size_t bytes);
+
+/* bindings.h:81-91 msplat_render. *out_img receives a device pointer to the (H,W,3)
+ * image in the frame cache, valid until the next call on this context (the
+ * reference likewise returns an alias of its cache, msplat_cpu.cpp:1196). */
+int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3d, const float *scales,
+                       float glob_scale, const float *quats, const float *viewmat, const float *projmat,
+                       float fx, float fy, float cx, float cy, unsigned img_height, unsigned img_width,
+                       int tiles_x, int tiles_y, float clip_thresh, unsigned degree, unsigned degrees_to_use,
+                       const float *cam_pos, const float *features_dc, const float *features_rest,
+                       const float *opacities, const float *background, const float **out_img);
+
+/* bindings.h:100-118 msplat_train_step: forward, L1 + SSIM loss, backward, Adam on the
+ * six parameter groups (means, scales, quats, features_dc, features_rest, opacities --
+ * the parameter arrays themselves, which the reference's adam_params alias,
+ * core/src/model.cpp:644-646), and the densification statistics. Adam runs only when
+ * num_adam_groups >= 5, as in the reference (msplat_cpu.cpp:1273). *radii_out (may be
+ * NULL) receives a device pointer to the int32 radii in the frame cache. When
+ * loss_out is not NULL the call synchronises and writes the loss; otherwise the loss
+ * stays on the device (msplat_cuda_loss_device). */
+int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d, float *scales, float glob_scale,
+                           float *quats, const float *viewmat, const float *projmat, float fx, float fy, float cx,
+                           float cy, unsigned img_height, unsigned img_width, int tiles_x, int tiles_y,
+                           float clip_thresh, unsigned degree, unsigned degrees_to_use, const float *cam_pos,
+                           float *features_dc, float *features_rest, float *opacities, const float *background,
+                           const float *gt, float ssim_weight, float loss_inv_n, int num_adam_groups,
+                           float *const *adam_exp_avg, float *const *adam_exp_avg_sq, const float *adam_step_sizes,
+                           const float *adam_bc2_sqrts, float adam_beta1, float adam_beta2, float adam_eps,
+                           float *vis_counts, float *xys_grad_norm, float *max_2d_size, float inv_max_dim,
+                           const int32_t **radii_out, float *loss_out);
+
+/* Device pointer of the last train step's loss (float, sum / (H*W)). */
+int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
+
+/* Per-frame intermediates of the last render / train step (test and debug hook, like
+ * the reference's _gpu_* hooks, python/bindings.cpp:655-738). Names: splats (N x 12
+ * floats: x y conic_a conic_b | conic_c sigmoid(opacity) r g | b depth - -), radii,
+ * aabb, tile_start, tile_end, isect_gid, out_img, final_Ts, final_idx, v_rendered and,
+ * with option keep_grads, v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat.
+ * *count is the element count (floats or int32). Device pointers. */
+int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count);
+/* Number of tile intersections of the last frame. */
+int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+"""ctypes binding of libmsplat_cuda.so (include/msplat_cuda.h).
+
+This is the product path: there is no CPU fallback. Loading fails loudly when the
+library has not been built or no CUDA device is present, and every non-zero status
+from the library raises ``MsplatCudaError`` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmsplat_cuda.so")
+
+_STATUS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: OverflowError, 5: NotImplementedError}
+
+
+class MsplatCudaError(RuntimeError):
+    pass
+
+
+_lib = None
+
+vp = C.c_void_p
+f32 = C.c_float
+i32 = C.c_int
+u32 = C.c_uint
+i64 = C.c_int64
+sz = C.c_size_t
+PP = C.POINTER(C.c_void_p)
+
+_SIGS = {
+    "msplat_cuda_last_error": (C.c_char_p, []),
+    "msplat_cuda_version": (i32, []),
+    "msplat_cuda_ctx_create": (i32, [PP]),
+    "msplat_cuda_ctx_destroy": (None, [vp]),
+    "msplat_cuda_default_ctx": (vp, []),
+    "msplat_cuda_ctx_set_stream": (i32, [vp, vp]),
+    "msplat_cuda_ctx_set_option": (i32, [vp, C.c_char_p, i64]),
+    "msplat_cuda_cleanup": (i32, [vp]),
+    "msplat_cuda_commit": (i32, [vp]),
+    "msplat_cuda_sync": (i32, [vp]),
+    "msplat_cuda_alloc": (i32, [sz, i32, PP]),
+    "msplat_cuda_free": (i32, [vp]),
+    "msplat_cuda_copy_buffer": (i32, [vp, vp, vp, sz]),
+    "msplat_cuda_render": (i32, [vp, i32, vp, vp, f32, vp, vp, vp, f32, f32, f32, f32, u32, u32, i32, i32, f32, u32,
+                                 u32, vp, vp, vp, vp, vp, PP]),
+    "msplat_cuda_train_step": (i32, [vp, i32, vp, vp, f32, vp, vp, vp, f32, f32, f32, f32, u32, u32, i32, i32, f32,
+                                     u32, u32, vp, vp, vp, vp, vp, vp, f32, f32, i32, vp, vp, vp, vp, f32, f32, f32,
+                                     vp, vp, vp, f32, PP, vp]),
+    "msplat_cuda_loss_device": (i32, [vp, PP]),
+    "msplat_cuda_frame": (i32, [vp, C.c_char_p, PP, C.POINTER(i64)]),
+    "msplat_cuda_num_isects": (i64, [vp]),
+}
+
+# entry points added later in the build; bound when the library exports them
+_OPTIONAL_SIGS: dict = {}
+
+
+def lib():
+    """The loaded library (built in-tree by msplat_street_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MsplatCudaError(
+                f"{LIB_PATH} is missing: build it with `python -m msplat_street_b200.build` (needs nvcc)")
+        l = C.CDLL(LIB_PATH)
+        for name, (res, args) in {**_SIGS, **_OPTIONAL_SIGS}.items():
+            fn = getattr(l, name, None)
+            if fn is None:
+                if name in _SIGS:
+                    raise MsplatCudaError(f"{LIB_PATH} does not export {name}")
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = lib().msplat_cuda_last_error().decode(errors="replace")
+        raise _STATUS.get(status, MsplatCudaError)(f"msplat_cuda error {status}: {msg}")
+
+
+def register(name: str, restype, argtypes) -> None:
+    """Declare a signature for an optional entry point (bound on first load)."""
+    _OPTIONAL_SIGS[name] = (restype, argtypes)
+    if _lib is not None:
+        fn = getattr(_lib, name, None)
+        if fn is not None:
+            fn.restype = restype
+            fn.argtypes = argtypes

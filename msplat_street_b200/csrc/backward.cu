@@ -1,0 +1,285 @@
+// Fused per-Gaussian backward + Adam + densification statistics.
+//
+// One thread per Gaussian replaces four reference passes:
+//  1. reduce_isect_grads (core/cpu/msplat_cpu.cpp:1034-1064): the Gaussian's
+//     intersection slots, found through the inverse sort permutation, are summed in
+//     sorted (= tile) order;
+//  2. project_and_sh_backward_adam (:1068-1139): projection, EWA and covariance VJPs
+//     (:197-291) for visible Gaussians, SH gradients fused into Adam for DC and rest;
+//  3. adam_dense (:1142-1147) over ALL N for means, scales, quats and opacity
+//     (invisible Gaussians see a zero gradient, their moments decay);
+//  4. the densification statistics (:1312-1324).
+// The SH-rest Adam is warp-cooperative: each lane computes its Gaussian's basis and
+// colour gradient, then the warp walks the 32 x (B-1) x 3 rest block of its 32
+// Gaussians in memory order, so those loads and stores coalesce.
+// Compiled with -fmad=false; expressions keep the reference's operation order.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace msplat {
+
+namespace {
+
+// pixel-centre VJP through the perspective divide (:197-205)
+__device__ __forceinline__ V3 center_vjp(const float *P, V3 p, uint32_t w, uint32_t h, float gx, float gy) {
+    float hx = P[0] * p.x + P[1] * p.y + P[2] * p.z + P[3];
+    float hy = P[4] * p.x + P[5] * p.y + P[6] * p.z + P[7];
+    float hw = P[12] * p.x + P[13] * p.y + P[14] * p.z + P[15];
+    float rw = 1.f / (hw + 1e-6f);
+    float nx = 0.5f * (float)w * gx, ny = 0.5f * (float)h * gy;
+    float px = nx * rw, py = ny * rw, pz = 0.f, pw = -(nx * hx + ny * hy) * rw * rw;
+    return V3{P[0] * px + P[4] * py + P[8] * pz + P[12] * pw, P[1] * px + P[5] * py + P[9] * pz + P[13] * pw,
+              P[2] * px + P[6] * py + P[10] * pz + P[14] * pw};
+}
+
+// conic VJP, -X G X with 2x2 column-major products (:207-214)
+__device__ __forceinline__ void conic_vjp(V3 cn, V3 g, float *out) {
+    const float X00 = cn.x, X01 = cn.y, X10 = cn.y, X11 = cn.z;  // X[col][row]
+    const float G00 = g.x, G01 = g.y, G10 = g.y, G11 = g.z;
+    // P = X * G
+    const float P00 = X00 * G00 + X10 * G01, P01 = X01 * G00 + X11 * G01;
+    const float P10 = X00 * G10 + X10 * G11, P11 = X01 * G10 + X11 * G11;
+    // Q = P * X
+    const float Q00 = P00 * X00 + P10 * X01, Q01 = P01 * X00 + P11 * X01;
+    const float Q10 = P00 * X10 + P10 * X11, Q11 = P01 * X10 + P11 * X11;
+    const float S00 = Q00 * -1.f, S01 = Q01 * -1.f, S10 = Q10 * -1.f, S11 = Q11 * -1.f;
+    out[0] = S00;
+    out[1] = S10 + S01;
+    out[2] = S11;
+}
+
+// EWA VJP (:216-255); adds the mean gradient into gm
+__device__ __forceinline__ void ewa_vjp(const float *cov, const float *vm, float fx, float fy, float tfx, float tfy,
+                                        V3 gc2, float *gm, float *gc3, V3 pv) {
+    float lx = 1.3f * tfx, ly = 1.3f * tfy;
+    pv.x = pv.z * fminf(lx, fmaxf(-lx, pv.x / pv.z));
+    pv.y = pv.z * fminf(ly, fmaxf(-ly, pv.y / pv.z));
+    float rz = 1.f / pv.z, rz2 = rz * rz;
+    M3 W = m3(vm[0], vm[4], vm[8], vm[1], vm[5], vm[9], vm[2], vm[6], vm[10]);
+    M3 J = m3(fx * rz, 0.f, 0.f, 0.f, fy * rz, 0.f, -fx * pv.x * rz2, -fy * pv.y * rz2, 0.f);
+    M3 V = m3(cov[0], cov[1], cov[2], cov[1], cov[3], cov[4], cov[2], cov[4], cov[5]);
+    M3 G = m3(gc2.x, 0.5f * gc2.y, 0.f, 0.5f * gc2.y, gc2.z, 0.f, 0.f, 0.f, 0.f);
+    M3 T = mul(J, W);
+    M3 gV = mul(mul(tr(T), G), T);
+    M3 gT = plus(mul(mul(G, T), tr(V)), mul(mul(tr(G), T), V));
+    gc3[0] = gV.c[0].x;
+    gc3[1] = gV.c[0].y + gV.c[1].x;
+    gc3[2] = gV.c[0].z + gV.c[2].x;
+    gc3[3] = gV.c[1].y;
+    gc3[4] = gV.c[1].z + gV.c[2].y;
+    gc3[5] = gV.c[2].z;
+    M3 gJ = mul(gT, tr(W));
+    float fxr2 = fx * rz2, fyr2 = fy * rz2, rz3 = rz2 * rz;
+    V3 gt{-fxr2 * gJ.c[2].x, -fyr2 * gJ.c[2].y,
+          -fxr2 * gJ.c[0].x + 2.f * fx * pv.x * rz3 * gJ.c[2].x - fyr2 * gJ.c[1].y + 2.f * fy * pv.y * rz3 * gJ.c[2].y};
+    gm[0] += dot3(gt, W.c[0]);
+    gm[1] += dot3(gt, W.c[1]);
+    gm[2] += dot3(gt, W.c[2]);
+}
+
+// rotation VJP, tangent to the unit sphere (:259-274). G(col, row) of the column-major v_R.
+__device__ __forceinline__ Q4 rotmat_vjp(Q4 q, const M3 &g) {
+    float s = 1.f / sqrtf(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
+    float w = q.x * s, x = q.y * s, y = q.z * s, z = q.w * s;
+#define G(col, row) el(g.c[col], row)
+    Q4 r;
+    r.x = 2.f * (x * (G(1, 2) - G(2, 1)) + y * (G(2, 0) - G(0, 2)) + z * (G(0, 1) - G(1, 0)));
+    r.y = 2.f * (-2.f * x * (G(1, 1) + G(2, 2)) + y * (G(0, 1) + G(1, 0)) + z * (G(0, 2) + G(2, 0)) +
+                 w * (G(1, 2) - G(2, 1)));
+    r.z = 2.f * (x * (G(0, 1) + G(1, 0)) - 2.f * y * (G(0, 0) + G(2, 2)) + z * (G(1, 2) + G(2, 1)) +
+                 w * (G(2, 0) - G(0, 2)));
+    r.w = 2.f * (x * (G(0, 2) + G(2, 0)) + y * (G(1, 2) + G(2, 1)) - 2.f * z * (G(0, 0) + G(1, 1)) +
+                 w * (G(0, 1) - G(1, 0)));
+#undef G
+    float radial = r.x * w + r.y * x + r.z * y + r.w * z;
+    return Q4{(r.x - radial * w) * s, (r.y - radial * x) * s, (r.z - radial * y) * s, (r.w - radial * z) * s};
+}
+
+// covariance VJP to scale and quaternion (:276-291)
+__device__ __forceinline__ void cov3d_vjp(V3 sc, float gs, Q4 q, const float *gc, float *gsv, float *gq) {
+    M3 gV = m3(gc[0], 0.5f * gc[1], 0.5f * gc[2], 0.5f * gc[1], gc[3], 0.5f * gc[4], 0.5f * gc[2], 0.5f * gc[4], gc[5]);
+    M3 R = rotmat(q);
+    M3 S = diag_scale(sc, gs);
+    M3 M = mul(R, S);
+    M3 gM = smul(2.f, mul(gV, M));
+    gsv[0] = dot3(R.c[0], gM.c[0]);
+    gsv[1] = dot3(R.c[1], gM.c[1]);
+    gsv[2] = dot3(R.c[2], gM.c[2]);
+    Q4 r = rotmat_vjp(q, mul(gM, S));
+    gq[0] = r.x;
+    gq[1] = r.y;
+    gq[2] = r.z;
+    gq[3] = r.w;
+}
+
+}  // namespace
+
+constexpr int BWD_THREADS = 256;
+constexpr int MAX_REST = 15;  // SH bases beyond DC that the backward updates (degree <= 3)
+
+__global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs a) {
+    __shared__ float s_basis[BWD_THREADS][MAX_REST + 1];
+    __shared__ float s_vrgb[BWD_THREADS][3];
+    __shared__ int s_vis[BWD_THREADS];
+    const int i = blockIdx.x * BWD_THREADS + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = i < a.n;
+    const bool vis = valid && a.radii[i] > 0;
+    const float b1 = a.beta1, b2 = a.beta2, eps = a.eps;
+
+    // 1. per-Gaussian sums of the intersection slots, in sorted order
+    float s9[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (vis) {
+        const int64_t e0 = a.offsets[i];
+        const int cnt = a.n_tiles[i];
+        for (int j = 0; j < cnt; j++) {
+            const float *sl = a.slots + (size_t)a.inv[e0 + j] * 9;
+#pragma unroll
+            for (int c = 0; c < 9; c++) s9[c] += sl[c];
+        }
+        if (a.v_xy) {
+            a.v_xy[2 * i] = s9[0];
+            a.v_xy[2 * i + 1] = s9[1];
+            a.v_conic[3 * i] = s9[2];
+            a.v_conic[3 * i + 1] = s9[3];
+            a.v_conic[3 * i + 2] = s9[4];
+            a.v_rgb[3 * i] = s9[5];
+            a.v_rgb[3 * i + 1] = s9[6];
+            a.v_rgb[3 * i + 2] = s9[7];
+            a.v_opacity[i] = s9[8];
+        }
+    } else if (valid && a.v_xy) {
+        a.v_xy[2 * i] = a.v_xy[2 * i + 1] = 0.f;
+        a.v_conic[3 * i] = a.v_conic[3 * i + 1] = a.v_conic[3 * i + 2] = 0.f;
+        a.v_rgb[3 * i] = a.v_rgb[3 * i + 1] = a.v_rgb[3 * i + 2] = 0.f;
+        a.v_opacity[i] = 0.f;
+    }
+
+    // 2. projection VJPs
+    float gm[3] = {0.f, 0.f, 0.f}, gsv[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f};
+    V3 dir{0.f, 0.f, 1.f};
+    if (vis) {
+        const float *vm = a.cam.viewmat;
+        V3 pw = ld3(a.means, i);
+        V3 vmn = center_vjp(a.cam.projmat, pw, a.cam.width, a.cam.height, s9[0], s9[1]);
+        vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, 0.f));  // no expected-depth term without priors
+        gm[0] = vmn.x;
+        gm[1] = vmn.y;
+        gm[2] = vmn.z;
+        const float4 sp0 = reinterpret_cast<const float4 *>(a.splats + i)[0];
+        const float4 sp1 = reinterpret_cast<const float4 *>(a.splats + i)[1];
+        float gc2[3];
+        conic_vjp(V3{sp0.z, sp0.w, sp1.x}, V3{s9[2], s9[3], s9[4]}, gc2);
+        V3 ls = ld3(a.scales, i);
+        V3 es{exp_ref(ls.x), exp_ref(ls.y), exp_ref(ls.z)};
+        const float4 qq = reinterpret_cast<const float4 *>(a.quats)[i];
+        Q4 q{qq.x, qq.y, qq.z, qq.w};
+        float cov[6];
+        cov3d_of(es, a.glob_scale, q, cov);
+        const float tfx = 0.5f * (float)a.cam.width / a.cam.fx, tfy = 0.5f * (float)a.cam.height / a.cam.fy;
+        V3 pv{vm[0] * pw.x + vm[1] * pw.y + vm[2] * pw.z + vm[3], vm[4] * pw.x + vm[5] * pw.y + vm[6] * pw.z + vm[7],
+              vm[8] * pw.x + vm[9] * pw.y + vm[10] * pw.z + vm[11]};
+        float gc3[6];
+        ewa_vjp(cov, vm, a.cam.fx, a.cam.fy, tfx, tfy, V3{gc2[0], gc2[1], gc2[2]}, gm, gc3, pv);
+        cov3d_vjp(es, a.glob_scale, q, gc3, gsv, gq);
+        gsv[0] *= es.x;
+        gsv[1] *= es.y;
+        gsv[2] *= es.z;
+        dir = unit(sub(pw, V3{a.cam.cam_pos[0], a.cam.cam_pos[1], a.cam.cam_pos[2]}));
+    }
+    if (valid && a.v_mean3d) {
+        for (int c = 0; c < 3; c++) {
+            a.v_mean3d[3 * i + c] = gm[c];
+            a.v_scale[3 * i + c] = gsv[c];
+        }
+        for (int c = 0; c < 4; c++) a.v_quat[4 * i + c] = gq[c];
+    }
+
+    // 3. dense Adam: means, scales, quats, opacity (all N)
+    if (valid && a.do_adam) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t k = 3 * (size_t)i + c;
+            adam_step(a.p[0][k], a.m1[0][k], a.m2[0][k], gm[c], a.ss[0], b1, b2, a.bc2[0], eps);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t k = 3 * (size_t)i + c;
+            adam_step(a.p[1][k], a.m1[1][k], a.m2[1][k], gsv[c], a.ss[1], b1, b2, a.bc2[1], eps);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const size_t k = 4 * (size_t)i + c;
+            adam_step(a.p[2][k], a.m1[2][k], a.m2[2][k], gq[c], a.ss[2], b1, b2, a.bc2[2], eps);
+        }
+        if (a.m1[5]) adam_step(a.p[5][i], a.m1[5][i], a.m2[5][i], s9[8], a.ss[5], b1, b2, a.bc2[5], eps);
+        // DC for visible Gaussians
+        if (vis) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t k = 3 * (size_t)i + c;
+                adam_step(a.p[3][k], a.m1[3][k], a.m2[3][k], SH_C0 * s9[5 + c], a.ss[3], b1, b2, a.bc2[3], eps);
+            }
+        }
+    }
+
+    // 4. densification statistics
+    if (vis && a.vis_counts) {
+        a.vis_counts[i] += 1.0f;
+        const float gx = s9[0], gy = s9[1];
+        a.xys_grad_norm[i] += sqrtf(gx * gx + gy * gy);
+        a.max_2d_size[i] = fmaxf(a.max_2d_size[i], (float)a.radii[i] * a.inv_max_dim);
+    }
+
+    // 5. SH rest Adam, warp-cooperative over the warp's 32 Gaussians
+    if (!a.do_adam || a.rest_stride <= 0) return;
+    const uint32_t dtu = a.cam.degrees_to_use;
+    const int active = dtu < 1 ? 0 : dtu < 2 ? 3 : dtu < 3 ? 8 : 15;  // bases updated
+    if (active == 0) return;
+    {
+        float x = dir.x, y = dir.y, z = dir.z;
+        float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
+        float *bs = s_basis[threadIdx.x];
+        bs[0] = -SH_C1 * y;
+        bs[1] = SH_C1 * z;
+        bs[2] = -SH_C1 * x;
+        bs[3] = SH_C2_0 * xy;
+        bs[4] = SH_C2_1 * yz;
+        bs[5] = SH_C2_2 * (2.f * zz - xx - yy);
+        bs[6] = SH_C2_3 * xz;
+        bs[7] = SH_C2_4 * (xx - yy);
+        bs[8] = SH_C3_0 * y * (3.f * xx - yy);
+        bs[9] = SH_C3_1 * xy * z;
+        bs[10] = SH_C3_2 * y * (4.f * zz - xx - yy);
+        bs[11] = SH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
+        bs[12] = SH_C3_4 * x * (4.f * zz - xx - yy);
+        bs[13] = SH_C3_5 * z * (xx - yy);
+        bs[14] = SH_C3_6 * x * (xx - 3.f * yy);
+        s_vrgb[threadIdx.x][0] = s9[5];
+        s_vrgb[threadIdx.x][1] = s9[6];
+        s_vrgb[threadIdx.x][2] = s9[7];
+        s_vis[threadIdx.x] = vis ? 1 : 0;
+    }
+    __syncwarp();
+    const int wbase_t = threadIdx.x - lane;               // first thread of this warp
+    const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;  // its Gaussian
+    const int stride = a.rest_stride;
+    const int total = 32 * stride;
+    float *rest = a.p[4] + g0 * stride, *r1 = a.m1[4] + g0 * stride, *r2 = a.m2[4] + g0 * stride;
+    for (int e = lane; e < total; e += 32) {
+        const int gl = e / stride;
+        if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
+        const int j = e - gl * stride;
+        const int base = j / 3, c = j - base * 3;
+        if (base >= active) continue;
+        const float g = s_basis[wbase_t + gl][base] * s_vrgb[wbase_t + gl][c];
+        adam_step(rest[e], r1[e], r2[e], g, a.ss[4], b1, b2, a.bc2[4], eps);
+    }
+}
+
+void launch_backward_adam(const BackwardArgs &a, cudaStream_t st) {
+    if (a.n <= 0) return;
+    backward_adam_kernel<<<(a.n + BWD_THREADS - 1) / BWD_THREADS, BWD_THREADS, 0, st>>>(a);
+}
+
+}  // namespace msplat

@@ -1,0 +1,514 @@
+// C-ABI entry points (include/msplat_cuda.h) and the per-context frame cache.
+//
+// The frame cache plays the role of the reference's FusedTensorCache / Frame
+// (core/metal/msplat_metal.mm:441-584, core/cpu/msplat_cpu.cpp:406-436): device
+// buffers that grow on demand and are reused across frames. Growth uses cudaMalloc
+// (which synchronises), so it happens only when a frame needs more room than any
+// before it; buffers grow with 25% headroom.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/msplat_cuda.h"
+#include "kernels.h"
+
+using namespace msplat;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (expr);                                                                \
+        if (_e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+struct Buf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct msplat_cuda_ctx {
+    cudaStream_t stream = nullptr;
+    bool keep_grads = false;
+    // frame description
+    int n = 0, W = 0, H = 0, tiles_x = 0, tiles_y = 0;
+    int64_t n_isect = 0;
+    int sorted = 0;  // which key/value buffer pair holds the sorted result
+    // per Gaussian
+    Buf splats, radii, aabb, n_tiles, offsets, scan_part, total;
+    Buf v_xy, v_conic, v_rgb, v_opacity, v_mean3d, v_scale, v_quat;
+    // per intersection
+    Buf keys[2], vals[2], emit_gid, isect_gid, inv, slots, radix_scratch;
+    // per tile / pixel
+    Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
+    int64_t *h_total = nullptr;  // pinned readback of the intersection count
+
+    ~msplat_cuda_ctx() { release(); }
+    void release() {
+        Buf *all[] = {&splats, &radii, &aabb, &n_tiles, &offsets, &scan_part, &total, &v_xy, &v_conic, &v_rgb,
+                      &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
+                      &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
+                      &final_idx, &v_rendered, &loss_part, &loss};
+        for (Buf *b : all) {
+            if (b->ptr) cudaFree(b->ptr);
+            b->ptr = nullptr;
+            b->bytes = 0;
+        }
+        if (h_total) cudaFreeHost(h_total);
+        h_total = nullptr;
+    }
+};
+
+namespace {
+
+template <typename T>
+int ensure(Buf &b, size_t count, T **out) {
+    const size_t need = std::max<size_t>(count, 1) * sizeof(T);
+    if (b.bytes < need) {
+        if (b.ptr) {
+            cudaError_t e = cudaFree(b.ptr);
+            if (e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "cudaFree: %s", cudaGetErrorString(e));
+        }
+        b.ptr = nullptr;
+        b.bytes = 0;
+        const size_t bytes = need + need / 4;
+        cudaError_t e = cudaMalloc(&b.ptr, bytes);
+        if (e != cudaSuccess) {
+            b.ptr = nullptr;
+            return fail(MSPLAT_CUDA_ECUDA, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+        }
+        b.bytes = bytes;
+    }
+    *out = reinterpret_cast<T *>(b.ptr);
+    return MSPLAT_CUDA_OK;
+}
+
+#define ENSURE(buf, count, type, var) \
+    type *var = nullptr;              \
+    if (int _r = ensure<type>(buf, (size_t)(count), &var)) return _r;
+
+int ceil_log2(int v) {
+    int b = 0;
+    while ((1 << b) < v) b++;
+    return b;
+}
+
+int check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigned degree, unsigned dtu,
+                 const float *viewmat, const float *projmat, const float *cam_pos, const float *bg) {
+    if (num_points < 0) return fail(MSPLAT_CUDA_EINVAL, "num_points must be >= 0 (got %d)", num_points);
+    if (W == 0 || H == 0) return fail(MSPLAT_CUDA_EINVAL, "image size must be positive (%ux%u)", W, H);
+    if (tx != (int)((W + TILE - 1) / TILE) || ty != (int)((H + TILE - 1) / TILE))
+        return fail(MSPLAT_CUDA_EINVAL, "tile bounds (%d, %d) do not match a %ux%u image with 16x16 tiles", tx, ty, W, H);
+    if ((int64_t)tx * ty >= (1ll << 31)) return fail(MSPLAT_CUDA_EINVAL, "too many tiles");
+    if (degree > 4 || dtu > degree) return fail(MSPLAT_CUDA_EINVAL, "SH degree %u / degrees_to_use %u", degree, dtu);
+    if (!viewmat || !projmat || !cam_pos || !bg) return fail(MSPLAT_CUDA_EINVAL, "null camera or background pointer");
+    return MSPLAT_CUDA_OK;
+}
+
+CamParams make_cam(const float *viewmat, const float *projmat, float fx, float fy, float cx, float cy,
+                   unsigned H, unsigned W, int tx, int ty, float clip, unsigned degree, unsigned dtu,
+                   const float *cam_pos) {
+    CamParams c;
+    std::memcpy(c.viewmat, viewmat, sizeof c.viewmat);
+    std::memcpy(c.projmat, projmat, sizeof c.projmat);
+    c.fx = fx;
+    c.fy = fy;
+    c.cx = cx;
+    c.cy = cy;
+    for (int i = 0; i < 3; i++) c.cam_pos[i] = cam_pos[i];
+    c.width = W;
+    c.height = H;
+    c.tiles_x = tx;
+    c.tiles_y = ty;
+    c.clip = clip;
+    c.degree = degree;
+    c.degrees_to_use = dtu;
+    return c;
+}
+
+// Projection, binning and forward rasterization: the shared forward of render and
+// train (core/cpu/msplat_cpu.cpp:629-657). One host synchronisation reads the
+// intersection count, which sizes the sort.
+int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales, float glob_scale,
+            const float *quats, const CamParams &cam, const float *dc, const float *rest, const float *opac,
+            const float *bg) {
+    cudaStream_t st = ctx->stream;
+    const int T = cam.tiles_x * cam.tiles_y;
+    ctx->n = n;
+    ctx->W = (int)cam.width;
+    ctx->H = (int)cam.height;
+    ctx->tiles_x = cam.tiles_x;
+    ctx->tiles_y = cam.tiles_y;
+    if (n > 0 && (!means || !scales || !quats || !dc || !opac || (cam.degree > 0 && !rest)))
+        return fail(MSPLAT_CUDA_EINVAL, "null Gaussian parameter pointer");
+    ENSURE(ctx->splats, n, Splat, splats);
+    ENSURE(ctx->radii, n, int32_t, radii);
+    ENSURE(ctx->aabb, 2 * (size_t)n, float, aabb);
+    ENSURE(ctx->n_tiles, n, int32_t, n_tiles);
+    ENSURE(ctx->offsets, n, int64_t, offsets);
+    ENSURE(ctx->scan_part, scan_blocks(std::max(n, 1)) + 1, int64_t, scan_part);
+    ENSURE(ctx->total, 1, int64_t, d_total);
+    ENSURE(ctx->tile_start, T, int32_t, tile_start);
+    ENSURE(ctx->tile_end, T, int32_t, tile_end);
+    const size_t npix = (size_t)cam.width * cam.height;
+    ENSURE(ctx->out_img, npix * 3, float, out_img);
+    ENSURE(ctx->final_T, npix, float, final_T);
+    ENSURE(ctx->final_idx, npix, int32_t, final_idx);
+    if (!ctx->h_total) CUDA_TRY(cudaMallocHost(&ctx->h_total, sizeof(int64_t)));
+
+    ProjectArgs pa;
+    pa.n = n;
+    pa.means = means;
+    pa.scales = scales;
+    pa.quats = quats;
+    pa.features_dc = dc;
+    pa.features_rest = rest;
+    pa.opacities = opac;
+    pa.rest_stride = (int)(num_sh_bases(cam.degree) - 1) * 3;
+    pa.glob_scale = glob_scale;
+    pa.cam = cam;
+    pa.splats = splats;
+    pa.radii = radii;
+    pa.aabb = aabb;
+    pa.n_tiles = n_tiles;
+    launch_project(pa, st);
+    scan_exclusive<int64_t>(n_tiles, offsets, n, d_total, scan_part, st);
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t n_isect = *ctx->h_total;
+    if (n_isect > (int64_t)INT32_MAX)
+        return fail(MSPLAT_CUDA_EOVERFLOW, "more than 2^31 tile intersections (%lld); lower the resolution",
+                    (long long)n_isect);
+    ctx->n_isect = n_isect;
+    ENSURE(ctx->keys[0], n_isect, uint64_t, k0);
+    ENSURE(ctx->keys[1], n_isect, uint64_t, k1);
+    ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
+    ENSURE(ctx->vals[1], n_isect, uint32_t, v1);
+    ENSURE(ctx->emit_gid, n_isect, int32_t, emit_gid);
+    ENSURE(ctx->isect_gid, n_isect, int32_t, isect_gid);
+    ENSURE(ctx->inv, n_isect, int32_t, inv);
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
+
+    launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y, k0, v0, emit_gid, st);
+    uint64_t *kk[2] = {k0, k1};
+    uint32_t *vv[2] = {v0, v1};
+    const int key_bits = 32 + ceil_log2(std::max(T, 1));
+    const int cur = radix_sort_pairs(kk, vv, (int)n_isect, key_bits, rscratch, st);
+    ctx->sorted = cur;
+    launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
+    launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
+
+    RasterArgs ra;
+    ra.W = (int)cam.width;
+    ra.H = (int)cam.height;
+    ra.tiles_x = cam.tiles_x;
+    ra.tiles_y = cam.tiles_y;
+    ra.tile_start = tile_start;
+    ra.tile_end = tile_end;
+    ra.isect_gid = isect_gid;
+    ra.splats = splats;
+    for (int c = 0; c < 3; c++) ra.bg[c] = bg[c];
+    ra.out_img = out_img;
+    ra.final_T = final_T;
+    ra.final_idx = final_idx;
+    launch_raster_fwd(ra, st);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+msplat_cuda_ctx *g_default = nullptr;
+std::mutex g_default_mu;
+
+}  // namespace
+
+extern "C" {
+
+const char *msplat_cuda_last_error(void) { return g_last_error.c_str(); }
+int msplat_cuda_version(void) { return 100; }
+
+int msplat_cuda_ctx_create(msplat_cuda_ctx **out) {
+    if (!out) return fail(MSPLAT_CUDA_EINVAL, "null output pointer");
+    *out = new msplat_cuda_ctx();
+    return MSPLAT_CUDA_OK;
+}
+
+void msplat_cuda_ctx_destroy(msplat_cuda_ctx *ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    delete ctx;
+}
+
+msplat_cuda_ctx *msplat_cuda_default_ctx(void) {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (!g_default) g_default = new msplat_cuda_ctx();
+    return g_default;
+}
+
+int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value) {
+    if (!ctx || !name) return fail(MSPLAT_CUDA_EINVAL, "null context or option name");
+    if (!std::strcmp(name, "keep_grads")) {
+        ctx->keep_grads = value != 0;
+        return MSPLAT_CUDA_OK;
+    }
+    return fail(MSPLAT_CUDA_EINVAL, "unknown option '%s'", name);
+}
+
+int msplat_cuda_cleanup(msplat_cuda_ctx *ctx) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    CUDA_TRY(ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize());
+    ctx->release();
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_commit(msplat_cuda_ctx *ctx) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_sync(msplat_cuda_ctx *ctx) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_alloc(size_t bytes, int zero, void **out) {
+    if (!out) return fail(MSPLAT_CUDA_EINVAL, "null output pointer");
+    if (bytes == 0) bytes = 4;
+    CUDA_TRY(cudaMallocManaged(out, bytes));
+    if (zero) std::memset(*out, 0, bytes);
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_free(void *ptr) {
+    if (ptr) CUDA_TRY(cudaFree(ptr));
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_copy_buffer(msplat_cuda_ctx *ctx, void *dst, const void *src, size_t bytes) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (!bytes) return MSPLAT_CUDA_OK;
+    if (!dst || !src) return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3d, const float *scales,
+                       float glob_scale, const float *quats, const float *viewmat, const float *projmat, float fx,
+                       float fy, float cx, float cy, unsigned img_height, unsigned img_width, int tiles_x,
+                       int tiles_y, float clip_thresh, unsigned degree, unsigned degrees_to_use,
+                       const float *cam_pos, const float *features_dc, const float *features_rest,
+                       const float *opacities, const float *background, const float **out_img) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (int r = check_camera(num_points, img_height, img_width, tiles_x, tiles_y, degree, degrees_to_use, viewmat,
+                             projmat, cam_pos, background))
+        return r;
+    CamParams cam = make_cam(viewmat, projmat, fx, fy, cx, cy, img_height, img_width, tiles_x, tiles_y, clip_thresh,
+                             degree, degrees_to_use, cam_pos);
+    if (int r = forward(ctx, num_points, means3d, scales, glob_scale, quats, cam, features_dc, features_rest,
+                        opacities, background))
+        return r;
+    if (out_img) *out_img = reinterpret_cast<const float *>(ctx->out_img.ptr);
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d, float *scales, float glob_scale,
+                           float *quats, const float *viewmat, const float *projmat, float fx, float fy, float cx,
+                           float cy, unsigned img_height, unsigned img_width, int tiles_x, int tiles_y,
+                           float clip_thresh, unsigned degree, unsigned degrees_to_use, const float *cam_pos,
+                           float *features_dc, float *features_rest, float *opacities, const float *background,
+                           const float *gt, float ssim_weight, float loss_inv_n, int num_adam_groups,
+                           float *const *adam_exp_avg, float *const *adam_exp_avg_sq, const float *adam_step_sizes,
+                           const float *adam_bc2_sqrts, float adam_beta1, float adam_beta2, float adam_eps,
+                           float *vis_counts, float *xys_grad_norm, float *max_2d_size, float inv_max_dim,
+                           const int32_t **radii_out, float *loss_out) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (int r = check_camera(num_points, img_height, img_width, tiles_x, tiles_y, degree, degrees_to_use, viewmat,
+                             projmat, cam_pos, background))
+        return r;
+    if (!gt) return fail(MSPLAT_CUDA_EINVAL, "null target image");
+    const bool adam = num_adam_groups >= 5;
+    if (adam && (!adam_exp_avg || !adam_exp_avg_sq || !adam_step_sizes || !adam_bc2_sqrts))
+        return fail(MSPLAT_CUDA_EINVAL, "null Adam state");
+    if (adam)
+        for (int g = 0; g < std::min(num_adam_groups, 6); g++)
+            if (num_points > 0 && (!adam_exp_avg[g] || !adam_exp_avg_sq[g]) && !(g == 4 && degree == 0))
+                return fail(MSPLAT_CUDA_EINVAL, "null Adam moment buffer for group %d", g);
+    CamParams cam = make_cam(viewmat, projmat, fx, fy, cx, cy, img_height, img_width, tiles_x, tiles_y, clip_thresh,
+                             degree, degrees_to_use, cam_pos);
+    if (int r = forward(ctx, num_points, means3d, scales, glob_scale, quats, cam, features_dc, features_rest,
+                        opacities, background))
+        return r;
+    cudaStream_t st = ctx->stream;
+    const size_t npix = (size_t)img_width * img_height;
+    const int n = num_points;
+    ENSURE(ctx->v_rendered, npix * 3, float, v_rendered);
+    ENSURE(ctx->loss_part, ssim_blocks((int)img_width, (int)img_height), double, loss_part);
+    ENSURE(ctx->loss, 1, float, d_loss);
+    ENSURE(ctx->slots, (size_t)ctx->n_isect * 9, float, slots);
+
+    SsimArgs sa;
+    sa.W = (int)img_width;
+    sa.H = (int)img_height;
+    sa.img = reinterpret_cast<const float *>(ctx->out_img.ptr);
+    sa.gt = gt;
+    sa.ssim_weight = ssim_weight;
+    sa.inv_n = loss_inv_n;
+    sa.v_out = v_rendered;
+    sa.partials = loss_part;
+    sa.loss = d_loss;
+    launch_ssim_loss(sa, st);
+
+    RasterBwdArgs rb;
+    rb.W = (int)img_width;
+    rb.H = (int)img_height;
+    rb.tiles_x = tiles_x;
+    rb.tiles_y = tiles_y;
+    rb.tile_start = reinterpret_cast<const int32_t *>(ctx->tile_start.ptr);
+    rb.tile_end = reinterpret_cast<const int32_t *>(ctx->tile_end.ptr);
+    rb.isect_gid = reinterpret_cast<const int32_t *>(ctx->isect_gid.ptr);
+    rb.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
+    for (int c = 0; c < 3; c++) rb.bg[c] = background[c];
+    rb.final_T = reinterpret_cast<const float *>(ctx->final_T.ptr);
+    rb.final_idx = reinterpret_cast<const int32_t *>(ctx->final_idx.ptr);
+    rb.v_out = v_rendered;
+    rb.slots = slots;
+    launch_raster_bwd(rb, st);
+
+    BackwardArgs ba;
+    std::memset(&ba, 0, sizeof ba);
+    ba.n = n;
+    ba.means = means3d;
+    ba.scales = scales;
+    ba.quats = quats;
+    ba.glob_scale = glob_scale;
+    ba.cam = cam;
+    ba.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
+    ba.radii = reinterpret_cast<const int32_t *>(ctx->radii.ptr);
+    ba.n_tiles = reinterpret_cast<const int32_t *>(ctx->n_tiles.ptr);
+    ba.inv = reinterpret_cast<const int32_t *>(ctx->inv.ptr);
+    ba.offsets = reinterpret_cast<const int64_t *>(ctx->offsets.ptr);
+    ba.slots = slots;
+    if (ctx->keep_grads) {
+        ENSURE(ctx->v_xy, 2 * (size_t)n, float, vxy);
+        ENSURE(ctx->v_conic, 3 * (size_t)n, float, vcon);
+        ENSURE(ctx->v_rgb, 3 * (size_t)n, float, vrgb);
+        ENSURE(ctx->v_opacity, n, float, vop);
+        ENSURE(ctx->v_mean3d, 3 * (size_t)n, float, vm3);
+        ENSURE(ctx->v_scale, 3 * (size_t)n, float, vsc);
+        ENSURE(ctx->v_quat, 4 * (size_t)n, float, vq);
+        ba.v_xy = vxy;
+        ba.v_conic = vcon;
+        ba.v_rgb = vrgb;
+        ba.v_opacity = vop;
+        ba.v_mean3d = vm3;
+        ba.v_scale = vsc;
+        ba.v_quat = vq;
+    }
+    ba.do_adam = adam ? 1 : 0;
+    float *params[6] = {means3d, scales, quats, features_dc, features_rest, opacities};
+    for (int g = 0; g < 6; g++) {
+        ba.p[g] = params[g];
+        if (adam && g < num_adam_groups) {
+            ba.m1[g] = adam_exp_avg[g];
+            ba.m2[g] = adam_exp_avg_sq[g];
+            ba.ss[g] = adam_step_sizes[g];
+            ba.bc2[g] = adam_bc2_sqrts[g];
+        }
+    }
+    if (adam && num_adam_groups < 6) {
+        // the reference updates only groups < num_adam_groups: no opacity Adam with 5
+        ba.m1[5] = ba.m2[5] = nullptr;
+    }
+    ba.beta1 = adam_beta1;
+    ba.beta2 = adam_beta2;
+    ba.eps = adam_eps;
+    ba.rest_stride = (int)(num_sh_bases(degree) - 1) * 3;
+    ba.vis_counts = vis_counts;
+    ba.xys_grad_norm = xys_grad_norm;
+    ba.max_2d_size = max_2d_size;
+    ba.inv_max_dim = inv_max_dim;
+    if (vis_counts && (!xys_grad_norm || !max_2d_size))
+        return fail(MSPLAT_CUDA_EINVAL, "densification statistics need all three buffers");
+    launch_backward_adam(ba, st);
+    CUDA_TRY(cudaGetLastError());
+    if (radii_out) *radii_out = reinterpret_cast<const int32_t *>(ctx->radii.ptr);
+    if (loss_out) {
+        CUDA_TRY(cudaMemcpyAsync(loss_out, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
+    if (!ctx || !loss) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    if (!ctx->loss.ptr) return fail(MSPLAT_CUDA_EINVAL, "no train step has run on this context");
+    *loss = reinterpret_cast<const float *>(ctx->loss.ptr);
+    return MSPLAT_CUDA_OK;
+}
+
+int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
+
+int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count) {
+    if (!ctx || !name || !dev_ptr || !count) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    const int64_t n = ctx->n, T = (int64_t)ctx->tiles_x * ctx->tiles_y, npix = (int64_t)ctx->W * ctx->H;
+    struct Entry {
+        const char *name;
+        Buf *buf;
+        int64_t count;
+    } table[] = {
+        {"splats", &ctx->splats, n * 12},
+        {"radii", &ctx->radii, n},
+        {"aabb", &ctx->aabb, n * 2},
+        {"tile_start", &ctx->tile_start, T},
+        {"tile_end", &ctx->tile_end, T},
+        {"isect_gid", &ctx->isect_gid, ctx->n_isect},
+        {"out_img", &ctx->out_img, npix * 3},
+        {"final_Ts", &ctx->final_T, npix},
+        {"final_idx", &ctx->final_idx, npix},
+        {"v_rendered", &ctx->v_rendered, npix * 3},
+        {"v_xy", &ctx->v_xy, n * 2},
+        {"v_conic", &ctx->v_conic, n * 3},
+        {"v_rgb", &ctx->v_rgb, n * 3},
+        {"v_opacity", &ctx->v_opacity, n},
+        {"v_mean3d", &ctx->v_mean3d, n * 3},
+        {"v_scale", &ctx->v_scale, n * 3},
+        {"v_quat", &ctx->v_quat, n * 4},
+    };
+    for (const Entry &e : table)
+        if (!std::strcmp(e.name, name)) {
+            if (!e.buf->ptr) return fail(MSPLAT_CUDA_EINVAL, "frame buffer '%s' has not been produced", name);
+            *dev_ptr = e.buf->ptr;
+            *count = e.count;
+            return MSPLAT_CUDA_OK;
+        }
+    return fail(MSPLAT_CUDA_EINVAL, "unknown frame buffer '%s'", name);
+}
+
+}  // extern "C"

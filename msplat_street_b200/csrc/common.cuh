@@ -1,0 +1,162 @@
+// Shared device helpers for the msplat B200 kernels.
+//
+// Parity contract. The splatting kernels reproduce the reference backend's float32
+// results (core/cpu/msplat_cpu.cpp, itself a port of core/metal/msplat_metal.metal)
+// bit for bit wherever an integer decision depends on them: tile rectangles, radii,
+// depth keys and the alpha / transmittance cut-offs. To that end
+//  * the translation units that compute them are compiled with -fmad=false, so every
+//    a*b+c stays two rounded operations, in the reference's order;
+//  * exponentials use exp_ref(): exp evaluated in double and rounded once to float,
+//    which agrees with a correctly rounded expf except in rare near-halfway cases;
+//  * division and square root are IEEE (nvcc's default -prec-div / -prec-sqrt).
+// Matrices are column-major (c[col] is a column) because the reference's helper
+// types follow MSL conventions (core/cpu/cpu_math.hpp:1-4).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace msplat {
+
+constexpr int TILE = 16;            // core/cpu/msplat_cpu.cpp:27
+constexpr int TILE_PIX = TILE * TILE;
+
+// Real SH basis constants (core/cpu/msplat_cpu.cpp:29-38).
+constexpr float SH_C0 = 0.28209479177387814f;
+constexpr float SH_C1 = 0.4886025119029199f;
+constexpr float SH_C2_0 = 1.0925484305920792f, SH_C2_1 = -1.0925484305920792f, SH_C2_2 = 0.31539156525252005f,
+                SH_C2_3 = -1.0925484305920792f, SH_C2_4 = 0.5462742152960396f;
+constexpr float SH_C3_0 = -0.5900435899266435f, SH_C3_1 = 2.890611442640554f, SH_C3_2 = -0.4570457994644658f,
+                SH_C3_3 = 0.3731763325901154f, SH_C3_4 = -0.4570457994644658f, SH_C3_5 = 1.445305721320277f,
+                SH_C3_6 = -0.5900435899266435f;
+constexpr float SH_C4_0 = 2.5033429417967046f, SH_C4_1 = -1.7701307697799304f, SH_C4_2 = 0.9461746957575601f,
+                SH_C4_3 = -0.6690465435572892f, SH_C4_4 = 0.10578554691520431f, SH_C4_5 = -0.6690465435572892f,
+                SH_C4_6 = 0.47308734787878004f, SH_C4_7 = -1.7701307697799304f, SH_C4_8 = 0.6258357354491761f;
+
+__host__ __device__ inline uint32_t num_sh_bases(uint32_t degree) {
+    return degree == 0 ? 1 : degree == 1 ? 4 : degree == 2 ? 9 : degree == 3 ? 16 : 25;
+}
+
+// exp in double, rounded once to float
+__device__ __forceinline__ float exp_ref(float x) { return (float)exp((double)x); }
+
+struct V2 { float x, y; };
+struct V3 { float x, y, z; };
+struct Q4 { float x, y, z, w; };  // quaternion stored (w, x, y, z) lands in x, y, z, w
+
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 add(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 sub(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 scl(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 scl(float s, V3 a) { return V3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 ld3(const float *p, int64_t i) { return V3{p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+__device__ __forceinline__ void st3(float *p, int64_t i, V3 v) {
+    p[3 * i] = v.x;
+    p[3 * i + 1] = v.y;
+    p[3 * i + 2] = v.z;
+}
+__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.f), 1.f); }
+__device__ __forceinline__ V3 unit(V3 a) { return scl(a, 1.f / sqrtf(dot3(a, a))); }
+
+struct M3 {
+    V3 c[3];
+};
+__device__ __forceinline__ M3 m3(float a0, float a1, float a2, float b0, float b1, float b2, float d0, float d1,
+                                 float d2) {
+    M3 m;
+    m.c[0] = V3{a0, a1, a2};
+    m.c[1] = V3{b0, b1, b2};
+    m.c[2] = V3{d0, d1, d2};
+    return m;
+}
+__device__ __forceinline__ float el(const V3 &v, int r) { return r == 0 ? v.x : (r == 1 ? v.y : v.z); }
+// Column-major product R[j][i] = sum_k A[k][i] * B[j][k], k in order 0,1,2
+__device__ __forceinline__ M3 mul(const M3 &A, const M3 &B) {
+    M3 R;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        float r0 = A.c[0].x * el(B.c[j], 0) + A.c[1].x * el(B.c[j], 1) + A.c[2].x * el(B.c[j], 2);
+        float r1 = A.c[0].y * el(B.c[j], 0) + A.c[1].y * el(B.c[j], 1) + A.c[2].y * el(B.c[j], 2);
+        float r2 = A.c[0].z * el(B.c[j], 0) + A.c[1].z * el(B.c[j], 1) + A.c[2].z * el(B.c[j], 2);
+        R.c[j] = V3{r0, r1, r2};
+    }
+    return R;
+}
+__device__ __forceinline__ M3 tr(const M3 &A) {
+    return m3(A.c[0].x, A.c[1].x, A.c[2].x, A.c[0].y, A.c[1].y, A.c[2].y, A.c[0].z, A.c[1].z, A.c[2].z);
+}
+__device__ __forceinline__ M3 plus(const M3 &A, const M3 &B) {
+    M3 R;
+    R.c[0] = add(A.c[0], B.c[0]);
+    R.c[1] = add(A.c[1], B.c[1]);
+    R.c[2] = add(A.c[2], B.c[2]);
+    return R;
+}
+__device__ __forceinline__ M3 smul(float s, const M3 &A) {
+    M3 R;
+    R.c[0] = scl(A.c[0], s);
+    R.c[1] = scl(A.c[1], s);
+    R.c[2] = scl(A.c[2], s);
+    return R;
+}
+
+// Rotation from the (w,x,y,z) quaternion, normalised (core/cpu/msplat_cpu.cpp:77-84)
+__device__ __forceinline__ M3 rotmat(Q4 q) {
+    float s = 1.f / sqrtf(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
+    float w = q.x * s, x = q.y * s, y = q.z * s, z = q.w * s;
+    return m3(1.f - 2.f * (y * y + z * z), 2.f * (x * y + w * z), 2.f * (x * z - w * y), 2.f * (x * y - w * z),
+              1.f - 2.f * (x * x + z * z), 2.f * (y * z + w * x), 2.f * (x * z + w * y), 2.f * (y * z - w * x),
+              1.f - 2.f * (x * x + y * y));
+}
+
+__device__ __forceinline__ M3 diag_scale(V3 s, float g) {
+    M3 S = m3(1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f);
+    S.c[0].x = g * s.x;
+    S.c[1].y = g * s.y;
+    S.c[2].z = g * s.z;
+    return S;
+}
+
+// 3D covariance R S S^T R^T, upper triangle (core/cpu/msplat_cpu.cpp:94-100)
+__device__ __forceinline__ void cov3d_of(V3 s, float g, Q4 q, float *cov) {
+    M3 M = mul(rotmat(q), diag_scale(s, g));
+    M3 t = mul(M, tr(M));
+    cov[0] = t.c[0].x;
+    cov[1] = t.c[0].y;
+    cov[2] = t.c[0].z;
+    cov[3] = t.c[1].y;
+    cov[4] = t.c[1].z;
+    cov[5] = t.c[2].z;
+}
+
+// One splat record per Gaussian, read by the rasterizer: centre, conic, sigmoid
+// opacity and raw SH colour, 48 bytes so it loads as three float4.
+struct __align__(16) Splat {
+    float x, y, cx, cy;   // pixel centre, conic (a, b)
+    float cz, op, r, g;   // conic c, sigmoid(opacity), raw colour r g
+    float b, depth, pad0, pad1;
+};
+
+// Counter-based RNG: PCG hash + Box-Muller (core/cpu/msplat_cpu.cpp:304-323)
+__host__ __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+__host__ __device__ __forceinline__ float rand_unif(uint32_t seed, uint32_t ctr) {
+    uint32_t h = pcg_hash(seed ^ pcg_hash(ctr));
+    return ((float)(h >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+// Adam with precomputed step_size = lr / bc1 (core/cpu/msplat_cpu.cpp:293-300)
+__device__ __forceinline__ void adam_step(float &p, float &m1, float &m2, float g, float ss, float b1, float b2,
+                                          float bc2, float eps) {
+    float m = b1 * m1 + (1.0f - b1) * g;
+    float v = b2 * m2 + (1.0f - b2) * g * g;
+    p -= ss * m / (sqrtf(v) / bc2 + eps);
+    m1 = m;
+    m2 = v;
+}
+
+}  // namespace msplat

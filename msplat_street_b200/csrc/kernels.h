@@ -1,0 +1,104 @@
+// Internal launch interface between the C-ABI layer (capi.cu) and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace msplat {
+
+// One view: the scalars msplat_render / msplat_train_step take about the camera.
+struct CamParams {
+    float viewmat[16];  // row-major world-to-camera
+    float projmat[16];  // row-major clip-from-world
+    float fx, fy, cx, cy;
+    float cam_pos[3];
+    uint32_t width, height;
+    int tiles_x, tiles_y;
+    float clip;
+    uint32_t degree, degrees_to_use;
+};
+
+struct ProjectArgs {
+    int n;
+    const float *means, *scales, *quats, *features_dc, *features_rest, *opacities;
+    int rest_stride;  // floats per Gaussian in features_rest
+    float glob_scale;
+    CamParams cam;
+    Splat *splats;
+    int32_t *radii;
+    float *aabb;
+    int32_t *n_tiles;
+};
+void launch_project(const ProjectArgs &a, cudaStream_t st);
+
+int scan_blocks(int n);
+template <typename TO>
+void scan_exclusive(const int32_t *in, TO *out, int n, TO *d_total, TO *partials, cudaStream_t st);
+
+void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
+                      int tiles_x, int tiles_y, uint64_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
+size_t radix_scratch_bytes(int n);
+int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st);
+void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st);
+void launch_isect_map(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid, int32_t *inv,
+                      cudaStream_t st);
+
+struct RasterArgs {
+    int W, H, tiles_x, tiles_y;
+    const int32_t *tile_start, *tile_end, *isect_gid;
+    const Splat *splats;
+    float bg[3];
+    float *out_img, *final_T;
+    int32_t *final_idx;
+};
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st);
+
+struct RasterBwdArgs {
+    int W, H, tiles_x, tiles_y;
+    const int32_t *tile_start, *tile_end, *isect_gid;
+    const Splat *splats;
+    float bg[3];
+    const float *final_T;
+    const int32_t *final_idx;
+    const float *v_out;
+    float *slots;  // 9 floats per sorted intersection
+};
+void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st);
+
+struct SsimArgs {
+    int W, H;
+    const float *img, *gt;
+    float ssim_weight, inv_n;
+    float *v_out;
+    double *partials;  // one per 32x32 block
+    float *loss;       // device scalar: sum / (W * H)
+};
+int ssim_blocks(int W, int H);
+void launch_ssim_loss(const SsimArgs &a, cudaStream_t st);
+
+struct BackwardArgs {
+    int n;
+    const float *means, *scales, *quats;
+    float glob_scale;
+    CamParams cam;
+    const Splat *splats;
+    const int32_t *radii, *n_tiles, *inv;
+    const int64_t *offsets;
+    const float *slots;
+    // optional per-Gaussian gradient outputs (null to skip)
+    float *v_xy, *v_conic, *v_rgb, *v_opacity, *v_mean3d, *v_scale, *v_quat;
+    // Adam: groups means, scales, quats, dc, rest, opacity
+    int do_adam;
+    float *p[6], *m1[6], *m2[6];
+    float ss[6], bc2[6];
+    float beta1, beta2, eps;
+    int rest_stride;
+    // densification statistics (null to skip)
+    float *vis_counts, *xys_grad_norm, *max_2d_size;
+    float inv_max_dim;
+};
+void launch_backward_adam(const BackwardArgs &a, cudaStream_t st);
+
+}  // namespace msplat

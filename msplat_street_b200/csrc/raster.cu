@@ -1,0 +1,210 @@
+// 16x16-tile front-to-back alpha compositing, forward and backward.
+//
+// One 256-thread CTA per tile, one pixel per thread. The tile's depth-sorted list is
+// walked in batches whose splat records are staged in shared memory; every thread
+// reads each record as a broadcast.
+//
+// Forward: rasterize_forward (core/cpu/msplat_cpu.cpp:574-626): sigma < 0 or >= 5.55
+// skips, alpha = min(0.999, o * exp(-sigma)) with alpha < 1/255 skipped, and the pixel
+// stops before the Gaussian that would take T to <= 1e-4 (last = k - 1). The block
+// leaves its loop when __syncthreads_count says all 256 pixels are done.
+//
+// Backward: rasterize_backward (:959-1031): back to front from final_idx, T recovered
+// by multiplying with 1/(1 - alpha), colour gradients gated on raw + 0.5 >= 0 and the
+// sigma gradients only for alpha < 0.999. Each (tile, Gaussian) pair -- one sorted
+// intersection -- gets one 9-float slot: xy(2) conic(3) rgb(3) opacity-logit(1),
+// reduced over the tile's pixels with warp shuffles and a fixed-order sum over warps,
+// so results do not depend on scheduling (the reference is deterministic too,
+// :952-956). The per-Gaussian sums happen in the fused backward/Adam kernel.
+//
+// Compiled with -fmad=false: the alpha and transmittance cut-offs must fall exactly
+// where the reference's do.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace msplat {
+
+constexpr int FWD_BATCH = TILE_PIX;
+constexpr int BWD_BATCH = 64;
+constexpr int BWD_WARPS = TILE_PIX / 32;
+
+__global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
+    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
+    const int tile = blockIdx.x;
+    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const int px = tx * TILE + (threadIdx.x % TILE), py = ty * TILE + (threadIdx.x / TILE);
+    const bool inside = px < a.W && py < a.H;
+    const int start = a.tile_start[tile], end = a.tile_end[tile];
+    const float fpx = (float)px, fpy = (float)py;
+    float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f;
+    int last = start - 1;
+    bool done = !inside;
+    for (int b0 = start; b0 < end; b0 += FWD_BATCH) {
+        if (__syncthreads_count(done) == TILE_PIX) break;
+        const int k = b0 + threadIdx.x;
+        if (k < end) {
+            const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
+            s0[threadIdx.x] = rec[0];
+            s1[threadIdx.x] = rec[1];
+            s2[threadIdx.x] = rec[2];
+        }
+        __syncthreads();
+        const int cnt = min(FWD_BATCH, end - b0);
+        for (int j = 0; j < cnt && !done; j++) {
+            const float4 A = s0[j], B = s1[j];
+            const float dx = A.x - fpx, dy = A.y - fpy;
+            const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
+            if (sigma < 0.f || sigma >= 5.55f) continue;
+            const float alpha = fminf(0.999f, B.y * exp_ref(-sigma));
+            if (alpha < 1.f / 255.f) continue;
+            const float nT = T * (1.f - alpha);
+            if (nT <= 1e-4f) {
+                last = b0 + j - 1;
+                done = true;
+                break;
+            }
+            const float vis = alpha * T;
+            cr = fmaxf(B.z + 0.5f, 0.f) * vis + cr;
+            cg = fmaxf(B.w + 0.5f, 0.f) * vis + cg;
+            cb = fmaxf(s2[j].x + 0.5f, 0.f) * vis + cb;
+            T = nT;
+            last = b0 + j;
+        }
+    }
+    if (!inside) return;
+    const int pid = py * a.W + px;
+    a.final_T[pid] = T;
+    a.final_idx[pid] = last;
+    float *o = a.out_img + 3 * (size_t)pid;
+    o[0] = clamp01(a.bg[0] * T + cr);
+    o[1] = clamp01(a.bg[1] * T + cg);
+    o[2] = clamp01(a.bg[2] * T + cb);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(TILE_PIX) raster_bwd_kernel(RasterBwdArgs a) {
+    __shared__ float4 s0[BWD_BATCH], s1[BWD_BATCH], s2[BWD_BATCH];
+    __shared__ float red[BWD_WARPS][BWD_BATCH][9];
+    __shared__ int kmax;
+    const int tile = blockIdx.x;
+    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const int px = tx * TILE + (threadIdx.x % TILE), py = ty * TILE + (threadIdx.x / TILE);
+    const bool inside = px < a.W && py < a.H;
+    const int start = a.tile_start[tile], end = a.tile_end[tile];
+    if (end <= start) return;  // block-uniform
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pid = py * a.W + px;
+    float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f;
+    int kf = start - 1;
+    if (inside) {
+        Tf = a.final_T[pid];
+        T = Tf;
+        kf = a.final_idx[pid];
+        const float *v = a.v_out + 3 * (size_t)pid;
+        vr = v[0];
+        vg = v[1];
+        vb = v[2];
+    }
+    if (threadIdx.x == 0) kmax = start - 1;
+    __syncthreads();
+    if (inside) atomicMax(&kmax, min(kf, end - 1));
+    __syncthreads();
+    const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
+    // T_final * bg, then the -ra * (T_final * bg) term of the reference's v_alpha
+    const float tbr = Tf * a.bg[0], tbg = Tf * a.bg[1], tbb = Tf * a.bg[2];
+    float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
+    const float fpx = (float)px, fpy = (float)py;
+    for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
+        const int b_start = max(start, b_end - BWD_BATCH);
+        const int cnt = b_end - b_start;
+        if (threadIdx.x < cnt) {
+            const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[b_start + threadIdx.x]);
+            s0[threadIdx.x] = rec[0];
+            s1[threadIdx.x] = rec[1];
+            s2[threadIdx.x] = rec[2];
+        }
+        __syncthreads();
+        for (int j = cnt - 1; j >= 0; j--) {
+            const int k = b_start + j;
+            float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            bool hit = false;
+            if (inside && k <= kf) {
+                const float4 A = s0[j], B = s1[j];
+                const float dx = A.x - fpx, dy = A.y - fpy;
+                const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
+                if (sigma >= 0.f && sigma < 5.55f) {
+                    const float op = B.y;
+                    const float alpha = fminf(0.999f, op * exp_ref(-sigma));
+                    if (alpha >= 1.f / 255.f) {
+                        hit = true;
+                        const float ra = 1.f / (1.f - alpha);
+                        T *= ra;
+                        const float fac = alpha * T;
+                        const float rawr = B.z, rawg = B.w, rawb = s2[j].x;
+                        const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),
+                                    cb = fmaxf(rawb + 0.5f, 0.f);
+                        const float nra = -ra;
+                        const float ir = -br * ra + nra * tbr, ig = -bgc * ra + nra * tbg, ib = -bb * ra + nra * tbb;
+                        const float orr = cr * T + ir, og = cg * T + ig, ob = cb * T + ib;
+                        const float va = orr * vr + og * vg + ob * vb;
+                        br = cr * fac + br;
+                        bgc = cg * fac + bgc;
+                        bb = cb * fac + bb;
+                        if (rawr + 0.5f >= 0.f) g[5] = fac * vr;
+                        if (rawg + 0.5f >= 0.f) g[6] = fac * vg;
+                        if (rawb + 0.5f >= 0.f) g[7] = fac * vb;
+                        if (alpha < 0.999f) {
+                            const float vs = -alpha * va;
+                            g[2] = 0.5f * vs * dx * dx;
+                            g[3] = 0.5f * vs * dx * dy;
+                            g[4] = 0.5f * vs * dy * dy;
+                            g[0] = vs * (A.z * dx + A.w * dy);
+                            g[1] = vs * (A.w * dx + B.x * dy);
+                            g[8] = -vs * (1.f - op);
+                        }
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, hit)) {
+#pragma unroll
+                for (int c = 0; c < 9; c++) g[c] = warp_sum(g[c]);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int c = 0; c < 9; c++) red[warp][j][c] = g[c];
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < cnt * 9; idx += blockDim.x) {
+            const int j = idx / 9, c = idx - j * 9;
+            float s = 0.f;
+#pragma unroll
+            for (int w = 0; w < BWD_WARPS; w++) s += red[w][j][c];
+            a.slots[(size_t)(b_start + j) * 9 + c] = s;
+        }
+        __syncthreads();
+    }
+    // intersections above every pixel's last contributor get zero slots
+    for (int k = kend + threadIdx.x; k < end; k += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 9; c++) a.slots[(size_t)k * 9 + c] = 0.f;
+}
+
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    raster_fwd_kernel<<<T, TILE_PIX, 0, st>>>(a);
+}
+
+void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    raster_bwd_kernel<<<T, TILE_PIX, 0, st>>>(a);
+}
+
+}  // namespace msplat

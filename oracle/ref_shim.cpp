@@ -34,7 +34,7 @@ struct Scene {
         vm = host_tensor({4, 4}, DType::Float32, v);
         pm = host_tensor({4, 4}, DType::Float32, p);
         dc = host_tensor({n, 3}, DType::Float32, d);
-        rest = host_tensor({n, std::max<int64_t>(nb - 1, 1), 3}, DType::Float32, r);
+        rest = host_tensor({n, nb - 1, 3}, DType::Float32, r);
         opac = host_tensor({n, 1}, DType::Float32, o);
         bg = host_tensor({3}, DType::Float32, b);
     }

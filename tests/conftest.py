@@ -1,0 +1,16 @@
+"""Test configuration: the ``gpu`` marker and import paths.
+
+``pytest -m "not gpu"`` runs on a machine without a GPU (oracle pinning, host logic,
+library loading); ``pytest -m gpu`` runs the parity tests on a CUDA device.
+"""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200 / sm_100a)")
