@@ -1,0 +1,382 @@
+"""Benchmark: street-scale plain training, iterations per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (msplat_street_b200.workloads.street_plain): a 500,000-Gaussian ground-truth
+street scene (20 x 4 x 20 m), 16 target views at 1024 x 512, training from 100,000
+kNN-initialised Gaussians with the densification schedule of the 2,000-iteration
+street config. A step is one training iteration of that schedule (one view): W
+untimed warm-up iterations, then K timed ones that continue the schedule, with any
+densification that falls in the window inside the timed step.
+
+value: iterations/s with the targets resident in HBM, device-timed with CUDA events
+per step (L2 flushed by a 256 MB write between steps, outside the events); e2e: the
+same schedule replayed through the public API with each step's target copied from
+pinned host memory and the loss read back, wall-clock timed. Training does not
+shard without a gradient exchange, so N GPUs run N independent replicas ("replicas
+only", weak scaling); value is the sum over ranks of K / max-over-ranks time.
+
+--impl reference times the reference's own CPU backend (core/cpu, built into
+oracle/_ref) on a bounded sample of the same schedule on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "train iters/s (street plain, 1024x512)"
+UNIT = "iters/s"
+WORKLOAD = ("street-plain: 500k-Gaussian GT scene (20x4x20 m), 16 views 1024x512, train from 100k kNN-init "
+            "Gaussians, densify every 100 from step 500, 2000-iteration schedule")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ------------------------------------------------------------------------------------
+# CPU baseline: the reference's own core/cpu backend on the host cores
+
+def cpu_reference_run(seconds: float, max_steps: int, warmup: int = 1):
+    """Trains the same street schedule with the reference's CPU backend until ``seconds``
+    of timed work or ``max_steps`` iterations; returns (iters/s, steps, threads, n)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from msplat_street_b200 import scenes, workloads
+    from oracle_lib import Oracle, available, new_adam_state
+    kind = "reference_fast" if available("reference_fast") else "restatement"
+    ref = Oracle(kind)
+    gt, poses, setups = workloads.street_views(workloads.STREET_GT_N)
+    pts, rgb = scenes.jittered_init_points(gt, workloads.STREET_INIT_N, seed=3)
+    s, q, d, o = ref.init_gaussians(pts, rgb, 42, float(np.log(0.1 / 0.9)))
+    g = scenes.Gaussians(pts.copy(), s, q, d, np.zeros((pts.shape[0], 15, 3), np.float32), o)
+    lrs = [0.00016, 0.005, 0.001, 0.0025, 0.000125, 0.05]
+    m1 = [np.zeros_like(a) for a in g.arrays()]
+    m2 = [np.zeros_like(a) for a in g.arrays()]
+    st = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+    order = list(np.random.default_rng(42).permutation(len(setups)))
+    targets = {}
+    done, elapsed, step = 0, 0.0, 0
+    while done < max_steps and (elapsed < seconds or done == 0):
+        ci = int(order[step % len(order)])
+        if ci not in targets:
+            targets[ci] = ref.render(gt, setups[ci], workloads.BACKGROUND)
+        step += 1
+        ad = new_adam_state(g, lrs, step)
+        ad["m1"], ad["m2"] = m1, m2
+        t0 = time.perf_counter()
+        ref.train_step(g, setups[ci], workloads.BACKGROUND, targets[ci], ad, st,
+                       degrees_to_use=min(step // 1000, 3))
+        dt = time.perf_counter() - t0
+        if step > warmup:
+            elapsed += dt
+            done += 1
+    threads = int(os.environ.get("MSPLAT_THREADS", os.cpu_count() or 1)) if kind != "restatement" else \
+        (os.cpu_count() or 1)
+    return done / elapsed, done, threads, g.n, kind
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    try:
+        rate, done, threads, n, kind = cpu_reference_run(seconds=min(60.0, 6.0 * max(args.steps, 1)),
+                                                         max_steps=max(args.steps, 1), warmup=min(args.warmup, 1))
+    except Exception as e:  # the reference build is missing
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU backend not runnable: {e}"}))
+        return
+    sample = (f"{done} training iterations of the street schedule from step 2 ({n} Gaussians, 1024x512) with the "
+              f"reference core/cpu backend, {threads} host threads")
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1000.0 / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads,
+                             "kind": "reference" if kind.startswith("reference") else "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+    from msplat_street_b200 import workloads
+    from msplat_street_b200.backend import Context
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    total_steps = args.warmup + args.steps
+    iters = max(2000, total_steps)
+
+    # ---- device-timed pass: targets resident in HBM ----
+    ctx = Context()
+    trainer, targets = workloads.street_plain(ctx, iterations=iters)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):
+        trainer.step()
+    torch.cuda.synchronize()
+    ctx.enable_stage_timing(True)
+    ctx.drain_stage_times()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    n_isects = []
+    barrier(world, dev)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record()
+            trainer.step()
+            evs[i][1].record()
+            n_isects.append(ctx.num_isects())
+        torch.cuda.synchronize()
+    barrier(world, dev)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(step_ms), world, dev)
+    stages = ctx.drain_stage_times()
+    ctx.enable_stage_timing(False)
+    final_n = trainer.splat_count
+    value = world * args.steps / (total_ms / 1e3)
+
+    if args.quick:  # device pass only (profiling runs)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "quick": True,
+                              "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
+                              "isects_mean": float(np.mean(n_isects))}))
+        return
+
+    # ---- end-to-end pass through the public API: host targets, loss read back ----
+    ctx2 = Context()
+    trainer2, targets2 = workloads.street_plain(ctx2, iterations=iters)
+    host_targets = [t.cpu().pin_memory() for t in targets2]
+    del targets2
+    trainer2._targets = [None] * len(host_targets)
+    for _ in range(args.warmup):
+        trainer2.step(target=_upload(trainer2, host_targets, dev), sync_loss=True)
+    barrier(world, dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        trainer2.step(target=_upload(trainer2, host_targets, dev), sync_loss=True)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+    barrier(world, dev)
+    e2e = world * args.steps / e2e_s
+    h2d = int(host_targets[0].numel() * 4)
+
+    # ---- roofline of the dominant stage (live CUDA-event durations) ----
+    peaks, peak_kind = measured_peaks()
+    roof = roofline(stages, n_isects, final_n, peaks, peak_kind)
+
+    # ---- CPU baseline (rank 0, N=1 only) ----
+    cpu = None
+    if world == 1:
+        try:
+            rate, done, threads, n, kind = cpu_reference_run(seconds=15.0, max_steps=200)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads,
+                   "kind": "reference" if kind.startswith("reference") else "port",
+                   "sample": f"{done} iterations of the same schedule from step 2 ({n} Gaussians), "
+                             f"reference core/cpu backend built -O3, all host threads"}
+        except Exception as e:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        ck = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "timed_window": f"iterations {args.warmup + 1}..{total_steps}",
+                       "gaussians_end": final_n, "isects_mean": float(np.mean(n_isects)),
+                       "l2": "256 MB write between timed steps", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+            "gpu_launches": int(args.steps * launches_per_step(np.mean(n_isects))),
+            "roofline": roof,
+            "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
+            "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+
+
+def _upload(trainer, host_targets, dev):
+    """Copy the next view's target from pinned host memory (the step's input)."""
+    import torch
+    if not trainer._order:
+        trainer._order = list(trainer._rng.permutation(len(trainer.ds.views)))
+    ci = trainer._order[-1]
+    return host_targets[ci].to(dev, non_blocking=True)
+
+
+def launches_per_step(n_isect: float) -> float:
+    """Kernels one plain training step launches: project + 3 scan + emit +
+    passes x (hist + 3 scan + scatter) + ranges + map + raster fwd + ssim + finalize
+    + raster bwd + backward/Adam."""
+    tiles_bits = 11  # 1024x512 -> 2048 tiles
+    passes = (32 + tiles_bits + 7) // 8
+    return 1 + 3 + 1 + passes * 5 + 2 + 1 + 2 + 1 + 1
+
+
+def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
+    """HBM roofline of the dominant stage by time. Algorithmic bytes per launch:
+     proj_sh_bwd_adam: per Gaussian 11 dense params x 3 arrays read + written (264 B)
+       + visible SH 48 x 3 x 2 (1152 B) + slots 36 B per intersection read;
+     rast_fwd: splat records 48 B + id 4 B per intersection + 20 B per pixel written;
+     rast_bwd: 48 + 4 B per intersection read + 36 B slot written + 32 B per pixel;
+     loss_fwd_bwd: 36 B per pixel (render + target read, gradient written);
+     bin_sort: 8 passes-worth of key/value traffic, 32 B per intersection per pass."""
+    if not stages:
+        return None
+    per = {k: v[0] / max(v[1], 1) for k, v in stages.items()}
+    dom = max(per, key=per.get)
+    isect = float(np.mean(n_isects)) if n_isects else 0.0
+    npix = 1024 * 512
+    algo = {
+        "proj_sh_bwd_adam": n_gauss * (264 + 1152) + isect * 40,
+        "rast_fwd": isect * 52 + npix * 20,
+        "rast_bwd": isect * 88 + npix * 32,
+        "loss_fwd_bwd": npix * 36,
+        "bin_sort": isect * 32 * 6 + isect * 24,
+        "proj_sh_fwd": n_gauss * (236 + 76),
+    }.get(dom, 0.0)
+    ms = per[dom]
+    achieved = algo / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
+    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+            "avg_ms": ms, "algorithmic_bytes": algo}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1990)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--quick", action="store_true", help="device-timed pass only (no e2e, no CPU baseline)")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -98,6 +98,36 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
                            float *vis_counts, float *xys_grad_norm, float *max_2d_size, float inv_max_dim,
                            const int32_t **radii_out, float *loss_out);
 
+/* bindings.h:120-135 msplat_densify. The 18 buffers are capacity-sized (buf_capacity
+ * rows): params[6] = means, scales, quats, features_dc, features_rest (fr_stride
+ * floats per row), opacities; exp_avg[6] / exp_avg_sq[6] likewise. Requires
+ * 3*N <= buf_capacity (else MSPLAT_CUDA_ECAPACITY, as the reference throws,
+ * msplat_cpu.cpp:1347). Synchronises once and writes the new count to *new_count. */
+int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float grad_thresh, float size_thresh,
+                        float screen_thresh, int check_screen, float cull_alpha_thresh, float cull_scale_thresh,
+                        float cull_screen_size, int check_huge, const float *xys_grad_norm, const float *vis_counts,
+                        const float *max_2d_size, float half_max_dim, float *const *params, int fr_stride,
+                        float *const *exp_avg, float *const *exp_avg_sq, uint32_t seed, int *new_count);
+
+/* bindings.h:139 msplat_opacity_reset -- logits clamped to <= reset_logit, the opacity
+ * group's Adam moments zeroed. */
+int msplat_cuda_opacity_reset(msplat_cuda_ctx *ctx, float *opacities, float *exp_avg, float *exp_avg_sq,
+                              int num_points, float reset_logit);
+
+/* bindings.h:147 msplat_radix_sort -- stable sort of (keys, vals) by the low key_bits
+ * bits of the keys, in place (device pointers). */
+int msplat_cuda_radix_sort(msplat_cuda_ctx *ctx, uint64_t *keys, int32_t *vals, uint32_t n, int key_bits);
+
+/* bindings.h:151 msplat_knn3_mean_dist -- exact mean distance from each of n points
+ * (n, 3) to its 3 nearest other points. */
+int msplat_cuda_knn3_mean_dist(msplat_cuda_ctx *ctx, const float *points, uint32_t n, float *mean_dist);
+
+/* bindings.h:155 msplat_init_gaussians -- 3-NN isotropic log-scales, random rotations,
+ * DC from RGB (uint8, n x 3), constant opacity logit. */
+int msplat_cuda_init_gaussians(msplat_cuda_ctx *ctx, const float *means, const uint8_t *rgb, uint32_t n,
+                               uint32_t seed, float opacity_logit, float *scales, float *quats, float *features_dc,
+                               float *opacities);
+
 /* Device pointer of the last train step's loss (float, sum / (H*W)). */
 int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
 
@@ -110,6 +140,15 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
 int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count);
 /* Number of tile intersections of the last frame. */
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx);
+
+/* bindings.h:34-39 msplat_enable_gpu_timing / msplat_drain_stage_times. With option
+ * "stage_timing" set, each render / train step records CUDA events at its stage
+ * boundaries (proj_sh_fwd, bin_sort, rast_fwd, loss_fwd_bwd, rast_bwd,
+ * proj_sh_bwd_adam); they are read back lazily, so timing adds no synchronisation to
+ * the calls. This waits for the recorded events, returns the milliseconds and call
+ * counts accumulated since the last drain, and resets them. */
+int msplat_cuda_drain_stage_times(msplat_cuda_ctx *ctx, double *ms, int64_t *calls, int max_stages, int *n_stages,
+                                  const char **names);
 
 #ifdef __cplusplus
 }

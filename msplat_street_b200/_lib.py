@@ -48,9 +48,16 @@ _SIGS = {
     "msplat_cuda_train_step": (i32, [vp, i32, vp, vp, f32, vp, vp, vp, f32, f32, f32, f32, u32, u32, i32, i32, f32,
                                      u32, u32, vp, vp, vp, vp, vp, vp, f32, f32, i32, vp, vp, vp, vp, f32, f32, f32,
                                      vp, vp, vp, f32, PP, vp]),
+    "msplat_cuda_densify": (i32, [vp, i32, i32, f32, f32, f32, i32, f32, f32, f32, i32, vp, vp, vp, f32, vp, i32, vp,
+                                  vp, C.c_uint32, C.POINTER(i32)]),
+    "msplat_cuda_opacity_reset": (i32, [vp, vp, vp, vp, i32, f32]),
+    "msplat_cuda_radix_sort": (i32, [vp, vp, vp, C.c_uint32, i32]),
+    "msplat_cuda_knn3_mean_dist": (i32, [vp, vp, C.c_uint32, vp]),
+    "msplat_cuda_init_gaussians": (i32, [vp, vp, vp, C.c_uint32, C.c_uint32, f32, vp, vp, vp, vp]),
     "msplat_cuda_loss_device": (i32, [vp, PP]),
     "msplat_cuda_frame": (i32, [vp, C.c_char_p, PP, C.POINTER(i64)]),
     "msplat_cuda_num_isects": (i64, [vp]),
+    "msplat_cuda_drain_stage_times": (i32, [vp, vp, vp, i32, C.POINTER(i32), vp]),
 }
 
 # entry points added later in the build; bound when the library exports them

@@ -96,12 +96,18 @@ class AdamState:
         return cls([torch.zeros_like(t) for t in p.tensors()], [torch.zeros_like(t) for t in p.tensors()], list(lrs))
 
     def step_scalars(self):
-        """Model::fullIteration's bias-corrected step sizes (core/src/model.cpp:638-651)."""
-        bc1 = np.float32(1.0) - np.float32(self.beta1) ** np.float32(self.step)
-        bc2 = np.float32(1.0) - np.float32(self.beta2) ** np.float32(self.step)
-        ss = _f32([np.float32(lr) / bc1 for lr in self.lrs])
-        b2 = _f32([np.sqrt(bc2)] * 6)
-        return ss, b2
+        return adam_step_scalars(self.lrs, self.step, self.beta1, self.beta2)
+
+
+def adam_step_scalars(lrs, step: int, beta1: float = 0.9, beta2: float = 0.999):
+    """Model::fullIteration's bias-corrected Adam scalars (core/src/model.cpp:638-651):
+    bc = 1 - pow(beta, t) is evaluated in double (std::pow(float, int)) and stored as
+    float; step_size = lr / bc1 and bc2_sqrt = sqrt(bc2) in float."""
+    bc1 = np.float32(1.0 - float(np.float32(beta1)) ** int(step))
+    bc2 = np.float32(1.0 - float(np.float32(beta2)) ** int(step))
+    ss = _f32([np.float32(lr) / bc1 for lr in lrs])
+    b2 = _f32([np.sqrt(bc2)] * len(lrs))
+    return ss, b2
 
 
 class Context:
@@ -195,6 +201,67 @@ class Context:
         check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out), src, 4))
         return out
 
+    # -- bindings.h:120-155 ----------------------------------------------------------
+    def densify(self, n: int, buffers: List[torch.Tensor], exp_avg: List[torch.Tensor],
+                exp_avg_sq: List[torch.Tensor], grad_norm: torch.Tensor, vis_counts: torch.Tensor,
+                max_2d: torch.Tensor, half_max_dim: float, seed: int, grad_thresh: float = 2e-4,
+                size_thresh: float = 0.01, screen_thresh: float = 0.05, check_screen: bool = True,
+                cull_alpha: float = 0.1, cull_scale: float = 0.5, cull_screen: float = 0.15,
+                check_huge: bool = True) -> int:
+        """msplat_densify over capacity-sized buffers (6 params + 12 moments), in place.
+        Returns the new Gaussian count (one host synchronisation)."""
+        self.bind_stream()
+        cap = int(buffers[0].shape[0])
+        fr_stride = int(buffers[4].numel() // cap) if cap else 0
+        pp = (C.c_void_p * 6)(*[t.data_ptr() for t in buffers])
+        m1 = (C.c_void_p * 6)(*[t.data_ptr() for t in exp_avg])
+        m2 = (C.c_void_p * 6)(*[t.data_ptr() for t in exp_avg_sq])
+        out = C.c_int(0)
+        check(self._lib.msplat_cuda_densify(
+            self.handle, n, cap, grad_thresh, size_thresh, screen_thresh, int(check_screen), cull_alpha, cull_scale,
+            cull_screen, int(check_huge), ptr(grad_norm), ptr(vis_counts), ptr(max_2d), half_max_dim,
+            C.cast(pp, C.c_void_p), fr_stride, C.cast(m1, C.c_void_p), C.cast(m2, C.c_void_p),
+            C.c_uint32(seed & 0xFFFFFFFF), C.byref(out)))
+        return int(out.value)
+
+    def opacity_reset(self, opacities: torch.Tensor, exp_avg: torch.Tensor, exp_avg_sq: torch.Tensor, n: int,
+                      reset_logit: float = -1.3862943611198906) -> None:
+        self.bind_stream()
+        check(self._lib.msplat_cuda_opacity_reset(self.handle, ptr(opacities), ptr(exp_avg), ptr(exp_avg_sq), n,
+                                                  reset_logit))
+
+    def radix_sort(self, keys: torch.Tensor, vals: torch.Tensor, key_bits: int) -> None:
+        """Stable in-place sort of int64 keys (by their low key_bits) with int32 values."""
+        self.bind_stream()
+        if keys.dtype != torch.int64 or vals.dtype != torch.int32 or not keys.is_cuda:
+            raise ValueError("keys must be int64 and vals int32 CUDA tensors")
+        check(self._lib.msplat_cuda_radix_sort(self.handle, ptr(keys), ptr(vals), keys.numel(), key_bits))
+
+    def knn3_mean_dist(self, points: torch.Tensor) -> torch.Tensor:
+        self.bind_stream()
+        require_cuda(points, "points")
+        out = torch.empty(points.shape[0], dtype=torch.float32, device=points.device)
+        check(self._lib.msplat_cuda_knn3_mean_dist(self.handle, ptr(points), points.shape[0], ptr(out)))
+        return out
+
+    def init_gaussians(self, means: torch.Tensor, rgb: torch.Tensor, seed: int = 42,
+                       opacity_logit: float = float(np.log(0.1 / 0.9)), sh_degree: int = 3) -> GaussianParams:
+        """msplat_init_gaussians + zero SH rest: the Model constructor's start state
+        (core/src/model.cpp:57-71)."""
+        self.bind_stream()
+        require_cuda(means, "means")
+        n = means.shape[0]
+        dev = means.device
+        scales = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        quats = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        dc = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        opac = torch.empty((n, 1), dtype=torch.float32, device=dev)
+        rgb = rgb.to(device=dev, dtype=torch.uint8).contiguous()
+        check(self._lib.msplat_cuda_init_gaussians(self.handle, ptr(means), ptr(rgb), n, seed & 0xFFFFFFFF,
+                                                   opacity_logit, ptr(scales), ptr(quats), ptr(dc), ptr(opac)))
+        rest = torch.zeros((n, (sh_degree + 1) ** 2 - 1, 3), dtype=torch.float32, device=dev)
+        return GaussianParams(means.clone(), scales, quats, dc, rest, opac)
+
     # -- intermediates -------------------------------------------------------------
     def frame(self, name: str) -> torch.Tensor:
         """A copy of one frame-cache buffer (see msplat_cuda_frame)."""
@@ -209,6 +276,19 @@ class Context:
 
     def num_isects(self) -> int:
         return int(self._lib.msplat_cuda_num_isects(self.handle))
+
+    def enable_stage_timing(self, on: bool = True) -> None:
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"stage_timing", int(on)))
+
+    def drain_stage_times(self):
+        """{stage: (total ms, calls)} accumulated since the last drain."""
+        ms = (C.c_double * 8)()
+        calls = (C.c_int64 * 8)()
+        names = (C.c_char_p * 8)()
+        n = C.c_int()
+        check(self._lib.msplat_cuda_drain_stage_times(self.handle, C.cast(ms, C.c_void_p), C.cast(calls, C.c_void_p),
+                                                      8, C.byref(n), C.cast(names, C.c_void_p)))
+        return {names[i].decode(): (float(ms[i]), int(calls[i])) for i in range(n.value)}
 
     def sync(self) -> None:
         check(self._lib.msplat_cuda_sync(self.handle))

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -46,9 +47,75 @@ struct Buf {
 
 }  // namespace
 
+// Stage timing with CUDA events on the context's stream (the reference's
+// PROFILE_STAGES, core/metal/msplat_metal.mm:29-32, drained by
+// msplat_drain_stage_times, core/metal/bindings.h:38).
+constexpr int N_STAGES = 6;
+const char *const STAGE_NAMES[N_STAGES] = {"proj_sh_fwd", "bin_sort", "rast_fwd", "loss_fwd_bwd", "rast_bwd",
+                                           "proj_sh_bwd_adam"};
+
+// Each call records its marks into one slot of a ring; a slot is read back only when
+// the ring comes round to it again (long finished by then) or on drain, so timing
+// adds no synchronisation to the calls themselves.
+constexpr int TIMER_RING = 64;
+
+struct StageTimer {
+    bool on = false;
+    int cur = 0;
+    cudaEvent_t ev[TIMER_RING][N_STAGES + 1] = {};
+    bool marked[TIMER_RING][N_STAGES + 1] = {};
+    double acc_ms[N_STAGES] = {};
+    int64_t calls[N_STAGES] = {};
+    void init() {
+        for (auto &slot : ev)
+            for (auto &e : slot)
+                if (!e) cudaEventCreate(&e);
+    }
+    void reset_marks() {
+        for (bool &m : marked[cur]) m = false;
+    }
+    void mark(int i, cudaStream_t st) {
+        if (!on) return;
+        cudaEventRecord(ev[cur][i], st);
+        marked[cur][i] = true;
+    }
+    // accumulate every consecutive pair of recorded marks of one slot
+    void collect_slot(int s) {
+        int last = -1;
+        for (int i = 0; i <= N_STAGES; i++) {
+            if (!marked[s][i]) continue;
+            if (last >= 0) {
+                cudaEventSynchronize(ev[s][i]);
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, ev[s][last], ev[s][i]) == cudaSuccess) {
+                    acc_ms[last] += ms;
+                    calls[last] += 1;
+                }
+            }
+            last = i;
+        }
+        for (bool &m : marked[s]) m = false;
+    }
+    // end of a call: move to the next slot, reading back the one found there
+    void collect() {
+        if (!on) return;
+        cur = (cur + 1) % TIMER_RING;
+        collect_slot(cur);
+    }
+    void drain() {
+        for (int s = 0; s < TIMER_RING; s++) collect_slot(s);
+    }
+    void destroy() {
+        for (auto &slot : ev)
+            for (auto &e : slot)
+                if (e) cudaEventDestroy(e), e = nullptr;
+    }
+};
+
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
     bool keep_grads = false;
+    StageTimer timer;
     // frame description
     int n = 0, W = 0, H = 0, tiles_x = 0, tiles_y = 0;
     int64_t n_isect = 0;
@@ -60,14 +127,21 @@ struct msplat_cuda_ctx {
     Buf keys[2], vals[2], emit_gid, isect_gid, inv, slots, radix_scratch;
     // per tile / pixel
     Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
+    // densification and primitive scratch
+    Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md;
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
+    int32_t *h_count = nullptr;  // pinned readback of the densified count
 
-    ~msplat_cuda_ctx() { release(); }
+    ~msplat_cuda_ctx() {
+        release();
+        timer.destroy();
+    }
     void release() {
         Buf *all[] = {&splats, &radii, &aabb, &n_tiles, &offsets, &scan_part, &total, &v_xy, &v_conic, &v_rgb,
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
-                      &final_idx, &v_rendered, &loss_part, &loss};
+                      &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
+                      &k_sorted, &k_box, &k_md};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);
             b->ptr = nullptr;
@@ -75,6 +149,8 @@ struct msplat_cuda_ctx {
         }
         if (h_total) cudaFreeHost(h_total);
         h_total = nullptr;
+        if (h_count) cudaFreeHost(h_count);
+        h_count = nullptr;
     }
 };
 
@@ -190,6 +266,8 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     pa.radii = radii;
     pa.aabb = aabb;
     pa.n_tiles = n_tiles;
+    ctx->timer.reset_marks();
+    ctx->timer.mark(0, st);
     launch_project(pa, st);
     scan_exclusive<int64_t>(n_tiles, offsets, n, d_total, scan_part, st);
     CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -208,6 +286,7 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ENSURE(ctx->inv, n_isect, int32_t, inv);
     ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
 
+    ctx->timer.mark(1, st);
     launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y, k0, v0, emit_gid, st);
     uint64_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
@@ -230,7 +309,9 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ra.out_img = out_img;
     ra.final_T = final_T;
     ra.final_idx = final_idx;
+    ctx->timer.mark(2, st);
     launch_raster_fwd(ra, st);
+    ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
 }
@@ -274,6 +355,12 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
     if (!ctx || !name) return fail(MSPLAT_CUDA_EINVAL, "null context or option name");
     if (!std::strcmp(name, "keep_grads")) {
         ctx->keep_grads = value != 0;
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "stage_timing")) {
+        if (value) ctx->timer.init();
+        ctx->timer.on = value != 0;
+        ctx->timer.reset_marks();
         return MSPLAT_CUDA_OK;
     }
     return fail(MSPLAT_CUDA_EINVAL, "unknown option '%s'", name);
@@ -334,6 +421,7 @@ int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3
     if (int r = forward(ctx, num_points, means3d, scales, glob_scale, quats, cam, features_dc, features_rest,
                         opacities, background))
         return r;
+    ctx->timer.collect();
     if (out_img) *out_img = reinterpret_cast<const float *>(ctx->out_img.ptr);
     return MSPLAT_CUDA_OK;
 }
@@ -384,6 +472,7 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     sa.partials = loss_part;
     sa.loss = d_loss;
     launch_ssim_loss(sa, st);
+    ctx->timer.mark(4, st);
 
     RasterBwdArgs rb;
     rb.W = (int)img_width;
@@ -400,6 +489,7 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     rb.v_out = v_rendered;
     rb.slots = slots;
     launch_raster_bwd(rb, st);
+    ctx->timer.mark(5, st);
 
     BackwardArgs ba;
     std::memset(&ba, 0, sizeof ba);
@@ -457,12 +547,157 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     if (vis_counts && (!xys_grad_norm || !max_2d_size))
         return fail(MSPLAT_CUDA_EINVAL, "densification statistics need all three buffers");
     launch_backward_adam(ba, st);
+    ctx->timer.mark(6, st);
     CUDA_TRY(cudaGetLastError());
+    ctx->timer.collect();
     if (radii_out) *radii_out = reinterpret_cast<const int32_t *>(ctx->radii.ptr);
     if (loss_out) {
         CUDA_TRY(cudaMemcpyAsync(loss_out, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
     }
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float grad_thresh, float size_thresh,
+                        float screen_thresh, int check_screen, float cull_alpha_thresh, float cull_scale_thresh,
+                        float cull_screen_size, int check_huge, const float *xys_grad_norm, const float *vis_counts,
+                        const float *max_2d_size, float half_max_dim, float *const *params, int fr_stride,
+                        float *const *exp_avg, float *const *exp_avg_sq, uint32_t seed, int *new_count) {
+    if (!ctx || !new_count) return fail(MSPLAT_CUDA_EINVAL, "null context or output");
+    if (N < 0 || fr_stride < 0) return fail(MSPLAT_CUDA_EINVAL, "negative size");
+    if ((int64_t)3 * N > buf_capacity)
+        return fail(MSPLAT_CUDA_ECAPACITY, "msplat_densify: 3*N (%lld) exceeds buf_capacity (%d)", 3ll * N,
+                    buf_capacity);
+    if (N > 0 && (!params || !exp_avg || !exp_avg_sq || !xys_grad_norm || !vis_counts || !max_2d_size))
+        return fail(MSPLAT_CUDA_EINVAL, "null densify buffer");
+    cudaStream_t st = ctx->stream;
+    DensifyArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = N;
+    a.grad_thresh = grad_thresh;
+    a.size_thresh = size_thresh;
+    a.screen_thresh = screen_thresh;
+    a.check_screen = check_screen;
+    a.cull_alpha = cull_alpha_thresh;
+    a.cull_scale = cull_scale_thresh;
+    a.cull_screen = cull_screen_size;
+    a.check_huge = check_huge;
+    a.grad_norm = xys_grad_norm;
+    a.vis_counts = vis_counts;
+    a.max_2d = max_2d_size;
+    a.half_max_dim = half_max_dim;
+    a.log_size_fac = std::log(1.6f);  // the host's logf, as the reference computes it (msplat_cpu.cpp:1348)
+    a.seed = seed;
+    const int strides[6] = {3, 3, 4, 3, fr_stride, 1};
+    int max_stride = 1;
+    for (int g = 0; g < 6; g++) {
+        a.stride[g] = strides[g];
+        max_stride = std::max(max_stride, strides[g]);
+        if (N > 0) {
+            a.buf[g] = params[g];
+            a.m1[g] = exp_avg[g];
+            a.m2[g] = exp_avg_sq[g];
+            if ((!a.buf[g] || !a.m1[g] || !a.m2[g]) && strides[g] > 0)
+                return fail(MSPLAT_CUDA_EINVAL, "null buffer for group %d", g);
+        }
+    }
+    const int64_t rows = 3 * (int64_t)std::max(N, 1);
+    ENSURE(ctx->d_flags, 6 * rows, int32_t, flags);
+    ENSURE(ctx->d_counts, 8 + scan_blocks((int)rows) + 1, int32_t, counts);
+    ENSURE(ctx->d_scratch, rows * max_stride, float, scratch);
+    if (!ctx->h_count) CUDA_TRY(cudaMallocHost(&ctx->h_count, sizeof(int32_t)));
+    DensifyScratch s;
+    s.split = flags;
+    s.dup = flags + rows;
+    s.split_ord = flags + 2 * rows;
+    s.dup_ord = flags + 3 * rows;
+    s.keep = flags + 4 * rows;
+    s.keep_ord = flags + 5 * rows;
+    s.n_split = counts;
+    s.n_dup = counts + 1;
+    s.n_new = counts + 2;
+    s.new_count = counts + 3;
+    s.scan_part = counts + 8;
+    s.scratch = scratch;
+    launch_densify(a, s, st);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_count, s.new_count, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *new_count = *ctx->h_count;
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_opacity_reset(msplat_cuda_ctx *ctx, float *opacities, float *exp_avg, float *exp_avg_sq,
+                              int num_points, float reset_logit) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (num_points < 0) return fail(MSPLAT_CUDA_EINVAL, "negative count");
+    if (num_points > 0 && (!opacities || !exp_avg || !exp_avg_sq)) return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    launch_opacity_reset(opacities, exp_avg, exp_avg_sq, num_points, reset_logit, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_radix_sort(msplat_cuda_ctx *ctx, uint64_t *keys, int32_t *vals, uint32_t n, int key_bits) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (n == 0) return MSPLAT_CUDA_OK;
+    if (!keys || !vals) return fail(MSPLAT_CUDA_EINVAL, "null keys or values");
+    if (n > (uint32_t)INT32_MAX) return fail(MSPLAT_CUDA_EINVAL, "too many keys");
+    if (key_bits <= 0) return MSPLAT_CUDA_OK;
+    if (key_bits > 64) key_bits = 64;
+    ENSURE(ctx->keys[1], n, uint64_t, k1);
+    ENSURE(ctx->vals[1], n, uint32_t, v1);
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n), unsigned char, rs);
+    uint64_t *kk[2] = {keys, k1};
+    uint32_t *vv[2] = {reinterpret_cast<uint32_t *>(vals), v1};
+    const int cur = radix_sort_pairs(kk, vv, (int)n, key_bits, rs, ctx->stream);
+    if (cur == 1) {
+        CUDA_TRY(cudaMemcpyAsync(keys, k1, (size_t)n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(vals, v1, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_knn3_mean_dist(msplat_cuda_ctx *ctx, const float *points, uint32_t n, float *mean_dist) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (n == 0) return MSPLAT_CUDA_OK;
+    if (!points || !mean_dist) return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    if (n > (uint32_t)INT32_MAX) return fail(MSPLAT_CUDA_EINVAL, "too many points");
+    const int nb = knn_boxes((int)n);
+    ENSURE(ctx->k_bounds, 8, unsigned int, bounds);
+    ENSURE(ctx->keys[0], n, uint64_t, k0);
+    ENSURE(ctx->keys[1], n, uint64_t, k1);
+    ENSURE(ctx->vals[0], n, uint32_t, v0);
+    ENSURE(ctx->vals[1], n, uint32_t, v1);
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n), unsigned char, rs);
+    ENSURE(ctx->k_sorted, n, float4, sorted);
+    ENSURE(ctx->k_box, 2 * (size_t)nb, float4, boxes);
+    KnnScratch s;
+    s.bounds = bounds;
+    s.keys[0] = k0;
+    s.keys[1] = k1;
+    s.vals[0] = v0;
+    s.vals[1] = v1;
+    s.radix_scratch = rs;
+    s.sorted = sorted;
+    s.bmin = boxes;
+    s.bmax = boxes + nb;
+    launch_knn3(points, (int)n, mean_dist, s, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_init_gaussians(msplat_cuda_ctx *ctx, const float *means, const uint8_t *rgb, uint32_t n,
+                               uint32_t seed, float opacity_logit, float *scales, float *quats, float *features_dc,
+                               float *opacities) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (n == 0) return MSPLAT_CUDA_OK;
+    if (!means || !rgb || !scales || !quats || !features_dc || !opacities)
+        return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    ENSURE(ctx->k_md, n, float, md);
+    if (int r = msplat_cuda_knn3_mean_dist(ctx, means, n, md)) return r;
+    launch_init_gaussians(md, rgb, (int)n, seed, opacity_logit, scales, quats, features_dc, opacities, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
 }
 
@@ -474,6 +709,24 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
 }
 
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
+
+int msplat_cuda_drain_stage_times(msplat_cuda_ctx *ctx, double *ms, int64_t *calls, int max_stages, int *n_stages,
+                                  const char **names) {
+    if (!ctx || !n_stages) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    ctx->timer.drain();
+    const int n = std::min(max_stages, N_STAGES);
+    for (int i = 0; i < n; i++) {
+        if (ms) ms[i] = ctx->timer.acc_ms[i];
+        if (calls) calls[i] = ctx->timer.calls[i];
+        if (names) names[i] = STAGE_NAMES[i];
+    }
+    for (int i = 0; i < N_STAGES; i++) {
+        ctx->timer.acc_ms[i] = 0.0;
+        ctx->timer.calls[i] = 0;
+    }
+    *n_stages = n;
+    return MSPLAT_CUDA_OK;
+}
 
 int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count) {
     if (!ctx || !name || !dev_ptr || !count) return fail(MSPLAT_CUDA_EINVAL, "null argument");

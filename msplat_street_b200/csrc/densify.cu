@@ -1,0 +1,199 @@
+// Densification: classify, split, duplicate, cull and stream compaction; opacity reset.
+//
+// Follows msplat_densify (core/cpu/msplat_cpu.cpp:1330-1465) step by step:
+//  1. classify (:1354-1369): a Gaussian seen in at least one view with mean screen
+//     gradient (gn / vc) * half_max_dim above the threshold is split when its largest
+//     scale exceeds size_thresh (or its screen size split_screen_size), and cloned
+//     when it is small;
+//  2. ordinals by exclusive scans (the reference counts serially, :1370-1375);
+//  3. split children at N + 2*ord + k, offset by a parent-rotated N(0, s) sample
+//     from the PCG/Box-Muller counter RNG, scales minus log(1.6); the parent's scales
+//     shrink too (:1387-1415); then clones at N + 2*n_split + ord (:1417-1430), after
+//     every split (a Gaussian may be both, and the clone copies the shrunk parent);
+//  4. cull (:1432-1448) over the N_new rows and order-preserving compaction of all 18
+//     buffers (6 parameters, 6 first moments, 6 second moments) through a scratch
+//     buffer, one buffer at a time (:1449-1464).
+// Child and clone moments are zeroed. Counts live on the device; the host reads the
+// final count once (the reference's Metal backend also syncs there,
+// core/metal/msplat_metal.mm:1998-2001).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace msplat {
+
+__global__ void densify_classify_kernel(DensifyArgs a, int32_t *split, int32_t *dup) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    int s = 0, d = 0;
+    const float vc = a.vis_counts[i];
+    if (vc > 0.0f) {
+        const bool high = (a.grad_norm[i] / vc) * a.half_max_dim > a.grad_thresh;
+        const float *sc = a.buf[1] + 3 * (size_t)i;
+        const float mx = fmaxf(fmaxf(exp_ref(sc[0]), exp_ref(sc[1])), exp_ref(sc[2]));
+        const bool large = mx > a.size_thresh;
+        bool sp = large;
+        if (a.check_screen && a.max_2d[i] > a.screen_thresh) sp = true;
+        s = (sp && high) ? 1 : 0;
+        d = (!large && high) ? 1 : 0;
+    }
+    split[i] = s;
+    dup[i] = d;
+}
+
+__device__ __forceinline__ void zero_moments(const DensifyArgs &a, int64_t row) {
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+        const int st = a.stride[g];
+        float *m1 = a.m1[g] + row * st, *m2 = a.m2[g] + row * st;
+        for (int j = 0; j < st; j++) {
+            m1[j] = 0.f;
+            m2[j] = 0.f;
+        }
+    }
+}
+
+__device__ __forceinline__ void copy_params(const DensifyArgs &a, int64_t dst, int64_t src) {
+    // means and scales are written by the caller where they differ
+    for (int j = 0; j < 4; j++) a.buf[2][4 * dst + j] = a.buf[2][4 * src + j];
+    for (int j = 0; j < 3; j++) a.buf[3][3 * dst + j] = a.buf[3][3 * src + j];
+    const int fr = a.stride[4];
+    for (int j = 0; j < fr; j++) a.buf[4][dst * fr + j] = a.buf[4][src * fr + j];
+    a.buf[5][dst] = a.buf[5][src];
+}
+
+// Box-Muller on the PCG counter RNG (core/cpu/msplat_cpu.cpp:315-323)
+__device__ __forceinline__ V3 rand_normal3(uint32_t seed, uint32_t stream) {
+    const uint32_t c = stream * 4u;
+    const float u0 = rand_unif(seed, c), u1 = rand_unif(seed, c + 1u);
+    const float u2 = rand_unif(seed, c + 2u), u3 = rand_unif(seed, c + 3u);
+    const float r0 = sqrtf(-2.0f * (float)log((double)u0)), r1 = sqrtf(-2.0f * (float)log((double)u2));
+    const float tau = 6.28318530717958647692f;
+    const float t0 = tau * u1, t1 = tau * u3;
+    return V3{r0 * (float)cos((double)t0), r0 * (float)sin((double)t0), r1 * (float)cos((double)t1)};
+}
+
+__global__ void densify_split_kernel(DensifyArgs a, const int32_t *split, const int32_t *split_ord) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n || !split[i]) return;
+    const int ord = split_ord[i];
+    float *means = a.buf[0], *scales = a.buf[1];
+    const float *q = a.buf[2] + 4 * (size_t)i;
+    float qw = q[0], qx = q[1], qy = q[2], qz = q[3];
+    const float ql = sqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
+    qw /= ql;
+    qx /= ql;
+    qy /= ql;
+    qz /= ql;
+    const float sx = exp_ref(scales[3 * i]), sy = exp_ref(scales[3 * i + 1]), sz = exp_ref(scales[3 * i + 2]);
+    for (int k = 0; k < 2; k++) {
+        const int64_t c = (int64_t)a.n + 2 * ord + k;
+        const V3 nr = rand_normal3(a.seed, (uint32_t)(ord * 2 + k));
+        const float r0 = nr.x * sx, r1 = nr.y * sy, r2 = nr.z * sz;
+        const float v0 = (1.f - 2.f * (qy * qy + qz * qz)) * r0 + 2.f * (qx * qy - qw * qz) * r1 +
+                         2.f * (qx * qz + qw * qy) * r2;
+        const float v1 = 2.f * (qx * qy + qw * qz) * r0 + (1.f - 2.f * (qx * qx + qz * qz)) * r1 +
+                         2.f * (qy * qz - qw * qx) * r2;
+        const float v2 = 2.f * (qx * qz - qw * qy) * r0 + 2.f * (qy * qz + qw * qx) * r1 +
+                         (1.f - 2.f * (qx * qx + qy * qy)) * r2;
+        means[3 * c] = means[3 * i] + v0;
+        means[3 * c + 1] = means[3 * i + 1] + v1;
+        means[3 * c + 2] = means[3 * i + 2] + v2;
+        for (int j = 0; j < 3; j++) scales[3 * c + j] = scales[3 * i + j] - a.log_size_fac;
+        copy_params(a, c, i);
+        zero_moments(a, c);
+    }
+    for (int j = 0; j < 3; j++) scales[3 * i + j] -= a.log_size_fac;
+}
+
+__global__ void densify_dup_kernel(DensifyArgs a, const int32_t *dup, const int32_t *dup_ord, const int32_t *n_split) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n || !dup[i]) return;
+    const int64_t d = (int64_t)a.n + 2 * (int64_t)(*n_split) + dup_ord[i];
+    for (int j = 0; j < 3; j++) a.buf[0][3 * d + j] = a.buf[0][3 * i + j];
+    for (int j = 0; j < 3; j++) a.buf[1][3 * d + j] = a.buf[1][3 * i + j];
+    copy_params(a, d, i);
+    zero_moments(a, d);
+}
+
+__global__ void densify_cull_kernel(DensifyArgs a, const int32_t *split, const int32_t *n_split,
+                                    const int32_t *n_dup, int32_t *keep, int32_t *n_new) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)a.n + 2 * (int64_t)(*n_split) + *n_dup;
+    if (i == 0) *n_new = (int32_t)total;
+    if (i >= 3 * (int64_t)a.n) return;
+    if (i >= total) {
+        keep[i] = 0;
+        return;
+    }
+    const float o = 1.0f / (1.0f + exp_ref(-a.buf[5][i]));
+    bool cull = o < a.cull_alpha;
+    if (i < a.n && split[i]) cull = true;
+    if (a.check_huge) {
+        const float *sc = a.buf[1] + 3 * i;
+        const float mx = fmaxf(fmaxf(exp_ref(sc[0]), exp_ref(sc[1])), exp_ref(sc[2]));
+        if (mx > a.cull_scale) cull = true;
+        if (a.check_screen && i < a.n && a.max_2d[i] > a.cull_screen) cull = true;
+    }
+    keep[i] = cull ? 0 : 1;
+}
+
+// one buffer: kept rows to scratch at their ordinal, then back
+__global__ void compact_gather_kernel(const float *src, float *scratch, int stride, const int32_t *keep,
+                                      const int32_t *keep_ord, const int32_t *n_new) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t row = t / stride;
+    if (row >= *n_new) return;
+    if (!keep[row]) return;
+    const int col = (int)(t - row * stride);
+    scratch[(int64_t)keep_ord[row] * stride + col] = src[t];
+}
+
+__global__ void compact_copy_back_kernel(float *dst, const float *scratch, int stride, const int32_t *new_count) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)(*new_count) * stride) return;
+    dst[t] = scratch[t];
+}
+
+__global__ void opacity_reset_kernel(float *o, float *m1, float *m2, int n, float reset_logit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    o[i] = fminf(o[i], reset_logit);
+    m1[i] = 0.f;
+    m2[i] = 0.f;
+}
+
+void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st) {
+    const int n = a.n;
+    if (n <= 0) {
+        cudaMemsetAsync(s.new_count, 0, sizeof(int32_t), st);
+        return;
+    }
+    const int bs = 256;
+    const int gb = (n + bs - 1) / bs;
+    densify_classify_kernel<<<gb, bs, 0, st>>>(a, s.split, s.dup);
+    scan_exclusive<int32_t>(s.split, s.split_ord, n, s.n_split, s.scan_part, st);
+    scan_exclusive<int32_t>(s.dup, s.dup_ord, n, s.n_dup, s.scan_part, st);
+    densify_split_kernel<<<gb, bs, 0, st>>>(a, s.split, s.split_ord);
+    densify_dup_kernel<<<gb, bs, 0, st>>>(a, s.dup, s.dup_ord, s.n_split);
+    const int64_t rows = 3 * (int64_t)n;
+    densify_cull_kernel<<<(unsigned)((rows + bs - 1) / bs), bs, 0, st>>>(a, s.split, s.n_split, s.n_dup, s.keep,
+                                                                       s.n_new);
+    scan_exclusive<int32_t>(s.keep, s.keep_ord, (int)rows, s.new_count, s.scan_part, st);
+    for (int b = 0; b < 18; b++) {
+        const int g = b % 6;
+        float *buf = b < 6 ? a.buf[g] : (b < 12 ? a.m1[g] : a.m2[g]);
+        const int stride = a.stride[g];
+        if (stride <= 0) continue;  // e.g. no SH rest at degree 0
+        const int64_t elems = rows * stride;
+        const unsigned grid = (unsigned)((elems + bs - 1) / bs);
+        compact_gather_kernel<<<grid, bs, 0, st>>>(buf, s.scratch, stride, s.keep, s.keep_ord, s.n_new);
+        compact_copy_back_kernel<<<grid, bs, 0, st>>>(buf, s.scratch, stride, s.new_count);
+    }
+}
+
+void launch_opacity_reset(float *o, float *m1, float *m2, int n, float reset_logit, cudaStream_t st) {
+    if (n <= 0) return;
+    opacity_reset_kernel<<<(n + 255) / 256, 256, 0, st>>>(o, m1, m2, n, reset_logit);
+}
+
+}  // namespace msplat

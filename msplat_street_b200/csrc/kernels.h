@@ -101,4 +101,36 @@ struct BackwardArgs {
 };
 void launch_backward_adam(const BackwardArgs &a, cudaStream_t st);
 
+struct DensifyArgs {
+    int n;
+    float grad_thresh, size_thresh, screen_thresh;
+    int check_screen;
+    float cull_alpha, cull_scale, cull_screen;
+    int check_huge;
+    const float *grad_norm, *vis_counts, *max_2d;
+    float half_max_dim, log_size_fac;
+    uint32_t seed;
+    float *buf[6], *m1[6], *m2[6];  // capacity-sized: means scales quats dc rest opacity
+    int stride[6];
+};
+struct DensifyScratch {
+    int32_t *split, *dup, *split_ord, *dup_ord, *keep, *keep_ord;
+    int32_t *n_split, *n_dup, *n_new, *new_count, *scan_part;
+    float *scratch;  // 3N x max(stride) floats
+};
+void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st);
+void launch_opacity_reset(float *o, float *m1, float *m2, int n, float reset_logit, cudaStream_t st);
+
+struct KnnScratch {
+    unsigned int *bounds;  // 6 ordered-bit floats: min xyz, max xyz
+    uint64_t *keys[2];
+    uint32_t *vals[2];
+    void *radix_scratch;
+    float4 *sorted, *bmin, *bmax;
+};
+int knn_boxes(int n);
+int launch_knn3(const float *pts, int n, float *out, KnnScratch &s, cudaStream_t st);
+void launch_init_gaussians(const float *md, const uint8_t *rgb, int n, uint32_t seed, float logit, float *scales,
+                           float *quats, float *dc, float *opac, cudaStream_t st);
+
 }  // namespace msplat

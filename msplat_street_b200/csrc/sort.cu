@@ -167,7 +167,7 @@ constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per war
 
 int radix_blocks(int n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
-__global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32_t *counts, int nb) {
+__global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32_t mask, uint32_t *counts, int nb) {
     __shared__ uint32_t h[RADIX];
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
     __syncthreads();
@@ -177,7 +177,7 @@ __global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32
     for (int j = 0; j < SORT_ITEMS; j++) {
         const int k = base + j * SORT_THREADS + threadIdx.x;
         const bool ok = k < n;
-        const int d = ok ? (int)((keys[k] >> shift) & (RADIX - 1)) : RADIX;
+        const int d = ok ? (int)((keys[k] >> shift) & mask) : RADIX;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
     }
@@ -187,7 +187,7 @@ __global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
 __global__ void radix_scatter_kernel(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout, int n,
-                                     int shift, const int32_t *offs, int nb) {
+                                     int shift, uint32_t mask, const int32_t *offs, int nb) {
     __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
     __shared__ uint32_t gbase[RADIX];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -205,7 +205,7 @@ __global__ void radix_scatter_kernel(const uint64_t *kin, const uint32_t *vin, u
         const bool ok = k < n;
         key[r] = ok ? kin[k] : 0ull;
         val[r] = ok ? vin[k] : 0u;
-        const int d = ok ? (int)((key[r] >> shift) & (RADIX - 1)) : RADIX;
+        const int d = ok ? (int)((key[r] >> shift) & mask) : RADIX;
         dig[r] = d;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = ok ? wcnt[warp][d] : 0u;
@@ -254,9 +254,13 @@ int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *
     int32_t *partials = offs + cnt;
     int cur = 0;
     for (int shift = 0; shift < key_bits; shift += 8) {
-        radix_hist_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], n, shift, reinterpret_cast<uint32_t *>(counts), nb);
+        const int bits = key_bits - shift < 8 ? key_bits - shift : 8;  // digits above key_bits are ignored
+        const uint32_t mask = (1u << bits) - 1u;
+        radix_hist_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], n, shift, mask, reinterpret_cast<uint32_t *>(counts),
+                                                       nb);
         scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, shift, offs, nb);
+        radix_scatter_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, shift, mask, offs,
+                                                          nb);
         cur ^= 1;
     }
     return cur;

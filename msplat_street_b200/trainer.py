@@ -1,0 +1,259 @@
+"""Training loop host logic: the reference's Model and GaussianTrainer for this backend.
+
+Restates core/src/model.cpp's training-side host code over the C-ABI:
+ * capacity-backed parameter and Adam buffers with views of the active rows
+   (setupOptimizers / refreshViews / ensureCapacity, model.cpp:81-193);
+ * per-group learning rates and the log-linear means decay (model.cpp:100, :140-143);
+ * Adam bias correction per step (fullIteration, :638-651);
+ * the densification schedule (afterTrain, :199-245): every refine_every steps after
+   the warm-up, densify while step < iterations / 2 and the reset-interval rule holds,
+   reset opacities on the reset interval, clear the statistics;
+ * SH degree ramp degrees_to_use = min(step // sh_degree_interval, sh_degree) (:535).
+The camera set-up (prepareCam) is msplat_street_b200.camera.prepare_cam. The public
+surface mirrors the reference's TrainingConfig / TrainingStats / GaussianTrainer
+(python/msplat/_core.pyi:157-267) for in-memory datasets; file loaders and the
+prior-guided "street" extras are outside this backend.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from .backend import AdamState, Context, GaussianParams
+from .camera import CameraSetup, prepare_cam
+
+LR_INIT = (0.00016, 0.005, 0.001, 0.0025, 0.000125, 0.05)  # model.cpp:100
+MEANS_LR_FINAL = 0.0000016                                   # model.cpp:111
+RESET_LOGIT = -1.3862943611198906                            # logit(0.2), model.cpp:236
+
+
+@dataclass
+class TrainingConfig:
+    """Field names and defaults of the reference's TrainingConfig (python/bindings.cpp:27-60)."""
+
+    iterations: int = 30000
+    sh_degree: int = 3
+    sh_degree_interval: int = 1000
+    ssim_weight: float = 0.2
+    refine_every: int = 100
+    warmup_length: int = 500
+    reset_alpha_every: int = 30
+    densify_grad_thresh: float = 0.0002
+    densify_size_thresh: float = 0.01
+    stop_screen_size_at: int = 4000
+    split_screen_size: float = 0.05
+    bg_color: Sequence[float] = (0.6130, 0.0101, 0.3984)
+    # the thresholds Model::afterTrain hard-codes (model.cpp:218), exposed here
+    cull_alpha_thresh: float = 0.1
+    cull_scale_thresh: float = 0.5
+    cull_screen_size: float = 0.15
+    # learning rates (model.cpp:100); None keeps the reference's
+    lrs: Optional[Sequence[float]] = None
+    seed: int = 42
+
+
+@dataclass
+class TrainingStats:
+    iteration: int
+    splat_count: int
+    ms_per_step: float
+
+
+@dataclass
+class View:
+    """One training camera: its pose, intrinsics and target image."""
+
+    cam_to_world: np.ndarray
+    width: int
+    height: int
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    image: Optional[np.ndarray] = None  # (H, W, 3) float32 in [0, 1]
+    setup: CameraSetup = field(init=False)
+
+    def __post_init__(self):
+        self.setup = prepare_cam(self.cam_to_world, self.width, self.height, self.fx, self.fy, self.cx, self.cy)
+
+
+class Dataset:
+    """In-memory training set: views (pose + intrinsics + image) and a point cloud."""
+
+    def __init__(self, views: List[View], points: np.ndarray, colors: np.ndarray):
+        self.views = views
+        self.points = np.ascontiguousarray(points, np.float32)
+        self.colors = np.ascontiguousarray(colors, np.uint8)
+
+    @classmethod
+    def from_setups(cls, setups: List[CameraSetup], images, points, colors, poses) -> "Dataset":
+        views = [View(p, s.width, s.height, s.fx, s.fy, s.cx, s.cy, img) for s, p, img in zip(setups, poses, images)]
+        return cls(views, points, colors)
+
+
+class GaussianTrainer:
+    """3D Gaussian Splatting trainer on the B200 backend (reference: GaussianTrainer,
+    python/bindings.cpp:217-427)."""
+
+    def __init__(self, dataset: Dataset, config: TrainingConfig, init: Optional[GaussianParams] = None,
+                 context: Optional[Context] = None, device: str = "cuda"):
+        self.cfg = config
+        self.ds = dataset
+        self.ctx = context or Context()
+        self.device = device
+        if init is None:
+            pts = torch.from_numpy(dataset.points).to(device)
+            init = self.ctx.init_gaussians(pts, torch.from_numpy(dataset.colors), seed=42,
+                                           opacity_logit=math.log(0.1 / 0.9), sh_degree=config.sh_degree)
+        self.lrs = list(config.lrs) if config.lrs is not None else list(LR_INIT)
+        self._setup_buffers(init)
+        self.current_step = 0
+        self.adam_step = 0
+        self.bg = np.asarray(config.bg_color, np.float32)
+        self._targets = [torch.from_numpy(np.ascontiguousarray(v.image, np.float32)).to(device)
+                         if v.image is not None else None for v in dataset.views]
+        self._order: List[int] = []
+        self._rng = np.random.default_rng(config.seed)
+        self.stats = None
+        self.last_loss = None
+        self.radii_ready = False
+        self.max_dim = max(max(v.width, v.height) for v in dataset.views) if dataset.views else 1
+
+    # -- capacity buffers (model.cpp:81-193) ------------------------------------------
+    def _setup_buffers(self, p: GaussianParams):
+        n = p.n
+        self.cap = max(4 * n, 4)
+        self.num_active = n
+        self.buf = []
+        for t in p.tensors():
+            shape = (self.cap,) + tuple(t.shape[1:])
+            b = torch.zeros(shape, dtype=torch.float32, device=self.device)
+            b[:n] = t
+            self.buf.append(b)
+        self.m1 = [torch.zeros_like(b) for b in self.buf]
+        self.m2 = [torch.zeros_like(b) for b in self.buf]
+
+    def ensure_capacity(self, needed: int) -> None:
+        if needed <= self.cap:
+            return
+        new_cap = max(needed, 2 * self.cap)
+        n = self.num_active
+
+        def grow(b):
+            nb = torch.zeros((new_cap,) + tuple(b.shape[1:]), dtype=b.dtype, device=b.device)
+            nb[:n] = b[:n]
+            return nb
+
+        self.buf = [grow(b) for b in self.buf]
+        self.m1 = [grow(b) for b in self.m1]
+        self.m2 = [grow(b) for b in self.m2]
+        self.cap = new_cap
+
+    @property
+    def params(self) -> GaussianParams:
+        n = self.num_active
+        return GaussianParams(*[b[:n] for b in self.buf])
+
+    def _adam_view(self) -> AdamState:
+        n = self.num_active
+        st = AdamState([b[:n] for b in self.m1], [b[:n] for b in self.m2], self.lrs)
+        st.step = self.adam_step
+        return st
+
+    # -- schedule -------------------------------------------------------------------
+    def _next_camera(self) -> int:
+        if not self._order:
+            self._order = list(self._rng.permutation(len(self.ds.views)))
+        return int(self._order.pop())
+
+    def degrees_to_use(self, step: Optional[int] = None) -> int:
+        s = self.current_step if step is None else step
+        return min(s // max(self.cfg.sh_degree_interval, 1), self.cfg.sh_degree)
+
+    def _schedulers_step(self, step: int) -> None:
+        """Log-linear means LR decay (model.cpp:140-143)."""
+        t = min(max(step / max(self.cfg.iterations, 1), 0.0), 1.0)
+        self.lrs[0] = float(np.float32(math.exp(math.log(LR_INIT[0]) * (1 - t) + math.log(MEANS_LR_FINAL) * t)))
+
+    def _after_train(self, step: int) -> None:
+        """Model::afterTrain (model.cpp:199-245)."""
+        c = self.cfg
+        if not (step % c.refine_every == 0 and step > c.warmup_length):
+            return
+        reset_interval = c.reset_alpha_every * c.refine_every
+        stop_split_at = c.iterations // 2
+        do_dens = step < stop_split_at and step % reset_interval > len(self.ds.views) + c.refine_every
+        if do_dens and self.stats is not None:
+            self.ensure_capacity(3 * self.num_active)
+            gn, vc, ms = self.stats[1], self.stats[0], self.stats[2]
+            self.num_active = self.ctx.densify(
+                self.num_active, self.buf, self.m1, self.m2, gn, vc, ms, 0.5 * self.max_dim,
+                (step * 2654435761) & 0xFFFFFFFF, grad_thresh=c.densify_grad_thresh,
+                size_thresh=c.densify_size_thresh, screen_thresh=c.split_screen_size,
+                check_screen=step < c.stop_screen_size_at, cull_alpha=c.cull_alpha_thresh,
+                cull_scale=c.cull_scale_thresh, cull_screen=c.cull_screen_size,
+                check_huge=step > c.refine_every * c.reset_alpha_every)
+        if step < stop_split_at and step % reset_interval == c.refine_every:
+            n = self.num_active
+            self.ctx.opacity_reset(self.buf[5][:n], self.m1[5][:n], self.m2[5][:n], n, RESET_LOGIT)
+        self.stats = None
+
+    # -- public API -----------------------------------------------------------------
+    def step(self, sync_loss: bool = False, target: Optional[torch.Tensor] = None) -> TrainingStats:
+        """One training iteration (GaussianTrainer::step, python/bindings.cpp:261-284)."""
+        t0 = time.perf_counter()
+        ci = self._next_camera()
+        view = self.ds.views[ci]
+        gt = target if target is not None else self._targets[ci]
+        if gt is None:
+            raise ValueError(f"view {ci} has no target image")
+        n = self.num_active
+        if self.stats is None:
+            self.stats = tuple(torch.zeros(n, dtype=torch.float32, device=self.device) for _ in range(3))
+        adam = self._adam_view()
+        self.last_loss = self.ctx.train_step(self.params, adam, view.setup, self.bg, gt, self.stats,
+                                             ssim_weight=self.cfg.ssim_weight,
+                                             degrees_to_use=self.degrees_to_use(), sync_loss=sync_loss)
+        self.adam_step = adam.step
+        self.current_step += 1
+        self._schedulers_step(self.current_step)
+        self._after_train(self.current_step)
+        return TrainingStats(self.current_step, self.num_active, (time.perf_counter() - t0) * 1e3)
+
+    def train(self, callback: Optional[Callable[[TrainingStats], None]] = None, callback_every: int = 100) -> None:
+        while self.current_step < self.cfg.iterations:
+            st = self.step()
+            if callback is not None and st.iteration % callback_every == 0:
+                callback(st)
+
+    def render_tensor(self, setup: CameraSetup) -> torch.Tensor:
+        return self.ctx.render(self.params, setup, self.bg, degrees_to_use=self.degrees_to_use())
+
+    def render(self, cam_idx: int) -> np.ndarray:
+        """(H, W, 3) float32 render of a training camera."""
+        return self.render_tensor(self.ds.views[cam_idx].setup).cpu().numpy()
+
+    def render_from_pose(self, cam_to_world: np.ndarray, ref_cam_idx: int = 0) -> np.ndarray:
+        """Render an OpenGL camera-to-world pose with a training camera's intrinsics."""
+        v = self.ds.views[ref_cam_idx]
+        setup = prepare_cam(np.asarray(cam_to_world, np.float32), v.width, v.height, v.fx, v.fy, v.cx, v.cy)
+        return self.render_tensor(setup).cpu().numpy()
+
+    def render_rgba8(self, cam_idx: int) -> np.ndarray:
+        img = self.render_tensor(self.ds.views[cam_idx].setup)
+        rgb = (img.clamp(0.0, 1.0) * 255.0).to(torch.uint8)
+        alpha = torch.full(rgb.shape[:-1] + (1,), 255, dtype=torch.uint8, device=rgb.device)
+        return torch.cat([rgb, alpha], dim=-1).cpu().numpy()
+
+    @property
+    def splat_count(self) -> int:
+        return self.num_active
+
+    @property
+    def iteration(self) -> int:
+        return self.current_step

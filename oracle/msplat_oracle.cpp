@@ -599,6 +599,11 @@ double ssim_loss(const float *r, const float *gt, uint32_t W, uint32_t H, float 
 
 constexpr int GS = 10;  // per-intersection slot: xy(2) conic(3) rgb(3) opacity depth
 
+// Test-only switch: visit a tile's pixels (and a Gaussian's slots) in reverse order
+// in the backward pass. The result is the same sum in another float rounding order,
+// which measures how far summation order alone moves the reference's gradients.
+bool g_reverse_sums = false;
+
 // core/cpu/msplat_cpu.cpp:959-1031 (non-aux) -- back to front, T recovered by
 // division; per-intersection slots accumulated over the tile's pixels
 void raster_bwd(State &f, const float *bg, const float *v_img) {
@@ -612,8 +617,11 @@ void raster_bwd(State &f, const float *bg, const float *v_img) {
         if (e == s) continue;
         float *lv = f.isect_grad.data() + (size_t)s * GS;
         const int tx = t % f.tx, ty = t / f.tx;
-        for (int i = ty * TILE; i < std::min(H, (ty + 1) * TILE); i++)
-            for (int j = tx * TILE; j < std::min(W, (tx + 1) * TILE); j++) {
+        const int i0 = ty * TILE, i1 = std::min(H, (ty + 1) * TILE), j0 = tx * TILE, j1 = std::min(W, (tx + 1) * TILE);
+        const int npx = (i1 - i0) * (j1 - j0);
+        for (int pi = 0; pi < npx; pi++) {
+                const int q = g_reverse_sums ? npx - 1 - pi : pi;
+                const int i = i0 + q / (j1 - j0), j = j0 + q % (j1 - j0);
                 const size_t pid = (size_t)i * W + j;
                 const float px = (float)j, py = (float)i;
                 const float Tf = f.final_Ts[pid];
@@ -677,7 +685,8 @@ void reduce_slots(State &f, int N) {
 #pragma omp parallel for schedule(static)
     for (int gi = 0; gi < N; gi++) {
         float s[GS] = {0};
-        for (int32_t q = off[gi]; q < off[gi + 1]; q++) {
+        for (int32_t qq = off[gi]; qq < off[gi + 1]; qq++) {
+            const int32_t q = g_reverse_sums ? off[gi + 1] - 1 - (qq - off[gi]) : qq;
             const float *v = f.isect_grad.data() + (size_t)lst[q] * GS;
             for (int c = 0; c < GS; c++) s[c] += v[c];
         }
@@ -815,6 +824,15 @@ struct Kd {
 }  // namespace
 
 extern "C" {
+
+// "reverse_sums": see g_reverse_sums. Returns 0, or -1 for an unknown option.
+int orc_set_option(const char *name, int value) {
+    if (std::string(name) == "reverse_sums") {
+        g_reverse_sums = value != 0;
+        return 0;
+    }
+    return -1;
+}
 
 int orc_render(int n, const float *means, const float *scales, float gsc, const float *quats, const float *vm,
                const float *P, float fx, float fy, float cx, float cy, unsigned H, unsigned W, int tx, int ty,

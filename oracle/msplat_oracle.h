@@ -23,6 +23,11 @@
 extern "C" {
 #endif
 
+/* Restatement only (the reference build does not export it): "reverse_sums" = 1 makes
+ * the backward visit pixels and intersection slots in reverse order, i.e. the same
+ * gradient sums in another float rounding order. Returns 0, or -1 if unknown. */
+int orc_set_option(const char *name, int value);
+
 /* core/metal/bindings.h:81-91 (msplat_render); writes the (H,W,3) image. */
 int orc_render(int num_points, const float *means, const float *scales, float glob_scale,
                const float *quats, const float *viewmat, const float *projmat,

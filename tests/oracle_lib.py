@@ -189,12 +189,19 @@ class Oracle:
 
 def new_adam_state(g, lrs, step: int, beta1=0.9, beta2=0.999, eps=1e-8):
     """Moments and the step sizes Model::fullIteration derives (core/src/model.cpp:638-651)."""
-    bc1 = 1.0 - np.float32(beta1) ** step
-    bc2 = 1.0 - np.float32(beta2) ** step
+    bc1 = np.float32(1.0 - float(np.float32(beta1)) ** int(step))
+    bc2 = np.float32(1.0 - float(np.float32(beta2)) ** int(step))
     return {
         "m1": [np.zeros_like(a) for a in g.arrays()],
         "m2": [np.zeros_like(a) for a in g.arrays()],
-        "step_sizes": [np.float32(lr) / np.float32(bc1) for lr in lrs],
-        "bc2": [np.float32(np.sqrt(np.float32(bc2)))] * 6,
+        "step_sizes": [np.float32(lr) / bc1 for lr in lrs],
+        "bc2": [np.float32(np.sqrt(bc2))] * 6,
         "beta1": beta1, "beta2": beta2, "eps": eps,
     }
+
+
+def set_option(oracle: "Oracle", name: str, value: int) -> None:
+    """Restatement-only switches (see orc_set_option in oracle/msplat_oracle.h)."""
+    fn = getattr(oracle.lib, "orc_set_option", None)
+    if fn is None or fn(name.encode(), C.c_int(value)) != 0:
+        raise KeyError(f"{oracle.kind} oracle has no option {name}")
