@@ -261,19 +261,19 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
         s_vis[threadIdx.x] = vis ? 1 : 0;
     }
     __syncwarp();
-    const int wbase_t = threadIdx.x - lane;               // first thread of this warp
+    const int wbase_t = threadIdx.x - lane;                          // first thread of this warp
     const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;  // its Gaussian
     const int stride = a.rest_stride;
-    const int total = 32 * stride;
-    float *rest = a.p[4] + g0 * stride, *r1 = a.m1[4] + g0 * stride, *r2 = a.m2[4] + g0 * stride;
-    for (int e = lane; e < total; e += 32) {
-        const int gl = e / stride;
+    const int used = 3 * active;  // floats of each row that get a gradient
+    for (int gl = 0; gl < 32; gl++) {  // one Gaussian's row at a time (warp-uniform)
         if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
-        const int j = e - gl * stride;
-        const int base = j / 3, c = j - base * 3;
-        if (base >= active) continue;
-        const float g = s_basis[wbase_t + gl][base] * s_vrgb[wbase_t + gl][c];
-        adam_step(rest[e], r1[e], r2[e], g, a.ss[4], b1, b2, a.bc2[4], eps);
+        const size_t off = (size_t)(g0 + gl) * stride;
+        float *rest = a.p[4] + off, *r1 = a.m1[4] + off, *r2 = a.m2[4] + off;
+        const float *bs = s_basis[wbase_t + gl], *vc = s_vrgb[wbase_t + gl];
+        for (int j = lane; j < used; j += 32) {
+            const int base = j / 3, c = j - base * 3;
+            adam_step(rest[j], r1[j], r2[j], bs[base] * vc[c], a.ss[4], b1, b2, a.bc2[4], eps);
+        }
     }
 }
 

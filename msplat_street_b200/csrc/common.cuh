@@ -131,12 +131,22 @@ __device__ __forceinline__ void cov3d_of(V3 s, float g, Q4 q, float *cov) {
 }
 
 // One splat record per Gaussian, read by the rasterizer: centre, conic, sigmoid
-// opacity and raw SH colour, 48 bytes so it loads as three float4.
+// opacity, raw SH colour and the half-extents of the box outside which it cannot be
+// composited (alpha < 1/255), 48 bytes so it loads as three float4.
 struct __align__(16) Splat {
     float x, y, cx, cy;   // pixel centre, conic (a, b)
     float cz, op, r, g;   // conic c, sigmoid(opacity), raw colour r g
-    float b, depth, pad0, pad1;
+    float b, depth, ex, ey;
 };
+
+// Pixels of a 16x16 tile owned by one warp: an 8x4 block (warp w covers columns
+// 8 * (w % 2) .. +7 and rows 4 * (w / 2) .. +3), compact so that per-warp culling
+// against a Gaussian's box skips as much as possible.
+__device__ __forceinline__ void tile_pixel(int t, int &lx, int &ly) {
+    const int w = t >> 5, l = t & 31;
+    lx = ((w & 1) << 3) + (l & 7);
+    ly = ((w >> 1) << 2) + (l >> 3);
+}
 
 // Counter-based RNG: PCG hash + Box-Muller (core/cpu/msplat_cpu.cpp:304-323)
 __host__ __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {

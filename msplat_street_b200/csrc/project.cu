@@ -126,10 +126,27 @@ __global__ void project_kernel(ProjectArgs a) {
     }
     // sigmoid opacity as the pack step computes it (core/cpu/msplat_cpu.cpp:560)
     const float op = 1.f / (1.f + exp_ref(-a.opacities[i]));
+    // Half-extents of the region a pixel can be composited in: sigma < 5.55 and
+    // op * exp(-sigma) >= 1/255, i.e. 0.5 d^T conic d <= L. Its bounding box has
+    // half-widths sqrt(2 L conic_c / det) and sqrt(2 L conic_a / det), evaluated in
+    // double with margins, so the rasterizers may skip pixel blocks outside it without
+    // changing any result. An empty box marks a Gaussian that never reaches 1/255.
+    float ex = -1e30f, ey = -1e30f;
+    const double L = fmin(5.55, log(255.0 * (double)op) + 1e-4);
+    if (L > 0.0) {
+        const double ca = conic.x, cb = conic.y, cc = conic.z;
+        const double cdet = ca * cc - cb * cb;
+        if (cdet > 0.0 && ca > 0.0 && cc > 0.0) {
+            ex = (float)(sqrt(2.0 * L * cc / cdet) * 1.001 + 0.5);
+            ey = (float)(sqrt(2.0 * L * ca / cdet) * 1.001 + 0.5);
+        } else {
+            ex = ey = 1e30f;  // not positive definite: never skip
+        }
+    }
     float4 *rec = reinterpret_cast<float4 *>(a.splats + i);
     rec[0] = make_float4(ctx, cty, conic.x, conic.y);
     rec[1] = make_float4(conic.z, op, col[0], col[1]);
-    rec[2] = make_float4(col[2], pv.z, 0.f, 0.f);
+    rec[2] = make_float4(col[2], pv.z, ex, ey);
 }
 
 void launch_project(const ProjectArgs &a, cudaStream_t st) {

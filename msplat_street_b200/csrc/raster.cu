@@ -13,9 +13,10 @@
 // by multiplying with 1/(1 - alpha), colour gradients gated on raw + 0.5 >= 0 and the
 // sigma gradients only for alpha < 0.999. Each (tile, Gaussian) pair -- one sorted
 // intersection -- gets one 9-float slot: xy(2) conic(3) rgb(3) opacity-logit(1),
-// reduced over the tile's pixels with warp shuffles and a fixed-order sum over warps,
-// so results do not depend on scheduling (the reference is deterministic too,
-// :952-956). The per-Gaussian sums happen in the fused backward/Adam kernel.
+// reduced over the tile's pixels in a fixed order (lanes through a transposed
+// shared-memory buffer, then warps), so results do not depend on scheduling (the
+// reference is deterministic too, :952-956). The per-Gaussian sums happen in the
+// fused backward/Adam kernel.
 //
 // Compiled with -fmad=false: the alpha and transmittance cut-offs must fall exactly
 // where the reference's do.
@@ -32,10 +33,16 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
     const int tile = blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    const int px = tx * TILE + (threadIdx.x % TILE), py = ty * TILE + (threadIdx.x / TILE);
+    int lx, ly;
+    tile_pixel(threadIdx.x, lx, ly);
+    const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
     const int start = a.tile_start[tile], end = a.tile_end[tile];
     const float fpx = (float)px, fpy = (float)py;
+    // this warp's 8x4 pixel block, for skipping Gaussians whose box misses it
+    const int w = threadIdx.x >> 5;
+    const float bx0 = (float)(tx * TILE + ((w & 1) << 3)), bx1 = bx0 + 7.f;
+    const float by0 = (float)(ty * TILE + ((w >> 1) << 2)), by1 = by0 + 3.f;
     float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f;
     int last = start - 1;
     bool done = !inside;
@@ -51,7 +58,9 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
         __syncthreads();
         const int cnt = min(FWD_BATCH, end - b0);
         for (int j = 0; j < cnt && !done; j++) {
-            const float4 A = s0[j], B = s1[j];
+            const float4 A = s0[j], C = s2[j];
+            if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
+            const float4 B = s1[j];
             const float dx = A.x - fpx, dy = A.y - fpy;
             const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
             if (sigma < 0.f || sigma >= 5.55f) continue;
@@ -66,7 +75,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
             const float vis = alpha * T;
             cr = fmaxf(B.z + 0.5f, 0.f) * vis + cr;
             cg = fmaxf(B.w + 0.5f, 0.f) * vis + cg;
-            cb = fmaxf(s2[j].x + 0.5f, 0.f) * vis + cb;
+            cb = fmaxf(C.x + 0.5f, 0.f) * vis + cb;
             T = nT;
             last = b0 + j;
         }
@@ -81,23 +90,36 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
     o[2] = clamp01(a.bg[2] * T + cb);
 }
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+// Per-warp reduction of the 9 gradient values over the warp's 32 pixels, done in
+// sub-batches of 8 Gaussians: each lane stores its contributions to a transposed
+// buffer (one row of 32 lane values per output), then each lane sums whole rows with
+// float4 loads. 72 outputs x 31 adds per sub-batch, in a fixed lane order.
+constexpr int SUB = 8;
+constexpr int SUB_OUT = SUB * 9;  // outputs per sub-batch
+constexpr int PB_STRIDE = 36;     // floats per row: 32 lanes + pad, keeps float4 rows conflict-free
+
+size_t raster_bwd_smem() {
+    return sizeof(float4) * 3 * BWD_BATCH + sizeof(float) * BWD_WARPS * BWD_BATCH * 9 +
+           sizeof(float) * BWD_WARPS * SUB_OUT * PB_STRIDE + 16;
 }
 
-__global__ void __launch_bounds__(TILE_PIX) raster_bwd_kernel(RasterBwdArgs a) {
-    __shared__ float4 s0[BWD_BATCH], s1[BWD_BATCH], s2[BWD_BATCH];
-    __shared__ float red[BWD_WARPS][BWD_BATCH][9];
+__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a) {
+    extern __shared__ __align__(16) float4 smem4[];
+    float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
+    float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][9]
+    float *pbuf = red + BWD_WARPS * BWD_BATCH * 9;            // [BWD_WARPS][SUB_OUT][PB_STRIDE]
     __shared__ int kmax;
     const int tile = blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    const int px = tx * TILE + (threadIdx.x % TILE), py = ty * TILE + (threadIdx.x / TILE);
+    int lx, ly;
+    tile_pixel(threadIdx.x, lx, ly);
+    const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
     const int start = a.tile_start[tile], end = a.tile_end[tile];
     if (end <= start) return;  // block-uniform
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float bx0 = (float)(tx * TILE + ((warp & 1) << 3)), bx1 = bx0 + 7.f;
+    const float by0 = (float)(ty * TILE + ((warp >> 1) << 2)), by1 = by0 + 3.f;
     const int pid = py * a.W + px;
     float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f;
     int kf = start - 1;
@@ -119,6 +141,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_bwd_kernel(RasterBwdArgs a) {
     const float tbr = Tf * a.bg[0], tbg = Tf * a.bg[1], tbb = Tf * a.bg[2];
     float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
     const float fpx = (float)px, fpy = (float)py;
+    float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
     for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
         const int b_start = max(start, b_end - BWD_BATCH);
         const int cnt = b_end - b_start;
@@ -129,62 +152,86 @@ __global__ void __launch_bounds__(TILE_PIX) raster_bwd_kernel(RasterBwdArgs a) {
             s2[threadIdx.x] = rec[2];
         }
         __syncthreads();
-        for (int j = cnt - 1; j >= 0; j--) {
-            const int k = b_start + j;
-            float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            bool hit = false;
-            if (inside && k <= kf) {
-                const float4 A = s0[j], B = s1[j];
-                const float dx = A.x - fpx, dy = A.y - fpy;
-                const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
-                if (sigma >= 0.f && sigma < 5.55f) {
-                    const float op = B.y;
-                    const float alpha = fminf(0.999f, op * exp_ref(-sigma));
-                    if (alpha >= 1.f / 255.f) {
-                        hit = true;
-                        const float ra = 1.f / (1.f - alpha);
-                        T *= ra;
-                        const float fac = alpha * T;
-                        const float rawr = B.z, rawg = B.w, rawb = s2[j].x;
-                        const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),
-                                    cb = fmaxf(rawb + 0.5f, 0.f);
-                        const float nra = -ra;
-                        const float ir = -br * ra + nra * tbr, ig = -bgc * ra + nra * tbg, ib = -bb * ra + nra * tbb;
-                        const float orr = cr * T + ir, og = cg * T + ig, ob = cb * T + ib;
-                        const float va = orr * vr + og * vg + ob * vb;
-                        br = cr * fac + br;
-                        bgc = cg * fac + bgc;
-                        bb = cb * fac + bb;
-                        if (rawr + 0.5f >= 0.f) g[5] = fac * vr;
-                        if (rawg + 0.5f >= 0.f) g[6] = fac * vg;
-                        if (rawb + 0.5f >= 0.f) g[7] = fac * vb;
-                        if (alpha < 0.999f) {
-                            const float vs = -alpha * va;
-                            g[2] = 0.5f * vs * dx * dx;
-                            g[3] = 0.5f * vs * dx * dy;
-                            g[4] = 0.5f * vs * dy * dy;
-                            g[0] = vs * (A.z * dx + A.w * dy);
-                            g[1] = vs * (A.w * dx + B.x * dy);
-                            g[8] = -vs * (1.f - op);
+        for (int sb = (cnt - 1) / SUB; sb >= 0; sb--) {
+            const int jlo = sb * SUB, jhi = min(cnt - 1, jlo + SUB - 1);
+            unsigned any = 0u;  // bit jj: some lane of this warp touched Gaussian jlo + jj
+            for (int j = jhi; j >= jlo; j--) {
+                const int k = b_start + j;
+                const float4 A = s0[j], C = s2[j];
+                if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
+                float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                bool hit = false;
+                if (inside && k <= kf) {
+                    const float4 B = s1[j];
+                    const float dx = A.x - fpx, dy = A.y - fpy;
+                    const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
+                    if (sigma >= 0.f && sigma < 5.55f) {
+                        const float op = B.y;
+                        const float alpha = fminf(0.999f, op * exp_ref(-sigma));
+                        if (alpha >= 1.f / 255.f) {
+                            hit = true;
+                            const float ra = __frcp_rn(1.f - alpha);  // == 1.f / (1.f - alpha), IEEE
+                            T *= ra;
+                            const float fac = alpha * T;
+                            const float rawr = B.z, rawg = B.w, rawb = C.x;
+                            const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),
+                                        cb = fmaxf(rawb + 0.5f, 0.f);
+                            const float nra = -ra;
+                            const float ir = -br * ra + nra * tbr, ig = -bgc * ra + nra * tbg, ib = -bb * ra + nra * tbb;
+                            const float orr = cr * T + ir, og = cg * T + ig, ob = cb * T + ib;
+                            const float va = orr * vr + og * vg + ob * vb;
+                            br = cr * fac + br;
+                            bgc = cg * fac + bgc;
+                            bb = cb * fac + bb;
+                            if (rawr + 0.5f >= 0.f) g[5] = fac * vr;
+                            if (rawg + 0.5f >= 0.f) g[6] = fac * vg;
+                            if (rawb + 0.5f >= 0.f) g[7] = fac * vb;
+                            if (alpha < 0.999f) {
+                                const float vs = -alpha * va;
+                                g[2] = 0.5f * vs * dx * dx;
+                                g[3] = 0.5f * vs * dx * dy;
+                                g[4] = 0.5f * vs * dy * dy;
+                                g[0] = vs * (A.z * dx + A.w * dy);
+                                g[1] = vs * (A.w * dx + B.x * dy);
+                                g[8] = -vs * (1.f - op);
+                            }
                         }
                     }
                 }
+                if (__ballot_sync(0xffffffffu, hit)) {
+                    any |= 1u << (j - jlo);
+                    float *row = mypb + (j - jlo) * 9 * PB_STRIDE + lane;
+    #pragma unroll
+                    for (int c = 0; c < 9; c++) row[c * PB_STRIDE] = g[c];
+                }
             }
-            if (__any_sync(0xffffffffu, hit)) {
+            __syncwarp();
+            // this warp's sums for the sub-batch: output o = jj * 9 + c
+            for (int o = lane; o < SUB_OUT; o += 32) {
+                const int jj = o / 9, c = o - jj * 9;
+                if (jlo + jj > jhi) continue;
+                float s = 0.f;
+                if ((any >> jj) & 1u) {
+                    const float4 *row = reinterpret_cast<const float4 *>(mypb + o * PB_STRIDE);
 #pragma unroll
-                for (int c = 0; c < 9; c++) g[c] = warp_sum(g[c]);
+                    for (int q = 0; q < 8; q++) {
+                        const float4 v = row[q];
+                        s += v.x;
+                        s += v.y;
+                        s += v.z;
+                        s += v.w;
+                    }
+                }
+                red[(warp * BWD_BATCH + jlo + jj) * 9 + c] = s;
             }
-            if (lane == 0) {
-#pragma unroll
-                for (int c = 0; c < 9; c++) red[warp][j][c] = g[c];
-            }
+            __syncwarp();
         }
         __syncthreads();
         for (int idx = threadIdx.x; idx < cnt * 9; idx += blockDim.x) {
             const int j = idx / 9, c = idx - j * 9;
             float s = 0.f;
 #pragma unroll
-            for (int w = 0; w < BWD_WARPS; w++) s += red[w][j][c];
+            for (int w = 0; w < BWD_WARPS; w++) s += red[(w * BWD_BATCH + j) * 9 + c];
             a.slots[(size_t)(b_start + j) * 9 + c] = s;
         }
         __syncthreads();
@@ -204,7 +251,13 @@ void launch_raster_fwd(const RasterArgs &a, cudaStream_t st) {
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    raster_bwd_kernel<<<T, TILE_PIX, 0, st>>>(a);
+    static bool attr_set = false;
+    const size_t smem = raster_bwd_smem();
+    if (!attr_set) {
+        cudaFuncSetAttribute(raster_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    raster_bwd_kernel<<<T, TILE_PIX, smem, st>>>(a);
 }
 
 }  // namespace msplat
