@@ -127,16 +127,32 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     const bool vis = valid && a.radii[i] > 0;
     const float b1 = a.beta1, b2 = a.beta2, eps = a.eps;
 
-    // 1. per-Gaussian sums of the intersection slots, in sorted order
+    // 1. per-Gaussian sums of the intersection slots. A Gaussian may cover hundreds of
+    // tiles, so the warp sums each of its visible Gaussians together: lane l takes the
+    // intersections l, l+32, ... and a fixed butterfly combines the lanes.
     float s9[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (vis) {
-        const int64_t e0 = a.offsets[i];
-        const int cnt = a.n_tiles[i];
-        for (int j = 0; j < cnt; j++) {
-            const float *sl = a.slots + (size_t)a.inv[e0 + j] * 9;
+    {
+        const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
+        const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + (threadIdx.x - lane);
+        for (int gl = 0; gl < 32; gl++) {
+            if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
+            const int64_t e0 = a.offsets[g0 + gl];
+            const int cnt = a.n_tiles[g0 + gl];
+            float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int j = lane; j < cnt; j += 32) {
+                const float *sl = a.slots + (size_t)a.inv[e0 + j] * 9;
 #pragma unroll
-            for (int c = 0; c < 9; c++) s9[c] += sl[c];
+                for (int c = 0; c < 9; c++) p[c] += sl[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) p[c] += __shfl_xor_sync(0xffffffffu, p[c], o);
+                if (lane == gl) s9[c] = p[c];
+            }
         }
+    }
+    if (vis) {
         if (a.v_xy) {
             a.v_xy[2 * i] = s9[0];
             a.v_xy[2 * i + 1] = s9[1];

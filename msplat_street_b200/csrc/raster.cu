@@ -167,7 +167,13 @@ __global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a
                     const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
                     if (sigma >= 0.f && sigma < 5.55f) {
                         const float op = B.y;
-                        const float alpha = fminf(0.999f, op * exp_ref(-sigma));
+                        // The fast exponential is within 8 ulps here; near the 1/255 and
+                        // 0.999 cut-offs alpha is recomputed exactly, so every decision
+                        // equals the forward pass's.
+                        const float va_fast = op * __expf(-sigma);
+                        float alpha = fminf(0.999f, va_fast);
+                        if (fabsf(va_fast - 1.f / 255.f) <= 1e-5f * (1.f / 255.f) || fabsf(va_fast - 0.999f) <= 1e-5f)
+                            alpha = fminf(0.999f, op * exp_ref(-sigma));
                         if (alpha >= 1.f / 255.f) {
                             hit = true;
                             const float ra = __frcp_rn(1.f - alpha);  // == 1.f / (1.f - alpha), IEEE
