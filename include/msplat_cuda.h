@@ -118,6 +118,24 @@ int msplat_cuda_opacity_reset(msplat_cuda_ctx *ctx, float *opacities, float *exp
  * bits of the keys, in place (device pointers). */
 int msplat_cuda_radix_sort(msplat_cuda_ctx *ctx, uint64_t *keys, int32_t *vals, uint32_t n, int key_bits);
 
+/* No counterpart in the reference. The same stable radix sort as
+ * msplat_cuda_radix_sort for callers that may not allocate GPU memory when they sort:
+ * a serving process whose HBM is fully committed to resident scenes, a render loop
+ * that cannot take the device-wide synchronisation of cudaMalloc / cudaFree, a plugin
+ * host that forbids libraries to allocate. It allocates nothing and takes no context:
+ * its scratch is one fixed array in device memory (MSPLAT_STATIC_SORT_BYTES, held on
+ * every GPU that loads the library until the process exits), so n is limited to
+ * MSPLAT_STATIC_SORT_MAX_KEYS (larger n returns MSPLAT_CUDA_ECAPACITY with a message
+ * in msplat_cuda_last_error). The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture begins. All calls share the one array, so calls
+ * whose work overlaps on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. Work is enqueued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream). */
+#define MSPLAT_STATIC_SORT_MAX_KEYS (1u << 20)
+#define MSPLAT_STATIC_SORT_BYTES (13u * 1024u * 1024u + 4096u)
+int msplat_cuda_radix_sort_static(void *stream, uint64_t *keys, int32_t *vals, uint32_t n, int key_bits);
+
 /* bindings.h:151 msplat_knn3_mean_dist -- exact mean distance from each of n points
  * (n, 3) to its 3 nearest other points. */
 int msplat_cuda_knn3_mean_dist(msplat_cuda_ctx *ctx, const float *points, uint32_t n, float *mean_dist);

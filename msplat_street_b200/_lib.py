@@ -52,6 +52,7 @@ _SIGS = {
                                   vp, C.c_uint32, C.POINTER(i32)]),
     "msplat_cuda_opacity_reset": (i32, [vp, vp, vp, vp, i32, f32]),
     "msplat_cuda_radix_sort": (i32, [vp, vp, vp, C.c_uint32, i32]),
+    "msplat_cuda_radix_sort_static": (i32, [vp, vp, vp, C.c_uint32, i32]),
     "msplat_cuda_knn3_mean_dist": (i32, [vp, vp, C.c_uint32, vp]),
     "msplat_cuda_init_gaussians": (i32, [vp, vp, vp, C.c_uint32, C.c_uint32, f32, vp, vp, vp, vp]),
     "msplat_cuda_loss_device": (i32, [vp, PP]),

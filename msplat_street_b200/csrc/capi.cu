@@ -34,6 +34,13 @@ int fail(int code, const char *fmt, ...) {
     return code;
 }
 
+}  // namespace
+
+// Lets other translation units report through msplat_cuda_last_error().
+int msplat::report_error(int code, const char *msg) { return fail(code, "%s", msg); }
+
+namespace {
+
 #define CUDA_TRY(expr)                                                                          \
     do {                                                                                        \
         cudaError_t _e = (expr);                                                                \

@@ -8,6 +8,9 @@
 
 namespace msplat {
 
+// Records a message for msplat_cuda_last_error() and returns code (capi.cu).
+int report_error(int code, const char *msg);
+
 // One view: the scalars msplat_render / msplat_train_step take about the camera.
 struct CamParams {
     float viewmat[16];  // row-major world-to-camera
