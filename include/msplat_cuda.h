@@ -146,6 +146,27 @@ int msplat_cuda_init_gaussians(msplat_cuda_ctx *ctx, const float *means, const u
                                uint32_t seed, float opacity_logit, float *scales, float *quats, float *features_dc,
                                float *opacities);
 
+/* Gradient-only backward of the last msplat_cuda_render on this context (same scene
+ * and camera), for differentiable rendering (torch.autograd): given dL/d(image)
+ * (H,W,3, device), writes dL/d(means, log-scales, quats, features_dc, features_rest,
+ * opacity logits) to the six device arrays, zero for Gaussians the render did not
+ * use. Composes rasterize_backward, reduce_isect_grads and the projection / SH VJPs
+ * (core/cpu/msplat_cpu.cpp:959-1139) without the fused Adam. */
+int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const float *means3d, const float *scales,
+                                float glob_scale, const float *quats, const float *viewmat, const float *projmat,
+                                float fx, float fy, float cx, float cy, unsigned img_height, unsigned img_width,
+                                int tiles_x, int tiles_y, float clip_thresh, unsigned degree, unsigned degrees_to_use,
+                                const float *cam_pos, const float *background, const float *v_img, float *v_means,
+                                float *v_scales, float *v_quats, float *v_features_dc, float *v_features_rest,
+                                float *v_opacities);
+
+/* The training loss of msplat_train_step on its own (core/cpu/msplat_cpu.cpp:669-785):
+ * L1 + ssim_weight * (1 - SSIM), forward and backward in one pass. Writes
+ * loss_inv_n-scaled dL/d(img) to v_img and the loss (sum / (H*W)) to the device
+ * scalar *loss. All pointers are device pointers. */
+int msplat_cuda_ssim_loss(msplat_cuda_ctx *ctx, const float *img, const float *gt, unsigned img_height,
+                          unsigned img_width, float ssim_weight, float loss_inv_n, float *v_img, float *loss);
+
 /* Device pointer of the last train step's loss (float, sum / (H*W)). */
 int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
 

@@ -55,6 +55,9 @@ _SIGS = {
     "msplat_cuda_radix_sort_static": (i32, [vp, vp, vp, C.c_uint32, i32]),
     "msplat_cuda_knn3_mean_dist": (i32, [vp, vp, C.c_uint32, vp]),
     "msplat_cuda_init_gaussians": (i32, [vp, vp, vp, C.c_uint32, C.c_uint32, f32, vp, vp, vp, vp]),
+    "msplat_cuda_render_backward": (i32, [vp, i32, vp, vp, f32, vp, vp, vp, f32, f32, f32, f32, u32, u32, i32, i32,
+                                          f32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "msplat_cuda_ssim_loss": (i32, [vp, vp, vp, u32, u32, f32, f32, vp, vp]),
     "msplat_cuda_loss_device": (i32, [vp, PP]),
     "msplat_cuda_frame": (i32, [vp, C.c_char_p, PP, C.POINTER(i64)]),
     "msplat_cuda_num_isects": (i64, [vp]),

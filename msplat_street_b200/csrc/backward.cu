@@ -152,23 +152,22 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
             }
         }
     }
-    if (vis) {
+    if (valid) {  // s9 is zero for invisible Gaussians
         if (a.v_xy) {
             a.v_xy[2 * i] = s9[0];
             a.v_xy[2 * i + 1] = s9[1];
+        }
+        if (a.v_conic) {
             a.v_conic[3 * i] = s9[2];
             a.v_conic[3 * i + 1] = s9[3];
             a.v_conic[3 * i + 2] = s9[4];
+        }
+        if (a.v_rgb) {
             a.v_rgb[3 * i] = s9[5];
             a.v_rgb[3 * i + 1] = s9[6];
             a.v_rgb[3 * i + 2] = s9[7];
-            a.v_opacity[i] = s9[8];
         }
-    } else if (valid && a.v_xy) {
-        a.v_xy[2 * i] = a.v_xy[2 * i + 1] = 0.f;
-        a.v_conic[3 * i] = a.v_conic[3 * i + 1] = a.v_conic[3 * i + 2] = 0.f;
-        a.v_rgb[3 * i] = a.v_rgb[3 * i + 1] = a.v_rgb[3 * i + 2] = 0.f;
-        a.v_opacity[i] = 0.f;
+        if (a.v_opacity) a.v_opacity[i] = s9[8];
     }
 
     // 2. projection VJPs
@@ -247,11 +246,17 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
         a.max_2d_size[i] = fmaxf(a.max_2d_size[i], (float)a.radii[i] * a.inv_max_dim);
     }
 
-    // 5. SH rest Adam, warp-cooperative over the warp's 32 Gaussians
-    if (!a.do_adam || a.rest_stride <= 0) return;
+    // gradient-only mode (autograd): the SH colour gradients as arrays
+    if (valid && a.g_dc) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) a.g_dc[3 * (size_t)i + c] = vis ? SH_C0 * s9[5 + c] : 0.f;
+    }
+
+    // 5. SH rest Adam (or its gradient), warp-cooperative over the warp's 32 Gaussians
+    if ((!a.do_adam && !a.g_rest) || a.rest_stride <= 0) return;
     const uint32_t dtu = a.cam.degrees_to_use;
     const int active = dtu < 1 ? 0 : dtu < 2 ? 3 : dtu < 3 ? 8 : 15;  // bases updated
-    if (active == 0) return;
+    if (active == 0 && !a.g_rest) return;
     {
         float x = dir.x, y = dir.y, z = dir.z;
         float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
@@ -281,6 +286,19 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;  // its Gaussian
     const int stride = a.rest_stride;
     const int used = 3 * active;  // floats of each row that get a gradient
+    if (a.g_rest) {  // gradient-only mode: every row, zero where invisible or inactive
+        for (int gl = 0; gl < 32; gl++) {
+            if (g0 + gl >= a.n) break;
+            const bool gv = s_vis[wbase_t + gl] != 0;
+            float *gr = a.g_rest + (size_t)(g0 + gl) * stride;
+            const float *bs = s_basis[wbase_t + gl], *vc = s_vrgb[wbase_t + gl];
+            for (int j = lane; j < stride; j += 32) {
+                const int base = j / 3, c = j - base * 3;
+                gr[j] = (gv && j < used) ? bs[base] * vc[c] : 0.f;
+            }
+        }
+        return;
+    }
     for (int gl = 0; gl < 32; gl++) {  // one Gaussian's row at a time (warp-uniform)
         if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
         const size_t off = (size_t)(g0 + gl) * stride;

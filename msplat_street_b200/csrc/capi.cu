@@ -565,6 +565,99 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     return MSPLAT_CUDA_OK;
 }
 
+int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const float *means3d, const float *scales,
+                                float glob_scale, const float *quats, const float *viewmat, const float *projmat,
+                                float fx, float fy, float cx, float cy, unsigned img_height, unsigned img_width,
+                                int tiles_x, int tiles_y, float clip_thresh, unsigned degree, unsigned degrees_to_use,
+                                const float *cam_pos, const float *background, const float *v_img, float *v_means,
+                                float *v_scales, float *v_quats, float *v_features_dc, float *v_features_rest,
+                                float *v_opacities) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (int r = check_camera(num_points, img_height, img_width, tiles_x, tiles_y, degree, degrees_to_use, viewmat,
+                             projmat, cam_pos, background))
+        return r;
+    if (ctx->n != num_points || ctx->W != (int)img_width || ctx->H != (int)img_height || !ctx->final_T.ptr)
+        return fail(MSPLAT_CUDA_EINVAL, "render_backward must follow msplat_cuda_render of the same scene and camera "
+                                        "on this context");
+    if (!v_img) return fail(MSPLAT_CUDA_EINVAL, "null image gradient");
+    if (num_points > 0 && (!means3d || !scales || !quats || !v_means || !v_scales || !v_quats || !v_features_dc ||
+                           !v_opacities || (degree > 0 && !v_features_rest)))
+        return fail(MSPLAT_CUDA_EINVAL, "null parameter or gradient pointer");
+    cudaStream_t st = ctx->stream;
+    const int n = num_points;
+    ENSURE(ctx->slots, (size_t)ctx->n_isect * 9, float, slots);
+    CamParams cam = make_cam(viewmat, projmat, fx, fy, cx, cy, img_height, img_width, tiles_x, tiles_y, clip_thresh,
+                             degree, degrees_to_use, cam_pos);
+    RasterBwdArgs rb;
+    rb.W = (int)img_width;
+    rb.H = (int)img_height;
+    rb.tiles_x = tiles_x;
+    rb.tiles_y = tiles_y;
+    rb.tile_start = reinterpret_cast<const int32_t *>(ctx->tile_start.ptr);
+    rb.tile_end = reinterpret_cast<const int32_t *>(ctx->tile_end.ptr);
+    rb.isect_gid = reinterpret_cast<const int32_t *>(ctx->isect_gid.ptr);
+    rb.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
+    for (int c = 0; c < 3; c++) rb.bg[c] = background[c];
+    rb.final_T = reinterpret_cast<const float *>(ctx->final_T.ptr);
+    rb.final_idx = reinterpret_cast<const int32_t *>(ctx->final_idx.ptr);
+    rb.v_out = v_img;
+    rb.slots = slots;
+    launch_raster_bwd(rb, st);
+    BackwardArgs ba;
+    std::memset(&ba, 0, sizeof ba);
+    ba.n = n;
+    ba.means = means3d;
+    ba.scales = scales;
+    ba.quats = quats;
+    ba.glob_scale = glob_scale;
+    ba.cam = cam;
+    ba.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
+    ba.radii = reinterpret_cast<const int32_t *>(ctx->radii.ptr);
+    ba.n_tiles = reinterpret_cast<const int32_t *>(ctx->n_tiles.ptr);
+    ba.inv = reinterpret_cast<const int32_t *>(ctx->inv.ptr);
+    ba.offsets = reinterpret_cast<const int64_t *>(ctx->offsets.ptr);
+    ba.slots = slots;
+    ba.v_mean3d = v_means;
+    ba.v_scale = v_scales;
+    ba.v_quat = v_quats;
+    ba.v_opacity = v_opacities;
+    ba.g_dc = v_features_dc;
+    ba.g_rest = degree > 0 ? v_features_rest : nullptr;
+    ba.rest_stride = (int)(num_sh_bases(degree) - 1) * 3;
+    if (ctx->keep_grads) {  // screen-space gradients for msplat_cuda_frame
+        ENSURE(ctx->v_xy, 2 * (size_t)n, float, vxy);
+        ENSURE(ctx->v_conic, 3 * (size_t)n, float, vcon);
+        ENSURE(ctx->v_rgb, 3 * (size_t)n, float, vrgb);
+        ba.v_xy = vxy;
+        ba.v_conic = vcon;
+        ba.v_rgb = vrgb;
+    }
+    launch_backward_adam(ba, st);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_ssim_loss(msplat_cuda_ctx *ctx, const float *img, const float *gt, unsigned img_height,
+                          unsigned img_width, float ssim_weight, float loss_inv_n, float *v_img, float *loss) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (!img || !gt || !v_img || !loss) return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    if (img_width == 0 || img_height == 0) return fail(MSPLAT_CUDA_EINVAL, "image size must be positive");
+    ENSURE(ctx->loss_part, ssim_blocks((int)img_width, (int)img_height), double, loss_part);
+    SsimArgs sa;
+    sa.W = (int)img_width;
+    sa.H = (int)img_height;
+    sa.img = img;
+    sa.gt = gt;
+    sa.ssim_weight = ssim_weight;
+    sa.inv_n = loss_inv_n;
+    sa.v_out = v_img;
+    sa.partials = loss_part;
+    sa.loss = loss;
+    launch_ssim_loss(sa, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
 int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float grad_thresh, float size_thresh,
                         float screen_thresh, int check_screen, float cull_alpha_thresh, float cull_scale_thresh,
                         float cull_screen_size, int check_huge, const float *xys_grad_norm, const float *vis_counts,

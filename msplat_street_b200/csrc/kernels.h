@@ -92,6 +92,7 @@ struct BackwardArgs {
     const float *slots;
     // optional per-Gaussian gradient outputs (null to skip)
     float *v_xy, *v_conic, *v_rgb, *v_opacity, *v_mean3d, *v_scale, *v_quat;
+    float *g_dc, *g_rest;  // SH gradients as arrays (gradient-only mode, no Adam)
     // Adam: groups means, scales, quats, dc, rest, opacity
     int do_adam;
     float *p[6], *m1[6], *m2[6];

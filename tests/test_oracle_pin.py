@@ -228,3 +228,23 @@ def test_reference_image_ops(rest):
     u8 = rng.integers(0, 256, (37, 53, 4)).astype(np.uint8)
     assert np.array_equal(rest.resize_area(u8, 53, 37), ref.resize_area(u8, 53, 37))
     assert np.array_equal(rest.pack_rgba8(a * 1.2 - 0.1), ref.pack_rgba8(a * 1.2 - 0.1))
+
+
+# ---- the oracle's gradients against float64 finite differences --------------------
+
+@pytest.mark.parametrize("view_dependent", [False, True])
+def test_oracle_gradients_match_finite_differences(rest, view_dependent):
+    """Like the reference's own gradient check (tests/gradcheck.cpp), on the smooth
+    64-Gaussian 32x32 scenes, against tests/golden/fd_smooth.npz."""
+    from grad_util import fd_agreement, oracle_param_grads
+    from smooth_scenes import smooth_scene
+    g, cam, gt = smooth_scene(view_dependent=view_dependent)
+    fx = _load("fd_smooth.npz")
+    tag = "vd" if view_dependent else "flat"
+    fd = [fx[f"{tag}_{k}"] for k in ("means", "scales", "quats", "dc", "rest", "opacities")]
+    ad = new_adam_state(g, C1_LRS, 1)
+    st = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+    rest.train_step(g.copy(), cam, BACKGROUND, gt, ad, st)
+    grads = oracle_param_grads(rest, g, cam, 3)
+    bad, checked, cos = fd_agreement(grads, fd, skip=(0,) if view_dependent else ())
+    assert bad == 0 and cos > 0.9999, (bad, checked, cos)
