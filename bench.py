@@ -277,6 +277,14 @@ def run_ours(args, world, rank, local):
     peaks, peak_kind = measured_peaks()
     roof = roofline(stages, n_isects, final_n, peaks, peak_kind)
 
+    # ---- differentiable path: recomputed vs stored transmittance (rank 0) ----
+    diff = None
+    if rank == 0:
+        try:
+            diff = differentiation_report(dev)
+        except Exception as e:
+            diff = {"error": str(e)}
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if world == 1:
@@ -305,8 +313,51 @@ def run_ours(args, world, rank, local):
             "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
             "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
             "cpu_baseline": cpu,
+            "differentiation": diff,
         }
         print(json.dumps(line))
+
+
+def differentiation_report(dev):
+    """Differentiable path on 200,000 Gaussians at 1024x768 (loss = L1 + 0.2 (1 - SSIM)
+    through torch.autograd): forward and backward times (CUDA events, median of 5 after
+    2 warm-ups) and device memory with recomputed vs stored transmittance."""
+    import torch
+    from msplat_street_b200 import autograd as ag
+    from msplat_street_b200 import scenes
+    from msplat_street_b200.backend import GaussianParams
+    from msplat_street_b200.workloads import BACKGROUND
+
+    g = scenes.random_gaussians(200_000, 21)
+    cam = scenes.small_camera(1024, 768, 1000.0, 3.0)
+    with torch.no_grad():
+        gt = ag.render(GaussianParams.from_numpy(scenes.random_gaussians(200_000, 22), dev), cam, BACKGROUND)
+    out = {"case": "200k Gaussians, 1024x768, L1+0.2(1-SSIM)"}
+    for mode, cap in (("recompute", 0), ("store", 256)):
+        ag.set_transmittance_mode(mode, cap or 256)
+        ag._POOL.clear()
+        torch.cuda.empty_cache()
+        torch.cuda.reset_peak_memory_stats(dev)
+        fw, bw = [], []
+        for it in range(7):
+            p = GaussianParams(*[torch.from_numpy(a).to(dev).requires_grad_(True) for a in g.arrays()])
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            loss = ag.ssim_l1_loss(ag.render(p, cam, BACKGROUND), gt)
+            e1.record()
+            loss.backward()
+            e2.record()
+            torch.cuda.synchronize()
+            if it >= 2:
+                fw.append(e0.elapsed_time(e1))
+                bw.append(e1.elapsed_time(e2))
+        out[mode] = {"forward_ms": statistics.median(fw), "backward_ms": statistics.median(bw),
+                     "frame_bytes": ag.pool_device_bytes(),
+                     "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev)),
+                     "peak_hbm_bytes": ag.pool_device_bytes() + int(torch.cuda.max_memory_allocated(dev))}
+    ag.set_transmittance_mode("recompute")
+    ag._POOL.clear()
+    return out
 
 
 def _upload(trainer, host_targets, dev):

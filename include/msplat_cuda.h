@@ -52,8 +52,15 @@ void msplat_cuda_ctx_destroy(msplat_cuda_ctx *ctx);
 msplat_cuda_ctx *msplat_cuda_default_ctx(void);
 /* Stream for all later work of this context (a cudaStream_t; NULL = legacy default). */
 int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
-/* Options: "keep_grads" (1 = keep per-Gaussian gradients for msplat_cuda_frame). */
+/* Options: "keep_grads" (1 = keep per-Gaussian gradients for msplat_cuda_frame);
+ * "stage_timing" (1 = time the stages, see msplat_cuda_drain_stage_times);
+ * "store_transmittance" (K > 0: the forward stores each pixel's transmittance before
+ * its first K contributions and the backward reads them instead of recovering T by
+ * division, which the reference does (msplat_cpu.cpp:996-997); pixels with more
+ * contributions fall back to division; 0 = off, the default). */
 int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
+/* Bytes of device memory the context's caches hold. */
+int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx);
 
 /* bindings.h:8 cleanup_msplat_metal -- release the context's cached buffers. */
 int msplat_cuda_cleanup(msplat_cuda_ctx *ctx);

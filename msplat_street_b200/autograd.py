@@ -31,13 +31,35 @@ from .camera import CameraSetup
 
 _POOL: List[Context] = []
 _POOL_LOCK = threading.Lock()
+_STORE_T = 0
+
+
+def set_transmittance_mode(mode: str = "recompute", capacity: int = 256) -> None:
+    """"recompute" (default): the backward recovers each pixel's transmittance from its
+    final value by division, back to front, as the reference does; memory does not grow
+    with the number of contributions. "store": the forward stores the transmittance
+    before each of a pixel's first ``capacity`` contributions (4 bytes each per pixel)
+    and the backward reads it (no division; pixels beyond capacity fall back)."""
+    global _STORE_T
+    if mode not in ("recompute", "store"):
+        raise ValueError("mode must be 'recompute' or 'store'")
+    _STORE_T = int(capacity) if mode == "store" else 0
 
 
 def _acquire() -> Context:
     with _POOL_LOCK:
-        if _POOL:
-            return _POOL.pop()
-    return Context()
+        c = _POOL.pop() if _POOL else None
+    if c is None:
+        c = Context()
+    if c.store_transmittance != _STORE_T:
+        c.set_store_transmittance(_STORE_T)
+    return c
+
+
+def pool_device_bytes() -> int:
+    """Device memory held by the idle contexts of the pool."""
+    with _POOL_LOCK:
+        return sum(c.device_bytes() for c in _POOL)
 
 
 def _release(c: Context) -> None:

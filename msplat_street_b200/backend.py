@@ -113,7 +113,7 @@ def adam_step_scalars(lrs, step: int, beta1: float = 0.9, beta2: float = 0.999):
 class Context:
     """One msplat_cuda context: a frame cache plus the stream it works on."""
 
-    def __init__(self, keep_grads: bool = False):
+    def __init__(self, keep_grads: bool = False, store_transmittance: int = 0):
         if not torch.cuda.is_available():
             raise _lib.MsplatCudaError("msplat_street_b200 needs a CUDA device (no CPU fallback)")
         self._lib = lib()
@@ -123,6 +123,17 @@ class Context:
         self.keep_grads = keep_grads
         if keep_grads:
             check(self._lib.msplat_cuda_ctx_set_option(h, b"keep_grads", 1))
+        self.set_store_transmittance(store_transmittance)
+
+    def set_store_transmittance(self, capacity: int) -> None:
+        """0: the backward recovers transmittance by division (the reference's way);
+        K > 0: the forward stores it for each pixel's first K contributions."""
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"store_transmittance", int(capacity)))
+        self.store_transmittance = int(capacity)
+
+    def device_bytes(self) -> int:
+        """Device memory held by this context's caches."""
+        return int(self._lib.msplat_cuda_ctx_device_bytes(self.handle))
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:

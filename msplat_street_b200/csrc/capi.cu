@@ -136,6 +136,9 @@ struct msplat_cuda_ctx {
     Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
     // densification and primitive scratch
     Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md;
+    // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
+    int tstore_cap = 0;
+    Buf tstore, tcount;
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
     int32_t *h_count = nullptr;  // pinned readback of the densified count
 
@@ -148,7 +151,7 @@ struct msplat_cuda_ctx {
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md};
+                      &k_sorted, &k_box, &k_md, &tstore, &tcount};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);
             b->ptr = nullptr;
@@ -316,6 +319,16 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ra.out_img = out_img;
     ra.final_T = final_T;
     ra.final_idx = final_idx;
+    ra.tstore = nullptr;
+    ra.tcount = nullptr;
+    ra.tcap = 0;
+    if (ctx->tstore_cap > 0) {
+        ENSURE(ctx->tstore, (size_t)ctx->tstore_cap * npix, float, ts);
+        ENSURE(ctx->tcount, npix, int32_t, tc);
+        ra.tstore = ts;
+        ra.tcount = tc;
+        ra.tcap = ctx->tstore_cap;
+    }
     ctx->timer.mark(2, st);
     launch_raster_fwd(ra, st);
     ctx->timer.mark(3, st);
@@ -362,6 +375,11 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
     if (!ctx || !name) return fail(MSPLAT_CUDA_EINVAL, "null context or option name");
     if (!std::strcmp(name, "keep_grads")) {
         ctx->keep_grads = value != 0;
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "store_transmittance")) {
+        if (value < 0 || value > 4096) return fail(MSPLAT_CUDA_EINVAL, "store_transmittance capacity must be 0..4096");
+        ctx->tstore_cap = (int)value;
         return MSPLAT_CUDA_OK;
     }
     if (!std::strcmp(name, "stage_timing")) {
@@ -495,6 +513,8 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     rb.final_idx = reinterpret_cast<const int32_t *>(ctx->final_idx.ptr);
     rb.v_out = v_rendered;
     rb.slots = slots;
+    rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
+    rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
     launch_raster_bwd(rb, st);
     ctx->timer.mark(5, st);
 
@@ -602,6 +622,8 @@ int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const floa
     rb.final_idx = reinterpret_cast<const int32_t *>(ctx->final_idx.ptr);
     rb.v_out = v_img;
     rb.slots = slots;
+    rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
+    rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
     launch_raster_bwd(rb, st);
     BackwardArgs ba;
     std::memset(&ba, 0, sizeof ba);
@@ -809,6 +831,21 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
 }
 
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
+
+int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
+    if (!ctx) return -1;
+    const Buf *all[] = {&ctx->splats, &ctx->radii, &ctx->aabb, &ctx->n_tiles, &ctx->offsets, &ctx->scan_part,
+                        &ctx->total, &ctx->v_xy, &ctx->v_conic, &ctx->v_rgb, &ctx->v_opacity, &ctx->v_mean3d,
+                        &ctx->v_scale, &ctx->v_quat, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1],
+                        &ctx->emit_gid, &ctx->isect_gid, &ctx->inv, &ctx->slots, &ctx->radix_scratch,
+                        &ctx->tile_start, &ctx->tile_end, &ctx->out_img, &ctx->final_T, &ctx->final_idx,
+                        &ctx->v_rendered, &ctx->loss_part, &ctx->loss, &ctx->d_flags, &ctx->d_counts,
+                        &ctx->d_scratch, &ctx->k_bounds, &ctx->k_sorted, &ctx->k_box, &ctx->k_md, &ctx->tstore,
+                        &ctx->tcount};
+    int64_t total = 0;
+    for (const Buf *b : all) total += (int64_t)b->bytes;
+    return total;
+}
 
 int msplat_cuda_drain_stage_times(msplat_cuda_ctx *ctx, double *ms, int64_t *calls, int max_stages, int *n_stages,
                                   const char **names) {

@@ -55,6 +55,11 @@ struct RasterArgs {
     float bg[3];
     float *out_img, *final_T;
     int32_t *final_idx;
+    // stored-transmittance mode (null = off): T before each contribution, slot-major
+    // ([tcap][W*H]), and the per-pixel count (-1 when it exceeded tcap)
+    float *tstore;
+    int32_t *tcount;
+    int tcap;
 };
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st);
 
@@ -67,6 +72,8 @@ struct RasterBwdArgs {
     const int32_t *final_idx;
     const float *v_out;
     float *slots;  // 9 floats per sorted intersection
+    const float *tstore;  // stored-transmittance mode, as RasterArgs (null = divide)
+    const int32_t *tcount;
 };
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st);
 

@@ -46,6 +46,9 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
     float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f;
     int last = start - 1;
     bool done = !inside;
+    const size_t npix = (size_t)a.W * a.H;
+    const size_t pid = inside ? (size_t)py * a.W + px : 0;
+    int stored = 0;  // contributions seen (stored-transmittance mode)
     for (int b0 = start; b0 < end; b0 += FWD_BATCH) {
         if (__syncthreads_count(done) == TILE_PIX) break;
         const int k = b0 + threadIdx.x;
@@ -72,6 +75,10 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
                 done = true;
                 break;
             }
+            if (a.tstore) {
+                if (stored < a.tcap) a.tstore[(size_t)stored * npix + pid] = T;
+                stored++;
+            }
             const float vis = alpha * T;
             cr = fmaxf(B.z + 0.5f, 0.f) * vis + cr;
             cg = fmaxf(B.w + 0.5f, 0.f) * vis + cg;
@@ -81,9 +88,9 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
         }
     }
     if (!inside) return;
-    const int pid = py * a.W + px;
     a.final_T[pid] = T;
     a.final_idx[pid] = last;
+    if (a.tcount) a.tcount[pid] = stored <= a.tcap ? stored : -1;
     float *o = a.out_img + 3 * (size_t)pid;
     o[0] = clamp01(a.bg[0] * T + cr);
     o[1] = clamp01(a.bg[1] * T + cg);
@@ -142,6 +149,9 @@ __global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a
     float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
     const float fpx = (float)px, fpy = (float)py;
     float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
+    // stored-transmittance mode: contributions left to pop, -1 = recover T by division
+    int tj = (a.tstore && inside) ? a.tcount[pid] : -1;
+    const size_t npix = (size_t)a.W * a.H;
     for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
         const int b_start = max(start, b_end - BWD_BATCH);
         const int cnt = b_end - b_start;
@@ -177,7 +187,12 @@ __global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a
                         if (alpha >= 1.f / 255.f) {
                             hit = true;
                             const float ra = __frcp_rn(1.f - alpha);  // == 1.f / (1.f - alpha), IEEE
-                            T *= ra;
+                            if (tj > 0) {
+                                tj--;
+                                T = a.tstore[(size_t)tj * npix + pid];  // T before this Gaussian, as stored
+                            } else {
+                                T *= ra;  // recovered by division (core/cpu/msplat_cpu.cpp:996-997)
+                            }
                             const float fac = alpha * T;
                             const float rawr = B.z, rawg = B.w, rawb = C.x;
                             const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),

@@ -114,3 +114,27 @@ def test_render_without_grad_matches_render():
         a = ag.render(p, cam, BACKGROUND)
     b = Oracle("restatement").render(g, cam, BACKGROUND)
     assert max_abs(a.cpu().numpy(), b) <= IMAGE_ATOL
+
+
+@pytest.mark.parametrize("capacity", [256, 4])
+def test_autograd_stored_transmittance(capacity):
+    """Stored transmittance (capacity 256: every pixel stored; 4: most pixels overflow
+    and fall back to division) gives the oracle's gradients like the default mode."""
+    g = scenes.random_gaussians(40_000, 31)
+    cam = scenes.small_camera(320, 240, 310.0, 3.0)
+    ora = Oracle("restatement")
+    gt = ora.render(scenes.random_gaussians(40_000, 32), cam, BACKGROUND)
+    ad = new_adam_state(g, C1_LRS, 1)
+    st = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+    ora.train_step(g.copy(), cam, BACKGROUND, gt, ad, st)
+    ref_grads = oracle_param_grads(ora, g, cam, 3)
+    v_ref = torch.from_numpy(np.ascontiguousarray(ora.frame("v_rendered").reshape(cam.height, cam.width, 3))).cuda()
+    ag.set_transmittance_mode("store", capacity)
+    try:
+        p = _leaf_params(g)
+        img = ag.render(p, cam, BACKGROUND)
+        img.backward(v_ref)
+    finally:
+        ag.set_transmittance_mode("recompute")
+    for t, b, nm in zip(p.tensors(), ref_grads, NAMES):
+        assert rel_l2(t.grad.cpu().numpy(), b) <= GRAD_RTOL_L2, (nm, capacity, rel_l2(t.grad.cpu().numpy(), b))
