@@ -285,6 +285,14 @@ def run_ours(args, world, rank, local):
         except Exception as e:
             diff = {"error": str(e)}
 
+    # ---- render serving (rank 0) ----
+    serve = None
+    if rank == 0 and args.serving_seconds > 0:
+        try:
+            serve = serving_report(dev, args.serving_seconds)
+        except Exception as e:
+            serve = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if world == 1:
@@ -314,8 +322,54 @@ def run_ours(args, world, rank, local):
             "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
             "cpu_baseline": cpu,
             "differentiation": diff,
+            "serving": serve,
         }
+        if serve and "rates" in serve:
+            hi = serve["rates"].get("1000") or next(iter(serve["rates"].values()))
+            line["render"] = {"p50_ms": hi["batched"]["p50_ms"], "p99_ms": hi["batched"]["p99_ms"],
+                              "p99_1080p_ms": hi["batched"]["p99_1080p_ms"],
+                              "plain_p50_ms": hi["plain"]["p50_ms"], "plain_p99_ms": hi["plain"]["p99_ms"],
+                              "at_rate_req_s": 1000}
         print(json.dumps(line))
+
+
+def serving_report(dev, seconds: float, rates=(200.0, 1000.0, 5000.0)):
+    """Render serving: 32 resident scenes (Gaussian counts log-uniform in [5e4, 3e6],
+    SH degree 3, FP32) under a 150 GB budget; Poisson request streams at each rate for
+    ``seconds`` with random cameras on a 5 m sphere and resolutions uniform over
+    {512x512, 1280x720, 1920x1080}. The batched server (3 slots, continuous batching
+    into the persistent rasterizer) and serial plain single-view renders serve the same
+    stream; latency = image complete on the device - arrival. "saturated" offers 1,500
+    requests at once (closed-loop capacity)."""
+    import torch
+    from msplat_street_b200 import serving
+    from msplat_street_b200.workloads import BACKGROUND
+
+    sizes = serving.scene_sizes(32, 50_000, 3_000_000, seed=5)
+    store = serving.SceneStore(150 * 10 ** 9, device=dev)
+    for i, n in enumerate(sizes):
+        store.add(i, serving.random_scene_tensors(n, 100 + i, device=dev), resident=True, host_copy=False)
+    torch.cuda.synchronize()
+    srv = serving.RenderServer(store, BACKGROUND, slots=3, max_batch=16, max_batch_pixels=16 * 1920 * 1080)
+    plain = serving.RenderServer(store, BACKGROUND, mode="plain")
+    warm = serving.poisson_requests(2000.0, 0.1, len(sizes), seed=1)
+    srv.run(warm, realtime=False)
+    plain.run(warm, realtime=False)
+    out = {"scenes": len(sizes), "gaussians_total": int(sum(sizes)), "budget_gb": 150,
+           "resident_gb": store.resident_bytes / 1e9, "stream_seconds": seconds, "rates": {}}
+    for rate in rates:
+        reqs = serving.poisson_requests(rate, seconds, len(sizes), seed=int(rate))
+        b = serving.latency_summary(srv.run(reqs, realtime=True))
+        p = serving.latency_summary(plain.run(reqs, realtime=True))
+        out["rates"][str(int(rate))] = {"batched": b, "plain": p}
+    burst = serving.poisson_requests(1e6, 1500 / 1e6, len(sizes), seed=3)
+    out["saturated"] = {"requests": len(burst),
+                        "batched": serving.latency_summary(srv.run(burst, realtime=False)),
+                        "plain": serving.latency_summary(plain.run(burst, realtime=False))}
+    out["server_reserved_gb"] = srv.reserved_bytes() / 1e9
+    srv.close()
+    plain.close()
+    return out
 
 
 def differentiation_report(dev):
@@ -415,6 +469,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quick", action="store_true", help="device-timed pass only (no e2e, no CPU baseline)")
+    ap.add_argument("--serving-seconds", type=float, default=1.0,
+                    help="length of each Poisson request stream in the serving report (0 = skip)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

@@ -86,6 +86,29 @@ int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3
                        const float *cam_pos, const float *features_dc, const float *features_rest,
                        const float *opacities, const float *background, const float **out_img);
 
+/* One view of a batched render: a scene (device parameter arrays, layouts as
+ * msplat_render) seen by one camera, and the device (H,W,3) image to write. */
+typedef struct msplat_cuda_view {
+    int32_t num_points;
+    const float *means3d, *scales, *quats, *features_dc, *features_rest, *opacities;
+    float glob_scale;
+    uint32_t degree, degrees_to_use;
+    float viewmat[16], projmat[16]; /* row-major */
+    float fx, fy, cx, cy;
+    uint32_t img_height, img_width;
+    float clip_thresh;
+    float cam_pos[3];
+    float background[3];
+    float *out_img;
+} msplat_cuda_view;
+
+/* Batched msplat_render (no counterpart in the reference, whose render takes one
+ * view, bindings.h:81-91): n_views views of any scenes and resolutions rendered by one
+ * projection launch, one sort and one persistent rasterizer launch that pulls
+ * (view, tile) work items. Each image equals what msplat_cuda_render gives for that
+ * view alone, bit for bit. Synchronises once (the intersection count sizes the sort). */
+int msplat_cuda_render_batch(msplat_cuda_ctx *ctx, int32_t n_views, const msplat_cuda_view *views);
+
 /* bindings.h:100-118 msplat_train_step: forward, L1 + SSIM loss, backward, Adam on the
  * six parameter groups (means, scales, quats, features_dc, features_rest, opacities --
  * the parameter arrays themselves, which the reference's adam_params alias,

@@ -65,6 +65,26 @@ _SIGS = {
     "msplat_cuda_drain_stage_times": (i32, [vp, vp, vp, i32, C.POINTER(i32), vp]),
 }
 
+class View(C.Structure):
+    """msplat_cuda_view (include/msplat_cuda.h): one view of a batched render."""
+    _fields_ = [
+        ("num_points", C.c_int32),
+        ("means3d", vp), ("scales", vp), ("quats", vp), ("features_dc", vp), ("features_rest", vp),
+        ("opacities", vp),
+        ("glob_scale", f32),
+        ("degree", C.c_uint32), ("degrees_to_use", C.c_uint32),
+        ("viewmat", f32 * 16), ("projmat", f32 * 16),
+        ("fx", f32), ("fy", f32), ("cx", f32), ("cy", f32),
+        ("img_height", C.c_uint32), ("img_width", C.c_uint32),
+        ("clip_thresh", f32),
+        ("cam_pos", f32 * 3),
+        ("background", f32 * 3),
+        ("out_img", vp),
+    ]
+
+
+_SIGS["msplat_cuda_render_batch"] = (i32, [vp, C.c_int32, C.POINTER(View)])
+
 # entry points added later in the build; bound when the library exports them
 _OPTIONAL_SIGS: dict = {}
 

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass, field
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -27,6 +27,10 @@ def ptr(t: Optional[torch.Tensor]):
 
 def _f32(a):
     return np.ascontiguousarray(np.asarray(a, np.float32))
+
+
+def _addr(t: Optional[torch.Tensor]):
+    return t.data_ptr() if t is not None else None
 
 
 def require_cuda(t: torch.Tensor, name: str) -> None:
@@ -110,6 +114,17 @@ def adam_step_scalars(lrs, step: int, beta1: float = 0.9, beta2: float = 0.999):
     return ss, b2
 
 
+@dataclass
+class BatchItem:
+    """One view of a batched render: a scene, a camera and the render scalars."""
+    params: "GaussianParams"
+    camera: CameraSetup
+    background: object
+    degrees_to_use: Optional[int] = None
+    glob_scale: float = 1.0
+    clip_thresh: float = 0.01
+
+
 class Context:
     """One msplat_cuda context: a frame cache plus the stream it works on."""
 
@@ -174,6 +189,45 @@ class Context:
             out = torch.empty((cam.height, cam.width, 3), dtype=torch.float32, device=p.means.device)
         check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out), C.c_void_p(src), out.numel() * 4))
         return out
+
+    def render_batch(self, items: Sequence["BatchItem"], outs: Optional[List[torch.Tensor]] = None,
+                     stream: Optional[torch.cuda.Stream] = None) -> List[torch.Tensor]:
+        """Batched msplat_render (msplat_cuda_render_batch): every item's view rendered
+        by one projection, one sort and one persistent rasterizer launch, each image
+        equal to the single-view render. Returns (H, W, 3) tensors (``outs`` if given)."""
+        self.bind_stream(stream)
+        if not items:
+            return []
+        views = (_lib.View * len(items))()
+        res = []
+        for k, it in enumerate(items):
+            p, cam = it.params, it.camera
+            if outs is not None:
+                out = outs[k]
+                if (out.shape != (cam.height, cam.width, 3) or out.dtype != torch.float32 or not out.is_cuda
+                        or not out.is_contiguous()):
+                    raise ValueError(f"outs[{k}] must be a contiguous float32 CUDA ({cam.height}, {cam.width}, 3)")
+            else:
+                out = torch.empty((cam.height, cam.width, 3), dtype=torch.float32, device=p.means.device)
+            res.append(out)
+            w = views[k]
+            w.num_points = p.n
+            w.means3d, w.scales, w.quats = _addr(p.means), _addr(p.scales), _addr(p.quats)
+            w.features_dc, w.features_rest, w.opacities = (_addr(p.features_dc), _addr(p.features_rest),
+                                                            _addr(p.opacities))
+            w.glob_scale = it.glob_scale
+            w.degree = p.sh_degree
+            w.degrees_to_use = p.sh_degree if it.degrees_to_use is None else it.degrees_to_use
+            w.viewmat[:] = [float(x) for x in cam.viewmat.reshape(-1)]
+            w.projmat[:] = [float(x) for x in cam.projmat.reshape(-1)]
+            w.fx, w.fy, w.cx, w.cy = cam.fx, cam.fy, cam.cx, cam.cy
+            w.img_height, w.img_width = cam.height, cam.width
+            w.clip_thresh = it.clip_thresh
+            w.cam_pos[:] = [float(x) for x in cam.cam_pos.reshape(-1)]
+            w.background[:] = [float(x) for x in _f32(it.background).reshape(-1)]
+            w.out_img = out.data_ptr()
+        check(self._lib.msplat_cuda_render_batch(self.handle, len(items), views))
+        return res
 
     # -- bindings.h:100-118 ----------------------------------------------------------
     def train_step(self, p: GaussianParams, adam: AdamState, cam: CameraSetup, background, gt: torch.Tensor,

@@ -112,6 +112,94 @@ __device__ __forceinline__ void cov3d_vjp(V3 sc, float gs, Q4 q, const float *gc
     gq[3] = r.w;
 }
 
+
+// Sums of the 9 raster-backward values over each visible Gaussian's intersection
+// slots, in sorted (tile) order. A Gaussian may cover hundreds of tiles, so the warp
+// sums each of its visible Gaussians together: lane l takes the intersections l,
+// l+32, ... and a fixed butterfly combines the lanes. g0 = index of the warp's first
+// Gaussian in offsets / n_tiles; s9 is zero for invisible Gaussians.
+__device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64_t *offsets, const int32_t *n_tiles,
+                                               const int32_t *inv, const float *slots, float s9[9]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 9; c++) s9[c] = 0.f;
+    const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
+    for (int gl = 0; gl < 32; gl++) {
+        if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
+        const int64_t e0 = offsets[g0 + gl];
+        const int cnt = n_tiles[g0 + gl];
+        float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int j = lane; j < cnt; j += 32) {
+            const float *sl = slots + (size_t)inv[e0 + j] * 9;
+#pragma unroll
+            for (int c = 0; c < 9; c++) p[c] += sl[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) p[c] += __shfl_xor_sync(0xffffffffu, p[c], o);
+            if (lane == gl) s9[c] = p[c];
+        }
+    }
+}
+
+// Projection, EWA and covariance VJPs of one visible Gaussian i seen by camera cam
+// (core/cpu/msplat_cpu.cpp:1068-1110): mean, scale and quaternion gradients from its
+// summed xy / conic gradients, and its unit view direction for the SH gradients.
+__device__ __forceinline__ void projection_vjp(const CamParams &cam, const float *means, const float *scales,
+                                               const float *quats, float glob_scale, const Splat *sp, int i,
+                                               const float s9[9], float gm[3], float gsv[3], float gq[4], V3 &dir) {
+    const float *vm = cam.viewmat;
+    V3 pw = ld3(means, i);
+    V3 vmn = center_vjp(cam.projmat, pw, cam.width, cam.height, s9[0], s9[1]);
+    vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, 0.f));  // no expected-depth term without priors
+    gm[0] = vmn.x;
+    gm[1] = vmn.y;
+    gm[2] = vmn.z;
+    const float4 sp0 = reinterpret_cast<const float4 *>(sp)[0];
+    const float4 sp1 = reinterpret_cast<const float4 *>(sp)[1];
+    float gc2[3];
+    conic_vjp(V3{sp0.z, sp0.w, sp1.x}, V3{s9[2], s9[3], s9[4]}, gc2);
+    V3 ls = ld3(scales, i);
+    V3 es{exp_ref(ls.x), exp_ref(ls.y), exp_ref(ls.z)};
+    const float4 qq = reinterpret_cast<const float4 *>(quats)[i];
+    Q4 q{qq.x, qq.y, qq.z, qq.w};
+    float cov[6];
+    cov3d_of(es, glob_scale, q, cov);
+    const float tfx = 0.5f * (float)cam.width / cam.fx, tfy = 0.5f * (float)cam.height / cam.fy;
+    V3 pv{vm[0] * pw.x + vm[1] * pw.y + vm[2] * pw.z + vm[3], vm[4] * pw.x + vm[5] * pw.y + vm[6] * pw.z + vm[7],
+          vm[8] * pw.x + vm[9] * pw.y + vm[10] * pw.z + vm[11]};
+    float gc3[6];
+    ewa_vjp(cov, vm, cam.fx, cam.fy, tfx, tfy, V3{gc2[0], gc2[1], gc2[2]}, gm, gc3, pv);
+    cov3d_vjp(es, glob_scale, q, gc3, gsv, gq);
+    gsv[0] *= es.x;
+    gsv[1] *= es.y;
+    gsv[2] *= es.z;
+    dir = unit(sub(pw, V3{cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]}));
+}
+
+// The 15 SH basis values beyond DC for unit direction (x, y, z)
+// (core/cpu/msplat_cpu.cpp:101-130).
+__device__ __forceinline__ void sh_rest_basis(V3 d, float *bs) {
+    float x = d.x, y = d.y, z = d.z;
+    float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
+    bs[0] = -SH_C1 * y;
+    bs[1] = SH_C1 * z;
+    bs[2] = -SH_C1 * x;
+    bs[3] = SH_C2_0 * xy;
+    bs[4] = SH_C2_1 * yz;
+    bs[5] = SH_C2_2 * (2.f * zz - xx - yy);
+    bs[6] = SH_C2_3 * xz;
+    bs[7] = SH_C2_4 * (xx - yy);
+    bs[8] = SH_C3_0 * y * (3.f * xx - yy);
+    bs[9] = SH_C3_1 * xy * z;
+    bs[10] = SH_C3_2 * y * (4.f * zz - xx - yy);
+    bs[11] = SH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
+    bs[12] = SH_C3_4 * x * (4.f * zz - xx - yy);
+    bs[13] = SH_C3_5 * z * (xx - yy);
+    bs[14] = SH_C3_6 * x * (xx - 3.f * yy);
+}
+
 }  // namespace
 
 constexpr int BWD_THREADS = 256;
@@ -127,31 +215,10 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     const bool vis = valid && a.radii[i] > 0;
     const float b1 = a.beta1, b2 = a.beta2, eps = a.eps;
 
-    // 1. per-Gaussian sums of the intersection slots. A Gaussian may cover hundreds of
-    // tiles, so the warp sums each of its visible Gaussians together: lane l takes the
-    // intersections l, l+32, ... and a fixed butterfly combines the lanes.
-    float s9[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    {
-        const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
-        const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + (threadIdx.x - lane);
-        for (int gl = 0; gl < 32; gl++) {
-            if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
-            const int64_t e0 = a.offsets[g0 + gl];
-            const int cnt = a.n_tiles[g0 + gl];
-            float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            for (int j = lane; j < cnt; j += 32) {
-                const float *sl = a.slots + (size_t)a.inv[e0 + j] * 9;
-#pragma unroll
-                for (int c = 0; c < 9; c++) p[c] += sl[c];
-            }
-#pragma unroll
-            for (int c = 0; c < 9; c++) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) p[c] += __shfl_xor_sync(0xffffffffu, p[c], o);
-                if (lane == gl) s9[c] = p[c];
-            }
-        }
-    }
+    // 1. per-Gaussian sums of the intersection slots
+    float s9[9];
+    warp_slot_sums(vis, (int64_t)blockIdx.x * BWD_THREADS + (threadIdx.x - lane), a.offsets, a.n_tiles, a.inv,
+                   a.slots, s9);
     if (valid) {  // s9 is zero for invisible Gaussians
         if (a.v_xy) {
             a.v_xy[2 * i] = s9[0];
@@ -173,35 +240,7 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     // 2. projection VJPs
     float gm[3] = {0.f, 0.f, 0.f}, gsv[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f};
     V3 dir{0.f, 0.f, 1.f};
-    if (vis) {
-        const float *vm = a.cam.viewmat;
-        V3 pw = ld3(a.means, i);
-        V3 vmn = center_vjp(a.cam.projmat, pw, a.cam.width, a.cam.height, s9[0], s9[1]);
-        vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, 0.f));  // no expected-depth term without priors
-        gm[0] = vmn.x;
-        gm[1] = vmn.y;
-        gm[2] = vmn.z;
-        const float4 sp0 = reinterpret_cast<const float4 *>(a.splats + i)[0];
-        const float4 sp1 = reinterpret_cast<const float4 *>(a.splats + i)[1];
-        float gc2[3];
-        conic_vjp(V3{sp0.z, sp0.w, sp1.x}, V3{s9[2], s9[3], s9[4]}, gc2);
-        V3 ls = ld3(a.scales, i);
-        V3 es{exp_ref(ls.x), exp_ref(ls.y), exp_ref(ls.z)};
-        const float4 qq = reinterpret_cast<const float4 *>(a.quats)[i];
-        Q4 q{qq.x, qq.y, qq.z, qq.w};
-        float cov[6];
-        cov3d_of(es, a.glob_scale, q, cov);
-        const float tfx = 0.5f * (float)a.cam.width / a.cam.fx, tfy = 0.5f * (float)a.cam.height / a.cam.fy;
-        V3 pv{vm[0] * pw.x + vm[1] * pw.y + vm[2] * pw.z + vm[3], vm[4] * pw.x + vm[5] * pw.y + vm[6] * pw.z + vm[7],
-              vm[8] * pw.x + vm[9] * pw.y + vm[10] * pw.z + vm[11]};
-        float gc3[6];
-        ewa_vjp(cov, vm, a.cam.fx, a.cam.fy, tfx, tfy, V3{gc2[0], gc2[1], gc2[2]}, gm, gc3, pv);
-        cov3d_vjp(es, a.glob_scale, q, gc3, gsv, gq);
-        gsv[0] *= es.x;
-        gsv[1] *= es.y;
-        gsv[2] *= es.z;
-        dir = unit(sub(pw, V3{a.cam.cam_pos[0], a.cam.cam_pos[1], a.cam.cam_pos[2]}));
-    }
+    if (vis) projection_vjp(a.cam, a.means, a.scales, a.quats, a.glob_scale, a.splats + i, i, s9, gm, gsv, gq, dir);
     if (valid && a.v_mean3d) {
         for (int c = 0; c < 3; c++) {
             a.v_mean3d[3 * i + c] = gm[c];
@@ -258,24 +297,7 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     const int active = dtu < 1 ? 0 : dtu < 2 ? 3 : dtu < 3 ? 8 : 15;  // bases updated
     if (active == 0 && !a.g_rest) return;
     {
-        float x = dir.x, y = dir.y, z = dir.z;
-        float xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
-        float *bs = s_basis[threadIdx.x];
-        bs[0] = -SH_C1 * y;
-        bs[1] = SH_C1 * z;
-        bs[2] = -SH_C1 * x;
-        bs[3] = SH_C2_0 * xy;
-        bs[4] = SH_C2_1 * yz;
-        bs[5] = SH_C2_2 * (2.f * zz - xx - yy);
-        bs[6] = SH_C2_3 * xz;
-        bs[7] = SH_C2_4 * (xx - yy);
-        bs[8] = SH_C3_0 * y * (3.f * xx - yy);
-        bs[9] = SH_C3_1 * xy * z;
-        bs[10] = SH_C3_2 * y * (4.f * zz - xx - yy);
-        bs[11] = SH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
-        bs[12] = SH_C3_4 * x * (4.f * zz - xx - yy);
-        bs[13] = SH_C3_5 * z * (xx - yy);
-        bs[14] = SH_C3_6 * x * (xx - 3.f * yy);
+        sh_rest_basis(dir, s_basis[threadIdx.x]);
         s_vrgb[threadIdx.x][0] = s9[5];
         s_vrgb[threadIdx.x][1] = s9[6];
         s_vrgb[threadIdx.x][2] = s9[7];
@@ -314,6 +336,139 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
 void launch_backward_adam(const BackwardArgs &a, cudaStream_t st) {
     if (a.n <= 0) return;
     backward_adam_kernel<<<(a.n + BWD_THREADS - 1) / BWD_THREADS, BWD_THREADS, 0, st>>>(a);
+}
+
+// The multi-view form: one thread per Gaussian walks the batch's views in order,
+// sums each view's slots (instance v * n + i), runs that view's projection VJPs and
+// accumulates the gradients, then applies one Adam step. The densification
+// statistics advance once per view that sees the Gaussian, as consecutive
+// single-view steps would advance them. A one-view batch reproduces
+// backward_adam_kernel's update.
+__global__ void __launch_bounds__(BWD_THREADS) backward_adam_batch_kernel(BackwardBatchArgs a) {
+    __shared__ float s_grest[BWD_THREADS][3 * MAX_REST];
+    __shared__ int s_vis[BWD_THREADS];
+    if (a.skip && *a.skip) return;  // block-uniform: the step overflowed its capacity
+    const int i = blockIdx.x * BWD_THREADS + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = i < a.n;
+    const float b1 = a.beta1, b2 = a.beta2, eps = a.eps;
+    const uint32_t dtu = a.degrees_to_use;
+    const int active = dtu < 1 ? 0 : dtu < 2 ? 3 : dtu < 3 ? 8 : 15;  // SH bases beyond DC with gradients
+    const int used = 3 * active;
+    float *grest = s_grest[threadIdx.x];
+    for (int j = 0; j < 3 * MAX_REST; j++) grest[j] = 0.f;
+    float gm[3] = {0.f, 0.f, 0.f}, gsv[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f};
+    float gop = 0.f, gdc[3] = {0.f, 0.f, 0.f};
+    float st_vis = 0.f, st_gn = 0.f, st_ms = 0.f;
+    if (valid && a.vis_counts) {
+        st_vis = a.vis_counts[i];
+        st_gn = a.xys_grad_norm[i];
+        st_ms = a.max_2d_size[i];
+    }
+    bool any = false;
+    for (int v = 0; v < a.n_views; v++) {
+        const int64_t g = (int64_t)v * a.n + i;
+        const bool vis = valid && a.radii[g] > 0;
+        float s9[9];
+        warp_slot_sums(vis, (int64_t)v * a.n + (int64_t)blockIdx.x * BWD_THREADS + (threadIdx.x - lane), a.offsets,
+                       a.n_tiles, a.inv, a.slots, s9);
+        if (!vis) continue;
+        any = true;
+        const CamParams &cam = a.proj[v].cam;
+        float vm[3] = {0.f, 0.f, 0.f}, vs[3] = {0.f, 0.f, 0.f}, vq[4] = {0.f, 0.f, 0.f, 0.f};
+        V3 dir;
+        projection_vjp(cam, a.means, a.scales, a.quats, a.glob_scale, a.splats + g, i, s9, vm, vs, vq, dir);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            gm[c] += vm[c];
+            gsv[c] += vs[c];
+            gdc[c] += SH_C0 * s9[5 + c];
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) gq[c] += vq[c];
+        gop += s9[8];
+        if (active > 0) {
+            float bs[MAX_REST];
+            sh_rest_basis(dir, bs);
+#pragma unroll
+            for (int k = 0; k < MAX_REST; k++) {
+                if (k >= active) break;
+#pragma unroll
+                for (int c = 0; c < 3; c++) grest[3 * k + c] += bs[k] * s9[5 + c];
+            }
+        }
+        st_vis += 1.0f;
+        st_gn += sqrtf(s9[0] * s9[0] + s9[1] * s9[1]);
+        st_ms = fmaxf(st_ms, (float)a.radii[g] * a.inv_max_dim[v]);
+    }
+    s_vis[threadIdx.x] = any ? 1 : 0;
+    if (valid && a.vis_counts && any) {
+        a.vis_counts[i] = st_vis;
+        a.xys_grad_norm[i] = st_gn;
+        a.max_2d_size[i] = st_ms;
+    }
+    if (valid && a.g[0]) {  // summed gradients (zero for Gaussians no view sees)
+        for (int c = 0; c < 3; c++) {
+            a.g[0][3 * (size_t)i + c] = gm[c];
+            a.g[1][3 * (size_t)i + c] = gsv[c];
+            a.g[3][3 * (size_t)i + c] = gdc[c];
+        }
+        for (int c = 0; c < 4; c++) a.g[2][4 * (size_t)i + c] = gq[c];
+        a.g[5][i] = gop;
+    }
+    const float *ss = a.adam_scalars, *bc2 = a.adam_scalars + 6;
+    if (valid && a.do_adam) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t k = 3 * (size_t)i + c;
+            adam_step(a.p[0][k], a.m1[0][k], a.m2[0][k], gm[c], ss[0], b1, b2, bc2[0], eps);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t k = 3 * (size_t)i + c;
+            adam_step(a.p[1][k], a.m1[1][k], a.m2[1][k], gsv[c], ss[1], b1, b2, bc2[1], eps);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const size_t k = 4 * (size_t)i + c;
+            adam_step(a.p[2][k], a.m1[2][k], a.m2[2][k], gq[c], ss[2], b1, b2, bc2[2], eps);
+        }
+        if (a.m1[5]) adam_step(a.p[5][i], a.m1[5][i], a.m2[5][i], gop, ss[5], b1, b2, bc2[5], eps);
+        if (any) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t k = 3 * (size_t)i + c;
+                adam_step(a.p[3][k], a.m1[3][k], a.m2[3][k], gdc[c], ss[3], b1, b2, bc2[3], eps);
+            }
+        }
+    }
+    // SH rest: Adam (or the gradient) warp-cooperatively over the warp's 32 Gaussians
+    if ((!a.do_adam && !a.g[4]) || a.rest_stride <= 0) return;
+    __syncwarp();
+    const int wbase_t = threadIdx.x - lane;
+    const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;
+    const int stride = a.rest_stride;
+    if (a.g[4]) {
+        for (int gl = 0; gl < 32; gl++) {
+            if (g0 + gl >= a.n) break;
+            float *gr = a.g[4] + (size_t)(g0 + gl) * stride;
+            const float *src = s_grest[wbase_t + gl];
+            for (int j = lane; j < stride; j += 32) gr[j] = j < used ? src[j] : 0.f;
+        }
+    }
+    if (!a.do_adam || active == 0) return;
+    for (int gl = 0; gl < 32; gl++) {
+        if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
+        const size_t off = (size_t)(g0 + gl) * stride;
+        float *rest = a.p[4] + off, *r1 = a.m1[4] + off, *r2 = a.m2[4] + off;
+        const float *src = s_grest[wbase_t + gl];
+        for (int j = lane; j < used; j += 32) adam_step(rest[j], r1[j], r2[j], src[j], ss[4], b1, b2, bc2[4], eps);
+    }
+}
+
+void launch_backward_adam_batch(const BackwardBatchArgs &a, cudaStream_t st) {
+    if (a.n <= 0) return;
+    backward_adam_batch_kernel<<<(a.n + BWD_THREADS - 1) / BWD_THREADS, BWD_THREADS, 0, st>>>(a);
 }
 
 }  // namespace msplat

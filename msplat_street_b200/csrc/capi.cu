@@ -141,6 +141,13 @@ struct msplat_cuda_ctx {
     Buf tstore, tcount;
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
     int32_t *h_count = nullptr;  // pinned readback of the densified count
+    // batched render: device view descriptors, their pinned staging copy, the
+    // persistent rasterizer's work counter, and an event after the last upload
+    Buf bdesc, bcounter;
+    unsigned char *h_bdesc = nullptr;
+    size_t h_bdesc_bytes = 0;
+    cudaEvent_t bdesc_ev = nullptr;
+    bool bdesc_pending = false;
 
     ~msplat_cuda_ctx() {
         release();
@@ -151,7 +158,7 @@ struct msplat_cuda_ctx {
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md, &tstore, &tcount};
+                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);
             b->ptr = nullptr;
@@ -161,6 +168,12 @@ struct msplat_cuda_ctx {
         h_total = nullptr;
         if (h_count) cudaFreeHost(h_count);
         h_count = nullptr;
+        if (h_bdesc) cudaFreeHost(h_bdesc);
+        h_bdesc = nullptr;
+        h_bdesc_bytes = 0;
+        if (bdesc_ev) cudaEventDestroy(bdesc_ev);
+        bdesc_ev = nullptr;
+        bdesc_pending = false;
     }
 };
 
@@ -336,6 +349,173 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     return MSPLAT_CUDA_OK;
 }
 
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Batched forward: the stages of forward() over every (view, Gaussian) instance and
+// every (view, tile) of a batch at once. The view descriptors go to the device in
+// two uploads from pinned staging: projection/emission fields first, the raster
+// fields once the intersection count has sized the per-intersection buffers.
+int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
+    cudaStream_t st = ctx->stream;
+    if (nv <= 0) return fail(MSPLAT_CUDA_EINVAL, "n_views must be positive (got %d)", nv);
+    if (!views) return fail(MSPLAT_CUDA_EINVAL, "null view array");
+    int64_t ni = 0, nt = 0;
+    for (int v = 0; v < nv; v++) {
+        const msplat_cuda_view &w = views[v];
+        const int tx = (int)((w.img_width + TILE - 1) / TILE), ty = (int)((w.img_height + TILE - 1) / TILE);
+        if (int r = check_camera(w.num_points, w.img_height, w.img_width, tx, ty, w.degree, w.degrees_to_use,
+                                 w.viewmat, w.projmat, w.cam_pos, w.background))
+            return fail(r, "view %d: %s", v, g_last_error.c_str());
+        if (w.num_points > 0 && (!w.means3d || !w.scales || !w.quats || !w.features_dc || !w.opacities ||
+                                 (w.degree > 0 && !w.features_rest)))
+            return fail(MSPLAT_CUDA_EINVAL, "view %d: null Gaussian parameter pointer", v);
+        if (!w.out_img) return fail(MSPLAT_CUDA_EINVAL, "view %d: null output image", v);
+        ni += w.num_points;
+        nt += (int64_t)tx * ty;
+    }
+    if (ni >= (int64_t)INT32_MAX || nt >= (int64_t)INT32_MAX)
+        return fail(MSPLAT_CUDA_EOVERFLOW, "batch too large: %lld instances, %lld tiles", (long long)ni,
+                    (long long)nt);
+    const int n = (int)ni, T = (int)nt;
+
+    // staging layout: ProjectArgs[nv] | RasterArgs[nv] | inst_off, tile_off [nv+1] | tiles_x, tiles_y [nv]
+    const size_t o_proj = 0;
+    const size_t o_ras = align_up(o_proj + nv * sizeof(ProjectArgs), 256);
+    const size_t o_inst = align_up(o_ras + nv * sizeof(RasterArgs), 256);
+    const size_t o_toff = o_inst + (nv + 1) * sizeof(int);
+    const size_t o_tx = o_toff + (nv + 1) * sizeof(int);
+    const size_t o_ty = o_tx + nv * sizeof(int);
+    const size_t bytes = o_ty + nv * sizeof(int);
+    if (ctx->bdesc_pending) {  // the previous batch's raster upload still reads the staging
+        CUDA_TRY(cudaEventSynchronize(ctx->bdesc_ev));
+        ctx->bdesc_pending = false;
+    }
+    if (ctx->h_bdesc_bytes < bytes) {
+        if (ctx->h_bdesc) cudaFreeHost(ctx->h_bdesc);
+        ctx->h_bdesc = nullptr;
+        ctx->h_bdesc_bytes = 0;
+        CUDA_TRY(cudaMallocHost(&ctx->h_bdesc, bytes + bytes / 4));
+        ctx->h_bdesc_bytes = bytes + bytes / 4;
+    }
+    if (!ctx->bdesc_ev) CUDA_TRY(cudaEventCreateWithFlags(&ctx->bdesc_ev, cudaEventDisableTiming));
+    ENSURE(ctx->bdesc, bytes, unsigned char, d_desc);
+    ENSURE(ctx->bcounter, 1, int, d_counter);
+    ENSURE(ctx->splats, n, Splat, splats);
+    ENSURE(ctx->radii, n, int32_t, radii);
+    ENSURE(ctx->aabb, 2 * (size_t)n, float, aabb);
+    ENSURE(ctx->n_tiles, n, int32_t, n_tiles);
+    ENSURE(ctx->offsets, n, int64_t, offsets);
+    ENSURE(ctx->scan_part, scan_blocks(std::max(n, 1)) + 1, int64_t, scan_part);
+    ENSURE(ctx->total, 1, int64_t, d_total);
+    ENSURE(ctx->tile_start, T, int32_t, tile_start);
+    ENSURE(ctx->tile_end, T, int32_t, tile_end);
+    if (!ctx->h_total) CUDA_TRY(cudaMallocHost(&ctx->h_total, sizeof(int64_t)));
+
+    unsigned char *h = ctx->h_bdesc;
+    ProjectArgs *hp = reinterpret_cast<ProjectArgs *>(h + o_proj);
+    RasterArgs *hr = reinterpret_cast<RasterArgs *>(h + o_ras);
+    int *h_inst = reinterpret_cast<int *>(h + o_inst), *h_toff = reinterpret_cast<int *>(h + o_toff);
+    int *h_tx = reinterpret_cast<int *>(h + o_tx), *h_ty = reinterpret_cast<int *>(h + o_ty);
+    int io = 0, to = 0;
+    for (int v = 0; v < nv; v++) {
+        const msplat_cuda_view &w = views[v];
+        const int tx = (int)((w.img_width + TILE - 1) / TILE), ty = (int)((w.img_height + TILE - 1) / TILE);
+        ProjectArgs &pa = hp[v];
+        pa.n = w.num_points;
+        pa.means = w.means3d;
+        pa.scales = w.scales;
+        pa.quats = w.quats;
+        pa.features_dc = w.features_dc;
+        pa.features_rest = w.features_rest;
+        pa.opacities = w.opacities;
+        pa.rest_stride = (int)(num_sh_bases(w.degree) - 1) * 3;
+        pa.glob_scale = w.glob_scale;
+        pa.cam = make_cam(w.viewmat, w.projmat, w.fx, w.fy, w.cx, w.cy, w.img_height, w.img_width, tx, ty,
+                          w.clip_thresh, w.degree, w.degrees_to_use, w.cam_pos);
+        pa.splats = splats;
+        pa.radii = radii;
+        pa.aabb = aabb;
+        pa.n_tiles = n_tiles;
+        h_inst[v] = io;
+        h_toff[v] = to;
+        h_tx[v] = tx;
+        h_ty[v] = ty;
+        io += w.num_points;
+        to += tx * ty;
+    }
+    h_inst[nv] = io;
+    h_toff[nv] = to;
+    BatchDesc d;
+    d.n_views = nv;
+    d.inst_off = reinterpret_cast<const int *>(d_desc + o_inst);
+    d.tile_off = reinterpret_cast<const int *>(d_desc + o_toff);
+    d.tiles_x = reinterpret_cast<const int *>(d_desc + o_tx);
+    d.tiles_y = reinterpret_cast<const int *>(d_desc + o_ty);
+    d.proj = reinterpret_cast<const ProjectArgs *>(d_desc + o_proj);
+    d.raster = reinterpret_cast<const RasterArgs *>(d_desc + o_ras);
+
+    ctx->n = n;
+    ctx->W = ctx->H = ctx->tiles_x = ctx->tiles_y = 0;  // no single-view frame to inspect
+    ctx->timer.reset_marks();
+    ctx->timer.mark(0, st);
+    CUDA_TRY(cudaMemcpyAsync(d_desc, h, o_ras, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(d_desc + o_inst, h + o_inst, bytes - o_inst, cudaMemcpyHostToDevice, st));
+    launch_project_batch(d, n, st);
+    scan_exclusive<int64_t>(n_tiles, offsets, n, d_total, scan_part, st);
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t n_isect = *ctx->h_total;
+    if (n_isect > (int64_t)INT32_MAX)
+        return fail(MSPLAT_CUDA_EOVERFLOW, "more than 2^31 tile intersections in the batch (%lld)",
+                    (long long)n_isect);
+    ctx->n_isect = n_isect;
+    ENSURE(ctx->keys[0], n_isect, uint64_t, k0);
+    ENSURE(ctx->keys[1], n_isect, uint64_t, k1);
+    ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
+    ENSURE(ctx->vals[1], n_isect, uint32_t, v1);
+    ENSURE(ctx->emit_gid, n_isect, int32_t, emit_gid);
+    ENSURE(ctx->isect_gid, n_isect, int32_t, isect_gid);
+    ENSURE(ctx->inv, n_isect, int32_t, inv);
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
+
+    ctx->timer.mark(1, st);
+    launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, d, k0, v0, emit_gid, st);
+    uint64_t *kk[2] = {k0, k1};
+    uint32_t *vv[2] = {v0, v1};
+    const int cur = radix_sort_pairs(kk, vv, (int)n_isect, 32 + ceil_log2(std::max(T, 1)), rscratch, st);
+    ctx->sorted = cur;
+    launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
+    launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
+
+    for (int v = 0; v < nv; v++) {
+        const msplat_cuda_view &w = views[v];
+        RasterArgs &ra = hr[v];
+        ra.W = (int)w.img_width;
+        ra.H = (int)w.img_height;
+        ra.tiles_x = h_tx[v];
+        ra.tiles_y = h_ty[v];
+        ra.tile_start = tile_start;
+        ra.tile_end = tile_end;
+        ra.isect_gid = isect_gid;
+        ra.splats = splats;
+        for (int c = 0; c < 3; c++) ra.bg[c] = w.background[c];
+        ra.out_img = w.out_img;
+        ra.final_T = nullptr;
+        ra.final_idx = nullptr;
+        ra.tstore = nullptr;
+        ra.tcount = nullptr;
+        ra.tcap = 0;
+    }
+    CUDA_TRY(cudaMemcpyAsync(d_desc + o_ras, h + o_ras, nv * sizeof(RasterArgs), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaEventRecord(ctx->bdesc_ev, st));
+    ctx->bdesc_pending = true;
+    ctx->timer.mark(2, st);
+    launch_raster_fwd_batch(d, T, d_counter, st);
+    ctx->timer.mark(3, st);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
 msplat_cuda_ctx *g_default = nullptr;
 std::mutex g_default_mu;
 
@@ -448,6 +628,13 @@ int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3
         return r;
     ctx->timer.collect();
     if (out_img) *out_img = reinterpret_cast<const float *>(ctx->out_img.ptr);
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_render_batch(msplat_cuda_ctx *ctx, int32_t n_views, const msplat_cuda_view *views) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (int r = forward_batch(ctx, n_views, views)) return r;
+    ctx->timer.collect();
     return MSPLAT_CUDA_OK;
 }
 

@@ -43,10 +43,14 @@ void scan_exclusive(const int32_t *in, TO *out, int n, TO *d_total, TO *partials
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
                       int tiles_x, int tiles_y, uint64_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
 size_t radix_scratch_bytes(int n);
-int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st);
-void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st);
+// d_n / d_T (optional): device-side counts capping the host-side capacities n / T
+int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
+                     const int *d_n = nullptr);
+void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
+                        const int *d_n = nullptr, const int *d_T = nullptr);
 void launch_isect_map(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid, int32_t *inv,
-                      cudaStream_t st);
+                      cudaStream_t st, const int *d_n = nullptr);
+void launch_clamp_count(const int64_t *total, int64_t cap, int *d_n, int *overflow, cudaStream_t st);
 
 struct RasterArgs {
     int W, H, tiles_x, tiles_y;
@@ -62,6 +66,36 @@ struct RasterArgs {
     int tcap;
 };
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st);
+
+// A batch of views rendered by one projection, one sort and one persistent raster
+// launch. Instances (view, Gaussian) and tiles (view, tile) are numbered globally,
+// view after view; every array lives in device memory.
+struct BatchDesc {
+    int n_views;
+    const int *inst_off;       // [n_views + 1] first instance of each view
+    const int *tile_off;       // [n_views + 1] first global tile of each view
+    const int *tiles_x, *tiles_y;
+    const ProjectArgs *proj;   // per view; outputs point at the batch-wide arrays
+    const RasterArgs *raster;  // per view; tile ranges and lists are batch-wide
+};
+
+// The view that holds global index g: the last v with off[v] <= g (views with no
+// instances share their offset with the next view and are skipped).
+__device__ __forceinline__ int find_view(const int *off, int n_views, int g) {
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+void launch_project_batch(const BatchDesc &d, int total, cudaStream_t st);
+void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
+                            const int64_t *offsets, const BatchDesc &d, uint64_t *keys, uint32_t *vals,
+                            int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st);
 
 struct RasterBwdArgs {
     int W, H, tiles_x, tiles_y;
@@ -111,6 +145,32 @@ struct BackwardArgs {
     float inv_max_dim;
 };
 void launch_backward_adam(const BackwardArgs &a, cudaStream_t st);
+
+// Multi-view backward + Adam: instances v * n + i of Gaussian i in each view v.
+struct BackwardBatchArgs {
+    int n, n_views;
+    const ProjectArgs *proj;   // per view (device): the camera
+    const float *inv_max_dim;  // per view (device): 1 / max(W, H)
+    const float *means, *scales, *quats;
+    float glob_scale;
+    uint32_t degrees_to_use;
+    const Splat *splats;
+    const int32_t *radii, *n_tiles, *inv;
+    const int64_t *offsets;
+    const float *slots;
+    float *g[6];  // optional summed gradients (null g[0] to skip): means scales quats dc rest opacity
+    int do_adam;
+    float *p[6], *m1[6], *m2[6];
+    const float *adam_scalars;  // device: step sizes [6], then bias-correction square roots [6]
+    float beta1, beta2, eps;
+    int rest_stride;
+    float *vis_counts, *xys_grad_norm, *max_2d_size;  // null to skip
+    const int *skip;  // device flag (capacity overflow): when set the kernel changes nothing
+};
+void launch_backward_adam_batch(const BackwardBatchArgs &a, cudaStream_t st);
+void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
+                             cudaStream_t st);
+void launch_ssim_loss_batch(const SsimArgs *d_views, const int *d_boff, int n_views, int *d_counter, cudaStream_t st);
 
 struct DensifyArgs {
     int n;

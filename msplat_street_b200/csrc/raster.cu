@@ -20,6 +20,8 @@
 //
 // Compiled with -fmad=false: the alpha and transmittance cut-offs must fall exactly
 // where the reference's do.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -29,10 +31,10 @@ constexpr int FWD_BATCH = TILE_PIX;
 constexpr int BWD_BATCH = 64;
 constexpr int BWD_WARPS = TILE_PIX / 32;
 
-__global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
-    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
-    const int tile = blockIdx.x;
-    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+// One 16x16 tile: `tile` indexes tile_start / tile_end (a global tile id in a batch),
+// (tx, ty) is its position in its view. Every thread of the block must call it.
+__device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
+                                                float4 *s1, float4 *s2) {
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -88,13 +90,59 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
         }
     }
     if (!inside) return;
-    a.final_T[pid] = T;
-    a.final_idx[pid] = last;
+    if (a.final_T) a.final_T[pid] = T;
+    if (a.final_idx) a.final_idx[pid] = last;
     if (a.tcount) a.tcount[pid] = stored <= a.tcap ? stored : -1;
     float *o = a.out_img + 3 * (size_t)pid;
     o[0] = clamp01(a.bg[0] * T + cr);
     o[1] = clamp01(a.bg[1] * T + cg);
     o[2] = clamp01(a.bg[2] * T + cb);
+}
+
+__global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
+    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
+    const int tile = blockIdx.x;
+    raster_fwd_tile(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
+}
+
+// Persistent forward over the tiles of a batch of views (each with its own scene,
+// camera, resolution and output): every block pulls global tile ids from a counter
+// until none are left. A tile's image equals what the per-view kernel renders: the
+// same list (the batch sort keeps each tile's order) and the same code.
+__global__ void __launch_bounds__(TILE_PIX) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
+    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
+    __shared__ int s_tile;
+    const int total_tiles = d.tile_off[d.n_views];  // read on the device: the launch is graph-capturable
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+        __syncthreads();
+        const int t = s_tile;
+        __syncthreads();  // everyone has read s_tile before thread 0 overwrites it
+        if (t >= total_tiles) break;
+        const int v = find_view(d.tile_off, d.n_views, t);
+        const RasterArgs &a = d.raster[v];
+        const int lt = t - d.tile_off[v];
+        raster_fwd_tile(a, t, lt % a.tiles_x, lt / a.tiles_x, s0, s1, s2);
+    }
+}
+
+// Resident blocks on the whole GPU (computed once, thread-safe static).
+int raster_fwd_batch_grid() {
+    static const int grid = [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_fwd_batch_kernel, TILE_PIX, 0);
+        return std::max(1, sms * std::max(per_sm, 1));
+    }();
+    return grid;
+}
+
+// tiles_hint: the batch's tile count when the host knows it (caps the grid), else 0
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st) {
+    cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+    const int grid = tiles_hint > 0 ? std::min(raster_fwd_batch_grid(), tiles_hint) : raster_fwd_batch_grid();
+    raster_fwd_batch_kernel<<<grid, TILE_PIX, 0, st>>>(d, d_counter);
 }
 
 // Per-warp reduction of the 9 gradient values over the warp's 32 pixels, done in
@@ -110,14 +158,14 @@ size_t raster_bwd_smem() {
            sizeof(float) * BWD_WARPS * SUB_OUT * PB_STRIDE + 16;
 }
 
-__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a) {
-    extern __shared__ __align__(16) float4 smem4[];
+// One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
+// global tile id in a batch), (tx, ty) is its position in its view. Every thread of
+// the block calls it; it ends with the block's shared memory free for reuse.
+__device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
+                                                int &kmax) {
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
     float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][9]
     float *pbuf = red + BWD_WARPS * BWD_BATCH * 9;            // [BWD_WARPS][SUB_OUT][PB_STRIDE]
-    __shared__ int kmax;
-    const int tile = blockIdx.x;
-    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -263,10 +311,55 @@ __global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a
         for (int c = 0; c < 9; c++) a.slots[(size_t)k * 9 + c] = 0.f;
 }
 
+__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a) {
+    extern __shared__ __align__(16) float4 smem4[];
+    __shared__ int kmax;
+    const int tile = blockIdx.x;
+    raster_bwd_tile(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
+}
+
+// Persistent backward over the tiles of a batch of views, pulling global tile ids
+// from a counter (the forward's counterpart, raster_fwd_batch_kernel).
+__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_batch_kernel(const RasterBwdArgs *views,
+                                                                        const int *tile_off, int n_views,
+                                                                        int *counter) {
+    extern __shared__ __align__(16) float4 smem4[];
+    __shared__ int kmax, s_tile;
+    const int total_tiles = tile_off[n_views];
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+        __syncthreads();
+        const int t = s_tile;
+        __syncthreads();  // everyone has read s_tile before thread 0 overwrites it
+        if (t >= total_tiles) break;
+        const int v = find_view(tile_off, n_views, t);
+        const RasterBwdArgs a = views[v];
+        const int lt = t - tile_off[v];
+        raster_bwd_tile(a, t, lt % a.tiles_x, lt / a.tiles_x, smem4, kmax);
+        __syncthreads();  // the tile's shared buffers are free before the next tile stages
+    }
+}
+
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
     raster_fwd_kernel<<<T, TILE_PIX, 0, st>>>(a);
+}
+
+void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
+                             cudaStream_t st) {
+    if (n_views <= 0) return;
+    const size_t smem = raster_bwd_smem();
+    static const int grid = [smem] {
+        cudaFuncSetAttribute(raster_bwd_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_bwd_batch_kernel, TILE_PIX, smem);
+        return sms * (per_sm > 0 ? per_sm : 1);
+    }();
+    cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+    raster_bwd_batch_kernel<<<grid, TILE_PIX, smem, st>>>(d_views, d_tile_off, n_views, d_counter);
 }
 
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st) {

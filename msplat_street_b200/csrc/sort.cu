@@ -157,6 +157,38 @@ void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32
                                                       emit_gid);
 }
 
+// Batched emission: instance g (a Gaussian of one view) keys its tiles with the
+// view's first global tile added, so one stable sort orders every view's tiles at
+// once and each tile's list is the one the single-view sort gives.
+__global__ void emit_keys_batch_kernel(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
+                                       const int64_t *offsets, const BatchDesc d, uint64_t *keys, uint32_t *vals,
+                                       int32_t *emit_gid, int64_t cap) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n || n_tiles[g] <= 0) return;
+    const int v = find_view(d.inst_off, d.n_views, g);
+    const int tiles_x = d.tiles_x[v], tiles_y = d.tiles_y[v];
+    const uint64_t base = (uint64_t)d.tile_off[v];
+    const Splat s = splats[g];
+    int x0, y0, x1, y1;
+    rect_of(s, aabb[2 * g], aabb[2 * g + 1], tiles_x, tiles_y, x0, y0, x1, y1);
+    const uint64_t db = (uint64_t)__float_as_uint(s.depth);
+    int64_t e = offsets[g];
+    for (int y = y0; y < y1; y++)
+        for (int x = x0; x < x1 && e < cap; x++, e++) {  // cap: buffer capacity (graph mode)
+            keys[e] = ((base + (uint64_t)(y * tiles_x + x)) << 32) | db;
+            vals[e] = (uint32_t)e;
+            emit_gid[e] = g;
+        }
+}
+
+void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
+                            const int64_t *offsets, const BatchDesc &d, uint64_t *keys, uint32_t *vals,
+                            int32_t *emit_gid, cudaStream_t st, int64_t cap) {
+    if (n <= 0) return;
+    emit_keys_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, n_tiles, offsets, d, keys, vals,
+                                                            emit_gid, cap);
+}
+
 // ---------------------------------------------------------------------------------
 // Stable LSD radix sort of (u64 key, u32 value) by key bits [0, key_bits).
 
@@ -167,8 +199,11 @@ constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per war
 
 int radix_blocks(int n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
-__global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32_t mask, uint32_t *counts, int nb) {
+// d_n (may be null): a device-side count that caps n (capacity-bounded launches)
+__global__ void radix_hist_kernel(const uint64_t *keys, int n, const int *d_n, int shift, uint32_t mask,
+                                  uint32_t *counts, int nb) {
     __shared__ uint32_t h[RADIX];
+    if (d_n) n = min(n, *d_n);
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -187,9 +222,10 @@ __global__ void radix_hist_kernel(const uint64_t *keys, int n, int shift, uint32
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
 __global__ void radix_scatter_kernel(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout, int n,
-                                     int shift, uint32_t mask, const int32_t *offs, int nb) {
+                                     const int *d_n, int shift, uint32_t mask, const int32_t *offs, int nb) {
     __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
     __shared__ uint32_t gbase[RADIX];
+    if (d_n) n = min(n, *d_n);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
@@ -244,9 +280,11 @@ size_t radix_scratch_bytes(int n) {
 }
 
 // Sorts (k[0], v[0]) using (k[1], v[1]) as the ping-pong buffers; returns the index
-// (0 or 1) of the buffer pair holding the result.
-int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st) {
-    if (n <= 1 || key_bits <= 0) return 0;
+// (0 or 1) of the buffer pair holding the result. With d_n, n is a capacity and the
+// count is read on the device (no host round trip; every pass runs).
+int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
+                     const int *d_n) {
+    if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
     const int nb = radix_blocks(n);
     const size_t cnt = (size_t)RADIX * nb;
     int32_t *counts = reinterpret_cast<int32_t *>(scratch);
@@ -256,11 +294,11 @@ int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *
     for (int shift = 0; shift < key_bits; shift += 8) {
         const int bits = key_bits - shift < 8 ? key_bits - shift : 8;  // digits above key_bits are ignored
         const uint32_t mask = (1u << bits) - 1u;
-        radix_hist_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], n, shift, mask, reinterpret_cast<uint32_t *>(counts),
-                                                       nb);
+        radix_hist_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
+                                                       reinterpret_cast<uint32_t *>(counts), nb);
         scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, shift, mask, offs,
-                                                          nb);
+        radix_scatter_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift, mask,
+                                                          offs, nb);
         cur ^= 1;
     }
     return cur;
@@ -270,8 +308,11 @@ int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *
 // Tile ranges by binary search (empty tiles get start == end == the running count,
 // as the reference's prefix sums give), and the per-slot Gaussian id / inverse map.
 
-__global__ void tile_ranges_kernel(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end) {
+__global__ void tile_ranges_kernel(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end,
+                                   const int *d_n, const int *d_T) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_n) n = min(n, *d_n);
+    if (d_T) T = min(T, *d_T);
     if (t > T) return;
     int lo = 0, hi = n;  // first position whose tile id >= t
     while (lo < hi) {
@@ -284,22 +325,38 @@ __global__ void tile_ranges_kernel(const uint64_t *keys, int n, int T, int32_t *
 }
 
 __global__ void isect_map_kernel(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid,
-                                 int32_t *inv) {
+                                 int32_t *inv, const int *d_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_n) n = min(n, *d_n);
     if (k >= n) return;
     const uint32_t e = sorted_e[k];
     isect_gid[k] = emit_gid[e];
     inv[e] = k;
 }
 
-void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st) {
-    tile_ranges_kernel<<<(T + 1 + 255) / 256, 256, 0, st>>>(keys, n, T, tile_start, tile_end);
+void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
+                        const int *d_n, const int *d_T) {
+    tile_ranges_kernel<<<(T + 1 + 255) / 256, 256, 0, st>>>(keys, n, T, tile_start, tile_end, d_n, d_T);
 }
 
 void launch_isect_map(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid, int32_t *inv,
-                      cudaStream_t st) {
+                      cudaStream_t st, const int *d_n) {
     if (n <= 0) return;
-    isect_map_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_e, n, emit_gid, isect_gid, inv);
+    isect_map_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_e, n, emit_gid, isect_gid, inv, d_n);
+}
+
+// Device-side intersection count for capacity-bounded (graph-capturable) steps:
+// d_n = total when it fits the capacity, else 0 with *overflow set (the step then
+// renders nothing and updates nothing; the host grows the buffers and repeats it).
+__global__ void clamp_count_kernel(const int64_t *total, int64_t cap, int *d_n, int *overflow) {
+    const int64_t t = *total;
+    const bool over = t > cap;
+    *d_n = over ? 0 : (int)t;
+    if (over) *overflow = 1;
+}
+
+void launch_clamp_count(const int64_t *total, int64_t cap, int *d_n, int *overflow, cudaStream_t st) {
+    clamp_count_kernel<<<1, 1, 0, st>>>(total, cap, d_n, overflow);
 }
 
 }  // namespace msplat

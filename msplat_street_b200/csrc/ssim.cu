@@ -37,11 +37,11 @@ struct SsimSmem {
     double red[SSIM_THREADS / 32];
 };
 
-__global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_kernel(SsimArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SsimSmem &s = *reinterpret_cast<SsimSmem *>(smem_raw);
+// One 32x32 output block (bx, by) of one image; its loss partial goes to
+// a.partials[pidx]. Every thread of the block calls it.
+__device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, int pidx, SsimSmem &s) {
     const int W = a.W, H = a.H;
-    const int x0 = blockIdx.x * ST, y0 = blockIdx.y * ST;
+    const int x0 = bx * ST, y0 = by * ST;
     const float w = a.ssim_weight;
     // each thread owns output pixels tid, tid+256, ... of the 32x32 tile
     float ssim_acc[4] = {0.f, 0.f, 0.f, 0.f}, l1_acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -186,11 +186,41 @@ __global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_kernel(SsimArgs a) {
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int i = 0; i < SSIM_THREADS / 32; i++) t += s.red[i];
-        a.partials[blockIdx.y * gridDim.x + blockIdx.x] = t;
+        a.partials[pidx] = t;
     }
 }
 
-__global__ void loss_finalize_kernel(const double *partials, int nb, double npix, float *loss) {
+__global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_kernel(SsimArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SsimSmem &s = *reinterpret_cast<SsimSmem *>(smem_raw);
+    ssim_block(a, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, s);
+}
+
+// Persistent loss over the blocks of a batch of images (each with its own size,
+// target and gradient output), pulling global block ids from a counter. Block b of
+// view v writes partial boff[v] + (its index within the view), so each view's
+// partials sit in the order the single-image kernel writes them.
+__global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_batch_kernel(const SsimArgs *views, const int *boff,
+                                                                       int n_views, int *counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SsimSmem &s = *reinterpret_cast<SsimSmem *>(smem_raw);
+    __shared__ int s_blk;
+    const int total = boff[n_views];
+    for (;;) {
+        if (threadIdx.x == 0) s_blk = atomicAdd(counter, 1);
+        __syncthreads();
+        const int b = s_blk;
+        __syncthreads();
+        if (b >= total) break;
+        const int v = find_view(boff, n_views, b);
+        const SsimArgs a = views[v];
+        const int lb = b - boff[v], nbx = (a.W + ST - 1) / ST;
+        ssim_block(a, lb % nbx, lb / nbx, b, s);
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void loss_finalize_block(const double *partials, int nb, double npix, float *loss) {
     __shared__ double red[32];
     double s = 0.0;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) s += partials[i];
@@ -205,16 +235,51 @@ __global__ void loss_finalize_kernel(const double *partials, int nb, double npix
     }
 }
 
+__global__ void loss_finalize_kernel(const double *partials, int nb, double npix, float *loss) {
+    loss_finalize_block(partials, nb, npix, loss);
+}
+
+// One 1024-thread block per view: the same reduction as loss_finalize_kernel over
+// that view's partials, so each view's loss equals its single-image loss.
+__global__ void loss_finalize_batch_kernel(const SsimArgs *views, const int *boff) {
+    const int v = blockIdx.x;
+    const SsimArgs &a = views[v];
+    loss_finalize_block(a.partials + boff[v], boff[v + 1] - boff[v], (double)a.W * a.H, a.loss);
+}
+
 int ssim_blocks(int W, int H) { return ((W + ST - 1) / ST) * ((H + ST - 1) / ST); }
+
+static void ssim_set_smem_attr() {
+    static const bool done = [] {
+        cudaFuncSetAttribute(ssim_loss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SsimSmem));
+        cudaFuncSetAttribute(ssim_loss_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(SsimSmem));
+        return true;
+    }();
+    (void)done;
+}
+
+// views[v].partials must all be the same batch-wide array (indexed by global block).
+void launch_ssim_loss_batch(const SsimArgs *d_views, const int *d_boff, int n_views, int *d_counter, cudaStream_t st) {
+    if (n_views <= 0) return;
+    ssim_set_smem_attr();
+    static const int grid = [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ssim_loss_batch_kernel, SSIM_THREADS,
+                                                      sizeof(SsimSmem));
+        return sms * (per_sm > 0 ? per_sm : 1);
+    }();
+    cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+    ssim_loss_batch_kernel<<<grid, SSIM_THREADS, sizeof(SsimSmem), st>>>(d_views, d_boff, n_views, d_counter);
+    loss_finalize_batch_kernel<<<n_views, 1024, 0, st>>>(d_views, d_boff);
+}
 
 void launch_ssim_loss(const SsimArgs &a, cudaStream_t st) {
     if (a.W <= 0 || a.H <= 0) return;
-    static bool attr_set = false;
     const size_t smem = sizeof(SsimSmem);
-    if (!attr_set) {
-        cudaFuncSetAttribute(ssim_loss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+    ssim_set_smem_attr();
     dim3 grid((a.W + ST - 1) / ST, (a.H + ST - 1) / ST);
     ssim_loss_kernel<<<grid, SSIM_THREADS, smem, st>>>(a);
     loss_finalize_kernel<<<1, 1024, 0, st>>>(a.partials, (int)(grid.x * grid.y), (double)a.W * a.H, a.loss);
