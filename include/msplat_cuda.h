@@ -53,6 +53,7 @@ msplat_cuda_ctx *msplat_cuda_default_ctx(void);
 /* Stream for all later work of this context (a cudaStream_t; NULL = legacy default). */
 int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
 /* Options: "keep_grads" (1 = keep per-Gaussian gradients for msplat_cuda_frame);
+ * "graph" (1 = msplat_cuda_train_batch replays a captured CUDA graph of its step);
  * "stage_timing" (1 = time the stages, see msplat_cuda_drain_stage_times);
  * "store_transmittance" (K > 0: the forward stores each pixel's transmittance before
  * its first K contributions and the backward reads them instead of recovering T by
@@ -108,6 +109,39 @@ typedef struct msplat_cuda_view {
  * (view, tile) work items. Each image equals what msplat_cuda_render gives for that
  * view alone, bit for bit. Synchronises once (the intersection count sizes the sort). */
 int msplat_cuda_render_batch(msplat_cuda_ctx *ctx, int32_t n_views, const msplat_cuda_view *views);
+
+/* One view of a batched training step: a camera and its device (H,W,3) target. */
+typedef struct msplat_cuda_train_view {
+    float viewmat[16], projmat[16]; /* row-major */
+    float fx, fy, cx, cy;
+    uint32_t img_height, img_width;
+    float cam_pos[3];
+    const float *gt;
+} msplat_cuda_train_view;
+
+/* Batched msplat_train_step (no counterpart in the reference, whose train step takes
+ * one view, bindings.h:100-118): n_views views of one scene, of any resolutions,
+ * trained in one step. Each view's loss is msplat's L1 + ssim_weight (1 - SSIM) with
+ * its gradient scaled by 1 / (3 W H), as the single-view step scales it; the
+ * gradients are summed over the views and ONE Adam step is applied (groups and
+ * scalars as msplat_cuda_train_step). The densification statistics advance once per
+ * view that sees a Gaussian. grads_out (NULL, or 6 device arrays in parameter layout)
+ * receives the summed gradients. losses_out (host, n_views floats, or NULL) receives
+ * each view's loss. A one-view batch gives msplat_cuda_train_step's update.
+ * With the context option "graph" = 1, steps after the first replay a CUDA graph of
+ * the whole step (projection to Adam; re-captured when a shape or buffer changes).
+ * Synchronises once per call (the intersection count, or the graph's completion). */
+int msplat_cuda_train_batch(msplat_cuda_ctx *ctx, int num_points, float *means3d, float *scales, float glob_scale,
+                            float *quats, float *features_dc, float *features_rest, float *opacities,
+                            unsigned degree, unsigned degrees_to_use, float clip_thresh, const float *background,
+                            int32_t n_views, const msplat_cuda_train_view *views, float ssim_weight,
+                            int num_adam_groups, float *const *adam_exp_avg, float *const *adam_exp_avg_sq,
+                            const float *adam_step_sizes, const float *adam_bc2_sqrts, float adam_beta1,
+                            float adam_beta2, float adam_eps, float *vis_counts, float *xys_grad_norm,
+                            float *max_2d_size, float *const *grads_out, float *losses_out);
+/* Graph statistics of msplat_cuda_train_batch: out4 = replays, captures, overflowed
+ * steps (repeated without the graph), per-intersection capacity. */
+int msplat_cuda_train_batch_stats(msplat_cuda_ctx *ctx, int64_t *out4);
 
 /* bindings.h:100-118 msplat_train_step: forward, L1 + SSIM loss, backward, Adam on the
  * six parameter groups (means, scales, quats, features_dc, features_rest, opacities --

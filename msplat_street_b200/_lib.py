@@ -85,6 +85,23 @@ class View(C.Structure):
 
 _SIGS["msplat_cuda_render_batch"] = (i32, [vp, C.c_int32, C.POINTER(View)])
 
+
+class TrainView(C.Structure):
+    """msplat_cuda_train_view (include/msplat_cuda.h): one view of a batched step."""
+    _fields_ = [
+        ("viewmat", f32 * 16), ("projmat", f32 * 16),
+        ("fx", f32), ("fy", f32), ("cx", f32), ("cy", f32),
+        ("img_height", C.c_uint32), ("img_width", C.c_uint32),
+        ("cam_pos", f32 * 3),
+        ("gt", vp),
+    ]
+
+
+_SIGS["msplat_cuda_train_batch"] = (i32, [vp, i32, vp, vp, f32, vp, vp, vp, vp, u32, u32, f32, vp, C.c_int32,
+                                          C.POINTER(TrainView), f32, i32, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp,
+                                          vp, vp])
+_SIGS["msplat_cuda_train_batch_stats"] = (i32, [vp, C.POINTER(i64)])
+
 # entry points added later in the build; bound when the library exports them
 _OPTIONAL_SIGS: dict = {}
 

@@ -258,6 +258,67 @@ class Context:
             C.byref(loss) if sync_loss else None))
         return float(loss.value) if sync_loss else None
 
+    def set_graph(self, on: bool = True) -> None:
+        """Replay a captured CUDA graph of each batched training step (train_batch)."""
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"graph", int(bool(on))))
+
+    def graph_stats(self) -> dict:
+        out = (C.c_int64 * 4)()
+        check(self._lib.msplat_cuda_train_batch_stats(self.handle, out))
+        return {"replays": out[0], "captures": out[1], "overflows": out[2], "isect_capacity": out[3]}
+
+    def train_batch(self, p: GaussianParams, adam: Optional[AdamState], views: Sequence, background,
+                    stats=None, ssim_weight: float = 0.2, degrees_to_use: Optional[int] = None,
+                    glob_scale: float = 1.0, clip_thresh: float = 0.01, grads: Optional[List[torch.Tensor]] = None,
+                    num_adam_groups: int = 6, sync_loss: bool = True):
+        """msplat_cuda_train_batch: ``views`` is a sequence of (CameraSetup, target
+        tensor) pairs trained in one step (gradients summed, one Adam step when
+        ``adam`` is given; ``adam.step`` is advanced first). ``grads`` (6 tensors in
+        parameter layout) receives the summed gradients. Returns the per-view losses
+        when ``sync_loss``."""
+        self.bind_stream()
+        deg = p.sh_degree
+        dtu = deg if degrees_to_use is None else degrees_to_use
+        tv = (_lib.TrainView * len(views))()
+        for k, (cam, gt) in enumerate(views):
+            require_cuda(gt, f"target {k}")
+            if tuple(gt.shape) != (cam.height, cam.width, 3):
+                raise ValueError(f"target {k} has shape {tuple(gt.shape)}, camera is {cam.height}x{cam.width}")
+            w = tv[k]
+            w.viewmat[:] = [float(x) for x in cam.viewmat.reshape(-1)]
+            w.projmat[:] = [float(x) for x in cam.projmat.reshape(-1)]
+            w.fx, w.fy, w.cx, w.cy = cam.fx, cam.fy, cam.cx, cam.cy
+            w.img_height, w.img_width = cam.height, cam.width
+            w.cam_pos[:] = [float(x) for x in cam.cam_pos.reshape(-1)]
+            w.gt = gt.data_ptr()
+        groups = 0
+        m1 = m2 = ss = bc2 = None
+        if adam is not None:
+            groups = num_adam_groups
+            adam.step += 1
+            s, b = adam.step_scalars()
+            ss, bc2 = s.ctypes.data, b.ctypes.data
+            m1a = (C.c_void_p * 6)(*[t.data_ptr() for t in adam.exp_avg])
+            m2a = (C.c_void_p * 6)(*[t.data_ptr() for t in adam.exp_avg_sq])
+            m1, m2 = C.cast(m1a, C.c_void_p), C.cast(m2a, C.c_void_p)
+        g = None
+        if grads is not None:
+            for t, ref in zip(grads, p.tensors()):
+                if t.shape != ref.shape:
+                    raise ValueError("gradient outputs must match the parameter shapes")
+                require_cuda(t, "gradient output")
+            ga = (C.c_void_p * 6)(*[t.data_ptr() for t in grads])
+            g = C.cast(ga, C.c_void_p)
+        vis, gn, ms = (stats if stats is not None else (None, None, None))
+        bg = _f32(background)
+        losses = np.zeros(len(views), np.float32)
+        check(self._lib.msplat_cuda_train_batch(
+            self.handle, p.n, ptr(p.means), ptr(p.scales), glob_scale, ptr(p.quats), ptr(p.features_dc),
+            ptr(p.features_rest), ptr(p.opacities), deg, dtu, clip_thresh, bg.ctypes.data, len(views), tv,
+            ssim_weight, groups, m1, m2, ss, bc2, adam.beta1 if adam else 0.9, adam.beta2 if adam else 0.999,
+            adam.eps if adam else 1e-8, ptr(vis), ptr(gn), ptr(ms), g, losses.ctypes.data if sync_loss else None))
+        return losses if sync_loss else None
+
     def loss_tensor(self) -> torch.Tensor:
         """The last train step's loss as a 0-d CUDA tensor (copied, no host sync)."""
         src = C.c_void_p()

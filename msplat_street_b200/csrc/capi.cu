@@ -16,15 +16,17 @@
 #include <string>
 
 #include "../../include/msplat_cuda.h"
-#include "kernels.h"
+#include "context.h"
 
 using namespace msplat;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-int fail(int code, const char *fmt, ...) {
+const char *msplat::last_error_text() { return g_last_error.c_str(); }
+
+int msplat::fail(int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -34,184 +36,10 @@ int fail(int code, const char *fmt, ...) {
     return code;
 }
 
-}  // namespace
-
 // Lets other translation units report through msplat_cuda_last_error().
 int msplat::report_error(int code, const char *msg) { return fail(code, "%s", msg); }
 
-namespace {
-
-#define CUDA_TRY(expr)                                                                          \
-    do {                                                                                        \
-        cudaError_t _e = (expr);                                                                \
-        if (_e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
-    } while (0)
-
-struct Buf {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-};
-
-}  // namespace
-
-// Stage timing with CUDA events on the context's stream (the reference's
-// PROFILE_STAGES, core/metal/msplat_metal.mm:29-32, drained by
-// msplat_drain_stage_times, core/metal/bindings.h:38).
-constexpr int N_STAGES = 6;
-const char *const STAGE_NAMES[N_STAGES] = {"proj_sh_fwd", "bin_sort", "rast_fwd", "loss_fwd_bwd", "rast_bwd",
-                                           "proj_sh_bwd_adam"};
-
-// Each call records its marks into one slot of a ring; a slot is read back only when
-// the ring comes round to it again (long finished by then) or on drain, so timing
-// adds no synchronisation to the calls themselves.
-constexpr int TIMER_RING = 64;
-
-struct StageTimer {
-    bool on = false;
-    int cur = 0;
-    cudaEvent_t ev[TIMER_RING][N_STAGES + 1] = {};
-    bool marked[TIMER_RING][N_STAGES + 1] = {};
-    double acc_ms[N_STAGES] = {};
-    int64_t calls[N_STAGES] = {};
-    void init() {
-        for (auto &slot : ev)
-            for (auto &e : slot)
-                if (!e) cudaEventCreate(&e);
-    }
-    void reset_marks() {
-        for (bool &m : marked[cur]) m = false;
-    }
-    void mark(int i, cudaStream_t st) {
-        if (!on) return;
-        cudaEventRecord(ev[cur][i], st);
-        marked[cur][i] = true;
-    }
-    // accumulate every consecutive pair of recorded marks of one slot
-    void collect_slot(int s) {
-        int last = -1;
-        for (int i = 0; i <= N_STAGES; i++) {
-            if (!marked[s][i]) continue;
-            if (last >= 0) {
-                cudaEventSynchronize(ev[s][i]);
-                float ms = 0.f;
-                if (cudaEventElapsedTime(&ms, ev[s][last], ev[s][i]) == cudaSuccess) {
-                    acc_ms[last] += ms;
-                    calls[last] += 1;
-                }
-            }
-            last = i;
-        }
-        for (bool &m : marked[s]) m = false;
-    }
-    // end of a call: move to the next slot, reading back the one found there
-    void collect() {
-        if (!on) return;
-        cur = (cur + 1) % TIMER_RING;
-        collect_slot(cur);
-    }
-    void drain() {
-        for (int s = 0; s < TIMER_RING; s++) collect_slot(s);
-    }
-    void destroy() {
-        for (auto &slot : ev)
-            for (auto &e : slot)
-                if (e) cudaEventDestroy(e), e = nullptr;
-    }
-};
-
-struct msplat_cuda_ctx {
-    cudaStream_t stream = nullptr;
-    bool keep_grads = false;
-    StageTimer timer;
-    // frame description
-    int n = 0, W = 0, H = 0, tiles_x = 0, tiles_y = 0;
-    int64_t n_isect = 0;
-    int sorted = 0;  // which key/value buffer pair holds the sorted result
-    // per Gaussian
-    Buf splats, radii, aabb, n_tiles, offsets, scan_part, total;
-    Buf v_xy, v_conic, v_rgb, v_opacity, v_mean3d, v_scale, v_quat;
-    // per intersection
-    Buf keys[2], vals[2], emit_gid, isect_gid, inv, slots, radix_scratch;
-    // per tile / pixel
-    Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
-    // densification and primitive scratch
-    Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md;
-    // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
-    int tstore_cap = 0;
-    Buf tstore, tcount;
-    int64_t *h_total = nullptr;  // pinned readback of the intersection count
-    int32_t *h_count = nullptr;  // pinned readback of the densified count
-    // batched render: device view descriptors, their pinned staging copy, the
-    // persistent rasterizer's work counter, and an event after the last upload
-    Buf bdesc, bcounter;
-    unsigned char *h_bdesc = nullptr;
-    size_t h_bdesc_bytes = 0;
-    cudaEvent_t bdesc_ev = nullptr;
-    bool bdesc_pending = false;
-
-    ~msplat_cuda_ctx() {
-        release();
-        timer.destroy();
-    }
-    void release() {
-        Buf *all[] = {&splats, &radii, &aabb, &n_tiles, &offsets, &scan_part, &total, &v_xy, &v_conic, &v_rgb,
-                      &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
-                      &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
-                      &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter};
-        for (Buf *b : all) {
-            if (b->ptr) cudaFree(b->ptr);
-            b->ptr = nullptr;
-            b->bytes = 0;
-        }
-        if (h_total) cudaFreeHost(h_total);
-        h_total = nullptr;
-        if (h_count) cudaFreeHost(h_count);
-        h_count = nullptr;
-        if (h_bdesc) cudaFreeHost(h_bdesc);
-        h_bdesc = nullptr;
-        h_bdesc_bytes = 0;
-        if (bdesc_ev) cudaEventDestroy(bdesc_ev);
-        bdesc_ev = nullptr;
-        bdesc_pending = false;
-    }
-};
-
-namespace {
-
-template <typename T>
-int ensure(Buf &b, size_t count, T **out) {
-    const size_t need = std::max<size_t>(count, 1) * sizeof(T);
-    if (b.bytes < need) {
-        if (b.ptr) {
-            cudaError_t e = cudaFree(b.ptr);
-            if (e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "cudaFree: %s", cudaGetErrorString(e));
-        }
-        b.ptr = nullptr;
-        b.bytes = 0;
-        const size_t bytes = need + need / 4;
-        cudaError_t e = cudaMalloc(&b.ptr, bytes);
-        if (e != cudaSuccess) {
-            b.ptr = nullptr;
-            return fail(MSPLAT_CUDA_ECUDA, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-        }
-        b.bytes = bytes;
-    }
-    *out = reinterpret_cast<T *>(b.ptr);
-    return MSPLAT_CUDA_OK;
-}
-
-#define ENSURE(buf, count, type, var) \
-    type *var = nullptr;              \
-    if (int _r = ensure<type>(buf, (size_t)(count), &var)) return _r;
-
-int ceil_log2(int v) {
-    int b = 0;
-    while ((1 << b) < v) b++;
-    return b;
-}
-
-int check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigned degree, unsigned dtu,
+int msplat::check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigned degree, unsigned dtu,
                  const float *viewmat, const float *projmat, const float *cam_pos, const float *bg) {
     if (num_points < 0) return fail(MSPLAT_CUDA_EINVAL, "num_points must be >= 0 (got %d)", num_points);
     if (W == 0 || H == 0) return fail(MSPLAT_CUDA_EINVAL, "image size must be positive (%ux%u)", W, H);
@@ -223,7 +51,7 @@ int check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigne
     return MSPLAT_CUDA_OK;
 }
 
-CamParams make_cam(const float *viewmat, const float *projmat, float fx, float fy, float cx, float cy,
+CamParams msplat::make_cam(const float *viewmat, const float *projmat, float fx, float fy, float cx, float cy,
                    unsigned H, unsigned W, int tx, int ty, float clip, unsigned degree, unsigned dtu,
                    const float *cam_pos) {
     CamParams c;
@@ -243,6 +71,8 @@ CamParams make_cam(const float *viewmat, const float *projmat, float fx, float f
     c.degrees_to_use = dtu;
     return c;
 }
+
+namespace {
 
 // Projection, binning and forward rasterization: the shared forward of render and
 // train (core/cpu/msplat_cpu.cpp:629-657). One host synchronisation reads the
@@ -349,8 +179,6 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     return MSPLAT_CUDA_OK;
 }
 
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
 // Batched forward: the stages of forward() over every (view, Gaussian) instance and
 // every (view, tile) of a batch at once. The view descriptors go to the device in
 // two uploads from pinned staging: projection/emission fields first, the raster
@@ -365,7 +193,7 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
         const int tx = (int)((w.img_width + TILE - 1) / TILE), ty = (int)((w.img_height + TILE - 1) / TILE);
         if (int r = check_camera(w.num_points, w.img_height, w.img_width, tx, ty, w.degree, w.degrees_to_use,
                                  w.viewmat, w.projmat, w.cam_pos, w.background))
-            return fail(r, "view %d: %s", v, g_last_error.c_str());
+            return fail(r, "view %d: %s", v, last_error_text());
         if (w.num_points > 0 && (!w.means3d || !w.scales || !w.quats || !w.features_dc || !w.opacities ||
                                  (w.degree > 0 && !w.features_rest)))
             return fail(MSPLAT_CUDA_EINVAL, "view %d: null Gaussian parameter pointer", v);
@@ -566,6 +394,10 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
         if (value) ctx->timer.init();
         ctx->timer.on = value != 0;
         ctx->timer.reset_marks();
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "graph")) {
+        ctx->tb.graph = value != 0;
         return MSPLAT_CUDA_OK;
     }
     return fail(MSPLAT_CUDA_EINVAL, "unknown option '%s'", name);
@@ -1028,7 +860,9 @@ int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
                         &ctx->tile_start, &ctx->tile_end, &ctx->out_img, &ctx->final_T, &ctx->final_idx,
                         &ctx->v_rendered, &ctx->loss_part, &ctx->loss, &ctx->d_flags, &ctx->d_counts,
                         &ctx->d_scratch, &ctx->k_bounds, &ctx->k_sorted, &ctx->k_box, &ctx->k_md, &ctx->tstore,
-                        &ctx->tcount};
+                        &ctx->tcount, &ctx->bdesc, &ctx->bcounter, &ctx->tb.desc, &ctx->tb.pix_img,
+                        &ctx->tb.pix_T, &ctx->tb.pix_idx, &ctx->tb.pix_v, &ctx->tb.partials, &ctx->tb.losses,
+                        &ctx->tb.counters};
     int64_t total = 0;
     for (const Buf *b : all) total += (int64_t)b->bytes;
     return total;

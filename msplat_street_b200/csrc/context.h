@@ -1,0 +1,254 @@
+// Host-side state shared by the C-ABI translation units: the context (stream, frame
+// cache, stage timer, batched-step state), device-buffer growth and error reporting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/msplat_cuda.h"
+#include "kernels.h"
+
+namespace msplat {
+
+// Records the message returned by msplat_cuda_last_error() (per thread); returns code.
+int fail(int code, const char *fmt, ...);
+const char *last_error_text();
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (expr);                                                                \
+        if (_e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+struct Buf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace msplat
+
+using msplat::Buf;
+
+// Stage timing with CUDA events on the context's stream (the reference's
+// PROFILE_STAGES, core/metal/msplat_metal.mm:29-32, drained by
+// msplat_drain_stage_times, core/metal/bindings.h:38).
+constexpr int N_STAGES = 6;
+const char *const STAGE_NAMES[N_STAGES] = {"proj_sh_fwd", "bin_sort", "rast_fwd", "loss_fwd_bwd", "rast_bwd",
+                                           "proj_sh_bwd_adam"};
+
+// Each call records its marks into one slot of a ring; a slot is read back only when
+// the ring comes round to it again (long finished by then) or on drain, so timing
+// adds no synchronisation to the calls themselves.
+constexpr int TIMER_RING = 64;
+
+struct StageTimer {
+    bool on = false;
+    int cur = 0;
+    cudaEvent_t ev[TIMER_RING][N_STAGES + 1] = {};
+    bool marked[TIMER_RING][N_STAGES + 1] = {};
+    double acc_ms[N_STAGES] = {};
+    int64_t calls[N_STAGES] = {};
+    void init() {
+        for (auto &slot : ev)
+            for (auto &e : slot)
+                if (!e) cudaEventCreate(&e);
+    }
+    void reset_marks() {
+        for (bool &m : marked[cur]) m = false;
+    }
+    void mark(int i, cudaStream_t st) {
+        if (!on) return;
+        cudaEventRecord(ev[cur][i], st);
+        marked[cur][i] = true;
+    }
+    // accumulate every consecutive pair of recorded marks of one slot
+    void collect_slot(int s) {
+        int last = -1;
+        for (int i = 0; i <= N_STAGES; i++) {
+            if (!marked[s][i]) continue;
+            if (last >= 0) {
+                cudaEventSynchronize(ev[s][i]);
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, ev[s][last], ev[s][i]) == cudaSuccess) {
+                    acc_ms[last] += ms;
+                    calls[last] += 1;
+                }
+            }
+            last = i;
+        }
+        for (bool &m : marked[s]) m = false;
+    }
+    // end of a call: move to the next slot, reading back the one found there
+    void collect() {
+        if (!on) return;
+        cur = (cur + 1) % TIMER_RING;
+        collect_slot(cur);
+    }
+    void drain() {
+        for (int s = 0; s < TIMER_RING; s++) collect_slot(s);
+    }
+    void destroy() {
+        for (auto &slot : ev)
+            for (auto &e : slot)
+                if (e) cudaEventDestroy(e), e = nullptr;
+    }
+};
+
+// State of the batched training step (msplat_cuda_train_batch): capacity-sized
+// buffers, the per-step view descriptors, and the CUDA graph of the step.
+struct TrainBatchState {
+    Buf desc;                                   // device view descriptors
+    unsigned char *h_stage[2] = {nullptr, nullptr};  // pinned staging, double-buffered
+    size_t h_stage_bytes = 0;
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};    // upload from slot k finished
+    bool stage_pending[2] = {false, false};
+    int slot = 0;
+    Buf pix_img, pix_T, pix_idx, pix_v, partials, losses, counters;
+    int64_t isect_cap = 0;  // elements the per-intersection buffers hold
+    int tile_cap = 0;       // key bits are sized for this many tiles
+    void *h_out = nullptr;  // pinned readback: overflow flag, count, per-view losses
+    size_t h_out_bytes = 0;
+    // graph mode (option "graph"): the step from projection to Adam is captured once
+    // per shape and replayed; the descriptors are uploaded before each replay
+    bool graph = false;
+    cudaStream_t gstream = nullptr;
+    cudaEvent_t ev_in = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> key;
+    int64_t replays = 0, captures = 0, overflows = 0;
+
+    void release() {
+        Buf *all[] = {&desc, &pix_img, &pix_T, &pix_idx, &pix_v, &partials, &losses, &counters};
+        for (Buf *b : all) {
+            if (b->ptr) cudaFree(b->ptr);
+            b->ptr = nullptr;
+            b->bytes = 0;
+        }
+        for (int k = 0; k < 2; k++) {
+            if (h_stage[k]) cudaFreeHost(h_stage[k]);
+            h_stage[k] = nullptr;
+            if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+            stage_ev[k] = nullptr;
+            stage_pending[k] = false;
+        }
+        h_stage_bytes = 0;
+        if (h_out) cudaFreeHost(h_out);
+        h_out = nullptr;
+        h_out_bytes = 0;
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+        if (ev_in) cudaEventDestroy(ev_in);
+        ev_in = nullptr;
+        if (gstream) cudaStreamDestroy(gstream);
+        gstream = nullptr;
+        isect_cap = 0;
+        tile_cap = 0;
+    }
+};
+
+struct msplat_cuda_ctx {
+    cudaStream_t stream = nullptr;
+    TrainBatchState tb;
+    bool keep_grads = false;
+    StageTimer timer;
+    // frame description
+    int n = 0, W = 0, H = 0, tiles_x = 0, tiles_y = 0;
+    int64_t n_isect = 0;
+    int sorted = 0;  // which key/value buffer pair holds the sorted result
+    // per Gaussian
+    Buf splats, radii, aabb, n_tiles, offsets, scan_part, total;
+    Buf v_xy, v_conic, v_rgb, v_opacity, v_mean3d, v_scale, v_quat;
+    // per intersection
+    Buf keys[2], vals[2], emit_gid, isect_gid, inv, slots, radix_scratch;
+    // per tile / pixel
+    Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
+    // densification and primitive scratch
+    Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md;
+    // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
+    int tstore_cap = 0;
+    Buf tstore, tcount;
+    int64_t *h_total = nullptr;  // pinned readback of the intersection count
+    int32_t *h_count = nullptr;  // pinned readback of the densified count
+    // batched render: device view descriptors, their pinned staging copy, the
+    // persistent rasterizer's work counter, and an event after the last upload
+    Buf bdesc, bcounter;
+    unsigned char *h_bdesc = nullptr;
+    size_t h_bdesc_bytes = 0;
+    cudaEvent_t bdesc_ev = nullptr;
+    bool bdesc_pending = false;
+
+    ~msplat_cuda_ctx() {
+        release();
+        timer.destroy();
+    }
+    void release() {
+        Buf *all[] = {&splats, &radii, &aabb, &n_tiles, &offsets, &scan_part, &total, &v_xy, &v_conic, &v_rgb,
+                      &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
+                      &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
+                      &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
+                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter};
+        for (Buf *b : all) {
+            if (b->ptr) cudaFree(b->ptr);
+            b->ptr = nullptr;
+            b->bytes = 0;
+        }
+        tb.release();  // its graph refers to the buffers just freed
+        if (h_total) cudaFreeHost(h_total);
+        h_total = nullptr;
+        if (h_count) cudaFreeHost(h_count);
+        h_count = nullptr;
+        if (h_bdesc) cudaFreeHost(h_bdesc);
+        h_bdesc = nullptr;
+        h_bdesc_bytes = 0;
+        if (bdesc_ev) cudaEventDestroy(bdesc_ev);
+        bdesc_ev = nullptr;
+        bdesc_pending = false;
+    }
+};
+
+namespace msplat {
+
+template <typename T>
+inline int ensure(Buf &b, size_t count, T **out) {
+    const size_t need = std::max<size_t>(count, 1) * sizeof(T);
+    if (b.bytes < need) {
+        if (b.ptr) {
+            cudaError_t e = cudaFree(b.ptr);
+            if (e != cudaSuccess) return fail(MSPLAT_CUDA_ECUDA, "cudaFree: %s", cudaGetErrorString(e));
+        }
+        b.ptr = nullptr;
+        b.bytes = 0;
+        const size_t bytes = need + need / 4;
+        cudaError_t e = cudaMalloc(&b.ptr, bytes);
+        if (e != cudaSuccess) {
+            b.ptr = nullptr;
+            return fail(MSPLAT_CUDA_ECUDA, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+        }
+        b.bytes = bytes;
+    }
+    *out = reinterpret_cast<T *>(b.ptr);
+    return MSPLAT_CUDA_OK;
+}
+
+#define ENSURE(buf, count, type, var) \
+    type *var = nullptr;              \
+    if (int _r = ensure<type>(buf, (size_t)(count), &var)) return _r;
+
+inline int ceil_log2(int v) {
+    int b = 0;
+    while ((1 << b) < v) b++;
+    return b;
+}
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigned degree, unsigned dtu,
+                 const float *viewmat, const float *projmat, const float *cam_pos, const float *bg);
+CamParams make_cam(const float *viewmat, const float *projmat, float fx, float fy, float cx, float cy, unsigned H,
+                   unsigned W, int tx, int ty, float clip, unsigned degree, unsigned dtu, const float *cam_pos);
+
+}  // namespace msplat
