@@ -333,6 +333,44 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line))
 
 
+def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_step: int = 8):
+    """Mixed-resolution street training (16 cameras at 640x480 / 1024x512 / 1280x720 /
+    1600x1060): the plain per-view step, the batched step (views_per_step views per
+    step, one launch per stage) without and with CUDA-graph replay. Each arm trains
+    ``views`` views after ``warmup_views`` from the same start (before the first
+    densification), wall-clock timed between device synchronisations."""
+    import torch
+    from msplat_street_b200 import workloads
+    from msplat_street_b200.backend import Context
+
+    out = {"views_per_step": views_per_step, "views_timed": views,
+           "resolutions": [list(r) for r in workloads.BATCH_RESOLUTIONS]}
+    arms = (("plain", False, False), ("batched", True, False), ("batched_graph", True, True))
+    for name, batched, graph in arms:
+        ctx = Context()
+        tr, _ = workloads.street_batched(ctx, views_per_step=views_per_step, graph=graph, batched=batched)
+        per = views_per_step if batched else 1
+        for _ in range(max(warmup_views // per, 3)):
+            tr.step()
+        torch.cuda.synchronize()
+        steps = views // per
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            tr.step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"views_per_s": steps * per / dt, "steps_per_s": steps / dt, "ms_per_step": dt / steps * 1e3,
+                     "gaussians": tr.splat_count}
+        if graph:
+            out[name]["graph"] = ctx.graph_stats()
+        del tr
+        ctx.close()
+        torch.cuda.empty_cache()
+    for name in ("batched", "batched_graph"):
+        out[name]["views_per_s_vs_plain"] = out[name]["views_per_s"] / out["plain"]["views_per_s"]
+    return out
+
+
 def serving_report(dev, seconds: float, rates=(200.0, 1000.0, 5000.0)):
     """Render serving: 32 resident scenes (Gaussian counts log-uniform in [5e4, 3e6],
     SH degree 3, FP32) under a 150 GB budget; Poisson request streams at each rate for

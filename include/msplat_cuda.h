@@ -54,12 +54,17 @@ msplat_cuda_ctx *msplat_cuda_default_ctx(void);
 int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
 /* Options: "keep_grads" (1 = keep per-Gaussian gradients for msplat_cuda_frame);
  * "graph" (1 = msplat_cuda_train_batch replays a captured CUDA graph of its step);
+ * "raster_variant" (0..7: the rasterizer's shared-memory staging sizes, see
+ * msplat_cuda_raster_variant; results do not depend on it, speed does);
  * "stage_timing" (1 = time the stages, see msplat_cuda_drain_stage_times);
  * "store_transmittance" (K > 0: the forward stores each pixel's transmittance before
  * its first K contributions and the backward reads them instead of recovering T by
  * division, which the reference does (msplat_cpu.cpp:996-997); pixels with more
  * contributions fall back to division; 0 = off, the default). */
 int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
+/* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
+ * backward round, and the backward reduction's sub-batch. Returns the variant count. */
+int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, int32_t *bwd_sub);
 /* Bytes of device memory the context's caches hold. */
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx);
 

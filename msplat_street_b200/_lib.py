@@ -101,6 +101,8 @@ _SIGS["msplat_cuda_train_batch"] = (i32, [vp, i32, vp, vp, f32, vp, vp, vp, vp, 
                                           C.POINTER(TrainView), f32, i32, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp,
                                           vp, vp])
 _SIGS["msplat_cuda_train_batch_stats"] = (i32, [vp, C.POINTER(i64)])
+_SIGS["msplat_cuda_raster_variant"] = (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32)])
 
 # entry points added later in the build; bound when the library exports them
 _OPTIONAL_SIGS: dict = {}

@@ -258,6 +258,11 @@ class Context:
             C.byref(loss) if sync_loss else None))
         return float(loss.value) if sync_loss else None
 
+    def set_raster_variant(self, v: int) -> None:
+        """Rasterizer staging variant (see raster_variants()); results do not depend on it."""
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"raster_variant", int(v)))
+        self.raster_variant = int(v)
+
     def set_graph(self, on: bool = True) -> None:
         """Replay a captured CUDA graph of each batched training step (train_batch)."""
         check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"graph", int(bool(on))))

@@ -173,7 +173,7 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
         ra.tcap = ctx->tstore_cap;
     }
     ctx->timer.mark(2, st);
-    launch_raster_fwd(ra, st);
+    launch_raster_fwd(ra, st, ctx->raster_variant);
     ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
@@ -338,7 +338,7 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     CUDA_TRY(cudaEventRecord(ctx->bdesc_ev, st));
     ctx->bdesc_pending = true;
     ctx->timer.mark(2, st);
-    launch_raster_fwd_batch(d, T, d_counter, st);
+    launch_raster_fwd_batch(d, T, d_counter, st, ctx->raster_variant);
     ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
@@ -394,6 +394,12 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
         if (value) ctx->timer.init();
         ctx->timer.on = value != 0;
         ctx->timer.reset_marks();
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "raster_variant")) {
+        if (value < 0 || value >= N_RASTER_VARIANTS)
+            return fail(MSPLAT_CUDA_EINVAL, "raster_variant must be 0..%d", N_RASTER_VARIANTS - 1);
+        ctx->raster_variant = (int)value;
         return MSPLAT_CUDA_OK;
     }
     if (!std::strcmp(name, "graph")) {
@@ -534,7 +540,7 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     rb.slots = slots;
     rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
     rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
-    launch_raster_bwd(rb, st);
+    launch_raster_bwd(rb, st, ctx->raster_variant);
     ctx->timer.mark(5, st);
 
     BackwardArgs ba;
@@ -643,7 +649,7 @@ int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const floa
     rb.slots = slots;
     rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
     rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
-    launch_raster_bwd(rb, st);
+    launch_raster_bwd(rb, st, ctx->raster_variant);
     BackwardArgs ba;
     std::memset(&ba, 0, sizeof ba);
     ba.n = n;
@@ -850,6 +856,15 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
 }
 
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
+
+int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, int32_t *bwd_sub) {
+    if (v >= 0 && v < N_RASTER_VARIANTS) {
+        if (fwd_batch) *fwd_batch = RASTER_VARIANTS[v].fwd_batch;
+        if (bwd_batch) *bwd_batch = RASTER_VARIANTS[v].bwd_batch;
+        if (bwd_sub) *bwd_sub = RASTER_VARIANTS[v].bwd_sub;
+    }
+    return N_RASTER_VARIANTS;
+}
 
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
     if (!ctx) return -1;

@@ -152,6 +152,7 @@ struct TrainBatchState {
 
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
+    int raster_variant = 0;  // option "raster_variant": index into RASTER_VARIANTS
     TrainBatchState tb;
     bool keep_grads = false;
     StageTimer timer;

@@ -65,7 +65,19 @@ struct RasterArgs {
     int32_t *tcount;
     int tcap;
 };
-void launch_raster_fwd(const RasterArgs &a, cudaStream_t st);
+// Rasterizer staging variants, chosen at run time (an autotuner times them): the
+// Gaussians staged in shared memory per forward round and per backward round, and
+// the backward's reduction sub-batch. Every variant computes the same images and
+// gradients (staging changes no arithmetic); variant 0 is the default.
+struct RasterVariant {
+    int fwd_batch, bwd_batch, bwd_sub;
+};
+constexpr int N_RASTER_VARIANTS = 8;
+constexpr RasterVariant RASTER_VARIANTS[N_RASTER_VARIANTS] = {
+    {128, 64, 4}, {256, 64, 8}, {256, 64, 4}, {256, 32, 4}, {128, 32, 4}, {64, 32, 4}, {256, 128, 4}, {128, 16, 4}};
+inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v : 0; }
+
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
 
 // A batch of views rendered by one projection, one sort and one persistent raster
 // launch. Instances (view, Gaussian) and tiles (view, tile) are numbered globally,
@@ -95,7 +107,7 @@ void launch_project_batch(const BatchDesc &d, int total, cudaStream_t st);
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
                             const int64_t *offsets, const BatchDesc &d, uint64_t *keys, uint32_t *vals,
                             int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
-void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st);
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant = 0);
 
 struct RasterBwdArgs {
     int W, H, tiles_x, tiles_y;
@@ -109,7 +121,7 @@ struct RasterBwdArgs {
     const float *tstore;  // stored-transmittance mode, as RasterArgs (null = divide)
     const int32_t *tcount;
 };
-void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st);
+void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant = 0);
 
 struct SsimArgs {
     int W, H;
@@ -169,7 +181,7 @@ struct BackwardBatchArgs {
 };
 void launch_backward_adam_batch(const BackwardBatchArgs &a, cudaStream_t st);
 void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
-                             cudaStream_t st);
+                             cudaStream_t st, int variant = 0);
 void launch_ssim_loss_batch(const SsimArgs *d_views, const int *d_boff, int n_views, int *d_counter, cudaStream_t st);
 
 struct DensifyArgs {

@@ -19,7 +19,13 @@
 // fused backward/Adam kernel.
 //
 // Compiled with -fmad=false: the alpha and transmittance cut-offs must fall exactly
-// where the reference's do.
+// where the reference's do. The backward's gradient arithmetic, which no decision
+// depends on, uses explicit fused multiply-adds.
+//
+// Staging sizes are template parameters (RASTER_VARIANTS, picked at run time by the
+// autotuner); no variant changes any arithmetic or summation order, so all of them
+// give the same bits. A persistent form of each pass pulls (view, tile) work items
+// for batches of views.
 #include <algorithm>
 
 #include "common.cuh"
@@ -27,12 +33,12 @@
 
 namespace msplat {
 
-constexpr int FWD_BATCH = TILE_PIX;
-constexpr int BWD_BATCH = 64;
 constexpr int BWD_WARPS = TILE_PIX / 32;
 
 // One 16x16 tile: `tile` indexes tile_start / tile_end (a global tile id in a batch),
 // (tx, ty) is its position in its view. Every thread of the block must call it.
+// FB: Gaussians staged in shared memory per round (at most one per thread).
+template <int FB>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
                                                 float4 *s1, float4 *s2) {
     int lx, ly;
@@ -51,17 +57,17 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     const size_t npix = (size_t)a.W * a.H;
     const size_t pid = inside ? (size_t)py * a.W + px : 0;
     int stored = 0;  // contributions seen (stored-transmittance mode)
-    for (int b0 = start; b0 < end; b0 += FWD_BATCH) {
+    for (int b0 = start; b0 < end; b0 += FB) {
         if (__syncthreads_count(done) == TILE_PIX) break;
         const int k = b0 + threadIdx.x;
-        if (k < end) {
+        if (threadIdx.x < FB && k < end) {
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
             s0[threadIdx.x] = rec[0];
             s1[threadIdx.x] = rec[1];
             s2[threadIdx.x] = rec[2];
         }
         __syncthreads();
-        const int cnt = min(FWD_BATCH, end - b0);
+        const int cnt = min(FB, end - b0);
         for (int j = 0; j < cnt && !done; j++) {
             const float4 A = s0[j], C = s2[j];
             if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
@@ -99,70 +105,88 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     o[2] = clamp01(a.bg[2] * T + cb);
 }
 
+template <int FB>
 __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
-    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
+    __shared__ float4 s0[FB], s1[FB], s2[FB];
     const int tile = blockIdx.x;
-    raster_fwd_tile(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
+    raster_fwd_tile<FB>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
 // camera, resolution and output): every block pulls global tile ids from a counter
 // until none are left. A tile's image equals what the per-view kernel renders: the
 // same list (the batch sort keeps each tile's order) and the same code.
+template <int FB>
 __global__ void __launch_bounds__(TILE_PIX) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
-    __shared__ float4 s0[FWD_BATCH], s1[FWD_BATCH], s2[FWD_BATCH];
-    __shared__ int s_tile;
+    __shared__ float4 s0[FB], s1[FB], s2[FB];
+    __shared__ int s_tile, s_lt;
+    __shared__ RasterArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
     const int total_tiles = d.tile_off[d.n_views];  // read on the device: the launch is graph-capturable
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+        __syncthreads();  // the previous tile's shared state is no longer read
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(counter, 1);
+            s_tile = t;
+            if (t < total_tiles) {
+                const int v = find_view(d.tile_off, d.n_views, t);
+                s_args = d.raster[v];
+                s_lt = t - d.tile_off[v];
+            }
+        }
         __syncthreads();
-        const int t = s_tile;
-        __syncthreads();  // everyone has read s_tile before thread 0 overwrites it
+        const int t = s_tile, lt = s_lt;
         if (t >= total_tiles) break;
-        const int v = find_view(d.tile_off, d.n_views, t);
-        const RasterArgs &a = d.raster[v];
-        const int lt = t - d.tile_off[v];
-        raster_fwd_tile(a, t, lt % a.tiles_x, lt / a.tiles_x, s0, s1, s2);
+        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2);
     }
 }
 
-// Resident blocks on the whole GPU (computed once, thread-safe static).
-int raster_fwd_batch_grid() {
-    static const int grid = [] {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_fwd_batch_kernel, TILE_PIX, 0);
-        return std::max(1, sms * std::max(per_sm, 1));
-    }();
-    return grid;
+// Resident blocks of a kernel on the whole GPU.
+template <typename K>
+int resident_grid(K kernel, size_t smem) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE_PIX, smem);
+    return std::max(1, sms * std::max(per_sm, 1));
+}
+
+template <int FB>
+void fwd_batch_launch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st) {
+    static const int grid = resident_grid(raster_fwd_batch_kernel<FB>, 0);  // once per variant, thread-safe
+    const int g = tiles_hint > 0 ? std::min(grid, tiles_hint) : grid;
+    raster_fwd_batch_kernel<FB><<<g, TILE_PIX, 0, st>>>(d, d_counter);
 }
 
 // tiles_hint: the batch's tile count when the host knows it (caps the grid), else 0
-void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st) {
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant) {
     cudaMemsetAsync(d_counter, 0, sizeof(int), st);
-    const int grid = tiles_hint > 0 ? std::min(raster_fwd_batch_grid(), tiles_hint) : raster_fwd_batch_grid();
-    raster_fwd_batch_kernel<<<grid, TILE_PIX, 0, st>>>(d, d_counter);
+    switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
+        case 64: fwd_batch_launch<64>(d, tiles_hint, d_counter, st); break;
+        case 256: fwd_batch_launch<256>(d, tiles_hint, d_counter, st); break;
+        default: fwd_batch_launch<128>(d, tiles_hint, d_counter, st); break;
+    }
 }
 
 // Per-warp reduction of the 9 gradient values over the warp's 32 pixels, done in
-// sub-batches of 8 Gaussians: each lane stores its contributions to a transposed
+// sub-batches of SB Gaussians: each lane stores its contributions to a transposed
 // buffer (one row of 32 lane values per output), then each lane sums whole rows with
-// float4 loads. 72 outputs x 31 adds per sub-batch, in a fixed lane order.
-constexpr int SUB = 8;
-constexpr int SUB_OUT = SUB * 9;  // outputs per sub-batch
-constexpr int PB_STRIDE = 36;     // floats per row: 32 lanes + pad, keeps float4 rows conflict-free
+// float4 loads. 9 SB outputs x 31 adds per sub-batch, in a fixed lane order. BB
+// Gaussians are staged in shared memory per round.
+constexpr int PB_STRIDE = 36;  // floats per row: 32 lanes + pad, keeps float4 rows conflict-free
 
-size_t raster_bwd_smem() {
-    return sizeof(float4) * 3 * BWD_BATCH + sizeof(float) * BWD_WARPS * BWD_BATCH * 9 +
-           sizeof(float) * BWD_WARPS * SUB_OUT * PB_STRIDE + 16;
+template <int BB, int SB>
+constexpr size_t raster_bwd_smem() {
+    return sizeof(float4) * 3 * BB + sizeof(float) * BWD_WARPS * BB * 9 + sizeof(float) * BWD_WARPS * SB * 9 * PB_STRIDE +
+           16;
 }
 
 // One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
 // global tile id in a batch), (tx, ty) is its position in its view. Every thread of
 // the block calls it; it ends with the block's shared memory free for reuse.
+template <int BB, int SB>
 __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
                                                 int &kmax) {
+    constexpr int BWD_BATCH = BB, SUB = SB, SUB_OUT = SB * 9;
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
     float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][9]
     float *pbuf = red + BWD_WARPS * BWD_BATCH * 9;            // [BWD_WARPS][SUB_OUT][PB_STRIDE]
@@ -245,24 +269,30 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                             const float rawr = B.z, rawg = B.w, rawb = C.x;
                             const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),
                                         cb = fmaxf(rawb + 0.5f, 0.f);
+                            // gradient arithmetic (no decision depends on it) uses fused
+                            // multiply-adds; the reference's values are met within the
+                            // gradient tolerance, not bit for bit
                             const float nra = -ra;
-                            const float ir = -br * ra + nra * tbr, ig = -bgc * ra + nra * tbg, ib = -bb * ra + nra * tbb;
-                            const float orr = cr * T + ir, og = cg * T + ig, ob = cb * T + ib;
-                            const float va = orr * vr + og * vg + ob * vb;
-                            br = cr * fac + br;
-                            bgc = cg * fac + bgc;
-                            bb = cb * fac + bb;
+                            const float ir = __fmaf_rn(-br, ra, nra * tbr), ig = __fmaf_rn(-bgc, ra, nra * tbg),
+                                        ib = __fmaf_rn(-bb, ra, nra * tbb);
+                            const float orr = __fmaf_rn(cr, T, ir), og = __fmaf_rn(cg, T, ig),
+                                        ob = __fmaf_rn(cb, T, ib);
+                            const float va = __fmaf_rn(orr, vr, __fmaf_rn(og, vg, ob * vb));
+                            br = __fmaf_rn(cr, fac, br);
+                            bgc = __fmaf_rn(cg, fac, bgc);
+                            bb = __fmaf_rn(cb, fac, bb);
                             if (rawr + 0.5f >= 0.f) g[5] = fac * vr;
                             if (rawg + 0.5f >= 0.f) g[6] = fac * vg;
                             if (rawb + 0.5f >= 0.f) g[7] = fac * vb;
                             if (alpha < 0.999f) {
                                 const float vs = -alpha * va;
-                                g[2] = 0.5f * vs * dx * dx;
-                                g[3] = 0.5f * vs * dx * dy;
-                                g[4] = 0.5f * vs * dy * dy;
-                                g[0] = vs * (A.z * dx + A.w * dy);
-                                g[1] = vs * (A.w * dx + B.x * dy);
-                                g[8] = -vs * (1.f - op);
+                                const float hv = 0.5f * vs;
+                                g[2] = hv * dx * dx;
+                                g[3] = hv * dx * dy;
+                                g[4] = hv * dy * dy;
+                                g[0] = vs * __fmaf_rn(A.z, dx, A.w * dy);
+                                g[1] = vs * __fmaf_rn(A.w, dx, B.x * dy);
+                                g[8] = __fmaf_rn(vs, op, -vs);  // -vs * (1 - op)
                             }
                         }
                     }
@@ -311,67 +341,111 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         for (int c = 0; c < 9; c++) a.slots[(size_t)k * 9 + c] = 0.f;
 }
 
-__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_kernel(RasterBwdArgs a) {
+template <int BB, int SB>
+__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_kernel(RasterBwdArgs a) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
     const int tile = blockIdx.x;
-    raster_bwd_tile(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
+    raster_bwd_tile<BB, SB>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
 }
 
 // Persistent backward over the tiles of a batch of views, pulling global tile ids
 // from a counter (the forward's counterpart, raster_fwd_batch_kernel).
-__global__ void __launch_bounds__(TILE_PIX, 2) raster_bwd_batch_kernel(const RasterBwdArgs *views,
+template <int BB, int SB>
+__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_batch_kernel(const RasterBwdArgs *views,
                                                                         const int *tile_off, int n_views,
                                                                         int *counter) {
     extern __shared__ __align__(16) float4 smem4[];
-    __shared__ int kmax, s_tile;
+    __shared__ int kmax, s_tile, s_lt;
+    __shared__ RasterBwdArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
     const int total_tiles = tile_off[n_views];
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(counter, 1);
+            s_tile = t;
+            if (t < total_tiles) {
+                const int v = find_view(tile_off, n_views, t);
+                s_args = views[v];
+                s_lt = t - tile_off[v];
+            }
+        }
         __syncthreads();
-        const int t = s_tile;
-        __syncthreads();  // everyone has read s_tile before thread 0 overwrites it
+        const int t = s_tile, lt = s_lt;
         if (t >= total_tiles) break;
-        const int v = find_view(tile_off, n_views, t);
-        const RasterBwdArgs a = views[v];
-        const int lt = t - tile_off[v];
-        raster_bwd_tile(a, t, lt % a.tiles_x, lt / a.tiles_x, smem4, kmax);
-        __syncthreads();  // the tile's shared buffers are free before the next tile stages
+        raster_bwd_tile<BB, SB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, smem4, kmax);
+        __syncthreads();  // the tile's shared state is free before thread 0 claims the next tile
     }
 }
 
-void launch_raster_fwd(const RasterArgs &a, cudaStream_t st) {
+template <int FB>
+void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
+    raster_fwd_kernel<FB><<<T, TILE_PIX, 0, st>>>(a);
+}
+
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    raster_fwd_kernel<<<T, TILE_PIX, 0, st>>>(a);
+    switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
+        case 64: fwd_launch<64>(a, T, st); break;
+        case 256: fwd_launch<256>(a, T, st); break;
+        default: fwd_launch<128>(a, T, st); break;
+    }
+}
+
+template <int BB, int SB>
+void bwd_launch(const RasterBwdArgs &a, int T, cudaStream_t st) {
+    constexpr size_t smem = raster_bwd_smem<BB, SB>();
+    static const bool attr = [] {  // once per variant, thread-safe
+        cudaFuncSetAttribute(raster_bwd_kernel<BB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return true;
+    }();
+    (void)attr;
+    raster_bwd_kernel<BB, SB><<<T, TILE_PIX, smem, st>>>(a);
+}
+
+template <int BB, int SB>
+void bwd_batch_launch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
+                      cudaStream_t st) {
+    constexpr size_t smem = raster_bwd_smem<BB, SB>();
+    static const int grid = [] {
+        cudaFuncSetAttribute(raster_bwd_batch_kernel<BB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        return resident_grid(raster_bwd_batch_kernel<BB, SB>, smem);
+    }();
+    raster_bwd_batch_kernel<BB, SB><<<grid, TILE_PIX, smem, st>>>(d_views, d_tile_off, n_views, d_counter);
+}
+
+// The backward variants' (staged batch, reduction sub-batch) pairs, dispatched to
+// their template instances.
+#define MSPLAT_BWD_VARIANTS(X) X(64, 4) X(64, 8) X(32, 4) X(128, 4) X(16, 4)
+
+void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    const RasterVariant &v = RASTER_VARIANTS[variant_index(variant)];
+#define X(bb, sb)                                    \
+    if (v.bwd_batch == bb && v.bwd_sub == sb) {      \
+        bwd_launch<bb, sb>(a, T, st);                \
+        return;                                      \
+    }
+    MSPLAT_BWD_VARIANTS(X)
+#undef X
+    bwd_launch<64, 4>(a, T, st);
 }
 
 void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
-                             cudaStream_t st) {
+                             cudaStream_t st, int variant) {
     if (n_views <= 0) return;
-    const size_t smem = raster_bwd_smem();
-    static const int grid = [smem] {
-        cudaFuncSetAttribute(raster_bwd_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_bwd_batch_kernel, TILE_PIX, smem);
-        return sms * (per_sm > 0 ? per_sm : 1);
-    }();
     cudaMemsetAsync(d_counter, 0, sizeof(int), st);
-    raster_bwd_batch_kernel<<<grid, TILE_PIX, smem, st>>>(d_views, d_tile_off, n_views, d_counter);
-}
-
-void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st) {
-    const int T = a.tiles_x * a.tiles_y;
-    if (T <= 0) return;
-    static bool attr_set = false;
-    const size_t smem = raster_bwd_smem();
-    if (!attr_set) {
-        cudaFuncSetAttribute(raster_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
+    const RasterVariant &v = RASTER_VARIANTS[variant_index(variant)];
+#define X(bb, sb)                                                      \
+    if (v.bwd_batch == bb && v.bwd_sub == sb) {                        \
+        bwd_batch_launch<bb, sb>(d_views, d_tile_off, n_views, d_counter, st); \
+        return;                                                        \
     }
-    raster_bwd_kernel<<<T, TILE_PIX, smem, st>>>(a);
+    MSPLAT_BWD_VARIANTS(X)
+#undef X
+    bwd_batch_launch<64, 4>(d_views, d_tile_off, n_views, d_counter, st);
 }
 
 }  // namespace msplat

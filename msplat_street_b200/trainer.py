@@ -98,14 +98,23 @@ class Dataset:
 
 class GaussianTrainer:
     """3D Gaussian Splatting trainer on the B200 backend (reference: GaussianTrainer,
-    python/bindings.cpp:217-427)."""
+    python/bindings.cpp:217-427).
+
+    ``views_per_step`` > 1 (or ``batched``) trains that many views per step with the
+    batched step (msplat_cuda_train_batch: gradients summed over the views, one Adam
+    step); ``graph`` replays a captured CUDA graph of that step."""
 
     def __init__(self, dataset: Dataset, config: TrainingConfig, init: Optional[GaussianParams] = None,
-                 context: Optional[Context] = None, device: str = "cuda"):
+                 context: Optional[Context] = None, device: str = "cuda", views_per_step: int = 1,
+                 batched: bool = False, graph: bool = False):
         self.cfg = config
         self.ds = dataset
         self.ctx = context or Context()
         self.device = device
+        self.views_per_step = max(1, int(views_per_step))
+        self.batched = batched or self.views_per_step > 1 or graph
+        if graph:
+            self.ctx.set_graph(True)
         if init is None:
             pts = torch.from_numpy(dataset.points).to(device)
             init = self.ctx.init_gaussians(pts, torch.from_numpy(dataset.colors), seed=42,
@@ -207,18 +216,32 @@ class GaussianTrainer:
     def step(self, sync_loss: bool = False, target: Optional[torch.Tensor] = None) -> TrainingStats:
         """One training iteration (GaussianTrainer::step, python/bindings.cpp:261-284)."""
         t0 = time.perf_counter()
-        ci = self._next_camera()
-        view = self.ds.views[ci]
-        gt = target if target is not None else self._targets[ci]
-        if gt is None:
-            raise ValueError(f"view {ci} has no target image")
         n = self.num_active
         if self.stats is None:
             self.stats = tuple(torch.zeros(n, dtype=torch.float32, device=self.device) for _ in range(3))
         adam = self._adam_view()
-        self.last_loss = self.ctx.train_step(self.params, adam, view.setup, self.bg, gt, self.stats,
-                                             ssim_weight=self.cfg.ssim_weight,
-                                             degrees_to_use=self.degrees_to_use(), sync_loss=sync_loss)
+        if self.batched:
+            if target is not None:
+                raise ValueError("a batched step takes its targets from the dataset")
+            views = []
+            for _ in range(self.views_per_step):
+                ci = self._next_camera()
+                if self._targets[ci] is None:
+                    raise ValueError(f"view {ci} has no target image")
+                views.append((self.ds.views[ci].setup, self._targets[ci]))
+            losses = self.ctx.train_batch(self.params, adam, views, self.bg, self.stats,
+                                          ssim_weight=self.cfg.ssim_weight, degrees_to_use=self.degrees_to_use(),
+                                          sync_loss=sync_loss)
+            self.last_loss = float(np.mean(losses)) if losses is not None else None
+        else:
+            ci = self._next_camera()
+            view = self.ds.views[ci]
+            gt = target if target is not None else self._targets[ci]
+            if gt is None:
+                raise ValueError(f"view {ci} has no target image")
+            self.last_loss = self.ctx.train_step(self.params, adam, view.setup, self.bg, gt, self.stats,
+                                                 ssim_weight=self.cfg.ssim_weight,
+                                                 degrees_to_use=self.degrees_to_use(), sync_loss=sync_loss)
         self.adam_step = adam.step
         self.current_step += 1
         self._schedulers_step(self.current_step)

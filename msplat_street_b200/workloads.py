@@ -49,3 +49,42 @@ def street_plain(ctx: Context, gt_n: int = STREET_GT_N, init_n: int = STREET_INI
     tr = GaussianTrainer(ds, street_config(iterations), context=ctx, device=device)
     tr._targets = targets
     return tr, targets
+
+
+# --- batching: the street scene and schedule, 16 cameras of mixed resolutions ---------
+
+BATCH_RESOLUTIONS = ((640, 480), (1024, 512), (1280, 720), (1600, 1060))
+
+
+def street_mixed_setups(seed: int = 4):
+    """The 16 street poses, each at a resolution drawn uniformly (seeded) from
+    BATCH_RESOLUTIONS, focal length half the width (the plain config's 90 degree
+    horizontal field of view)."""
+    from .camera import prepare_cam
+    poses = scenes.street_camera_poses(STREET_VIEWS, seed=2)
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in poses:
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(len(BATCH_RESOLUTIONS)))]
+        out.append(prepare_cam(p, w, h, 0.5 * w, 0.5 * w, w / 2.0, h / 2.0))
+    return poses, out
+
+
+def street_batched(ctx: Context, views_per_step: int = 8, graph: bool = True, batched: bool = True,
+                   gt_n: int = STREET_GT_N, init_n: int = STREET_INIT_N, iterations: int = 2000,
+                   device: str = "cuda"):
+    """(trainer, targets) for the batching config: street_plain's scene, start and
+    schedule with the mixed-resolution cameras; ``views_per_step`` views per step
+    through the batched step (``batched=False``: the plain per-view step)."""
+    gt = scenes.street_scene(0, gt_n)
+    poses, setups = street_mixed_setups()
+    pg = GaussianParams.from_numpy(gt, device)
+    targets = [ctx.render(pg, s, BACKGROUND).clone() for s in setups]
+    del pg
+    pts, rgb = scenes.jittered_init_points(gt, init_n, seed=3)
+    ds = Dataset.from_setups(setups, [None] * len(setups), pts, rgb, poses)
+    tr = GaussianTrainer(ds, street_config(iterations), context=ctx, device=device,
+                         views_per_step=views_per_step if batched else 1, batched=batched,
+                         graph=graph and batched)
+    tr._targets = targets
+    return tr, targets
