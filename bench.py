@@ -293,6 +293,14 @@ def run_ours(args, world, rank, local):
         except Exception as e:
             serve = {"error": f"{type(e).__name__}: {e}"}
 
+    # ---- batched multi-view training vs the plain per-view step (rank 0) ----
+    batching = None
+    if rank == 0 and not args.no_batching:
+        try:
+            batching = batching_report(dev)
+        except Exception as e:
+            batching = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if world == 1:
@@ -323,6 +331,7 @@ def run_ours(args, world, rank, local):
             "cpu_baseline": cpu,
             "differentiation": diff,
             "serving": serve,
+            "batching": batching,
         }
         if serve and "rates" in serve:
             hi = serve["rates"].get("1000") or next(iter(serve["rates"].values()))
@@ -368,6 +377,51 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
         torch.cuda.empty_cache()
     for name in ("batched", "batched_graph"):
         out[name]["views_per_s_vs_plain"] = out[name]["views_per_s"] / out["plain"]["views_per_s"]
+    out["small"] = small_batching_report(views_per_step)
+    return out
+
+
+def small_batching_report(views_per_step: int = 8, views: int = 960):
+    """Where one view cannot fill the GPU: a 10 k-Gaussian scene (the small plain
+    config's distributions), 16 cameras at 256 x 256 on a 3 m sphere (256 tiles each,
+    fewer than the resident blocks of one wave). Plain per-view steps vs batched steps
+    with graph replay; wall-clock views/s."""
+    import torch
+    from msplat_street_b200 import scenes
+    from msplat_street_b200.backend import Context, GaussianParams
+    from msplat_street_b200.trainer import Dataset, GaussianTrainer, TrainingConfig
+    from msplat_street_b200.workloads import BACKGROUND
+
+    from msplat_street_b200.camera import prepare_cam
+    rng = np.random.default_rng(12)
+    poses = [scenes.sphere_pose(rng, 3.0) for _ in range(16)]
+    f = 0.5 * 256 / np.tan(np.radians(30.0))
+    setups = [prepare_cam(p, 256, 256, f, f, 128.0, 128.0) for p in poses]
+    gt = GaussianParams.from_numpy(scenes.small_scene(1))
+    ctx0 = Context()
+    targets = [ctx0.render(gt, s, BACKGROUND).clone() for s in setups]
+    init = scenes.small_scene(0)
+    out = {"scene": "10k Gaussians, 16 views 256x256"}
+    for name, batched, graph in (("plain", False, False), ("batched_graph", True, True)):
+        ctx = Context()
+        ds = Dataset.from_setups(setups, [None] * 16, np.zeros((1, 3), np.float32), np.zeros((1, 3), np.uint8),
+                                 poses)
+        cfg = TrainingConfig(iterations=100000, warmup_length=10 ** 9)  # no densification in the window
+        tr = GaussianTrainer(ds, cfg, init=GaussianParams.from_numpy(init), context=ctx,
+                             views_per_step=views_per_step if batched else 1, batched=batched, graph=graph)
+        tr._targets = targets
+        per = views_per_step if batched else 1
+        for _ in range(max(32 // per, 3)):
+            tr.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(views // per):
+            tr.step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"views_per_s": (views // per) * per / dt}
+        ctx.close()
+    out["batched_graph"]["views_per_s_vs_plain"] = out["batched_graph"]["views_per_s"] / out["plain"]["views_per_s"]
     return out
 
 
@@ -509,6 +563,7 @@ def main(argv=None):
     ap.add_argument("--quick", action="store_true", help="device-timed pass only (no e2e, no CPU baseline)")
     ap.add_argument("--serving-seconds", type=float, default=1.0,
                     help="length of each Poisson request stream in the serving report (0 = skip)")
+    ap.add_argument("--no-batching", action="store_true", help="skip the batched-training report")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

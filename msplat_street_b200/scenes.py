@@ -118,11 +118,17 @@ def jittered_init_points(gt: Gaussians, n: int, seed: int = 3, sigma: float = 0.
 
 # --- serving: cameras on a sphere of radius 5 facing the centre ---
 
-def sphere_camera(rng: np.random.Generator, width: int, height: int, radius: float = 5.0,
-                  f_scale: float = 1.0) -> CameraSetup:
+def sphere_pose(rng: np.random.Generator, radius: float = 5.0) -> np.ndarray:
+    """Camera-to-world pose at a uniform point of a sphere of ``radius``, facing its centre."""
     v = rng.normal(size=3)
     v /= np.linalg.norm(v)
-    eye = radius * v
     up = (0.0, 1.0, 0.0) if abs(v[1]) < 0.95 else (1.0, 0.0, 0.0)
+    return look_at(radius * v, (0.0, 0.0, 0.0), up)
+
+
+def sphere_camera(rng: np.random.Generator, width: int, height: int, radius: float = 5.0,
+                  f_scale: float = 1.0) -> CameraSetup:
+    """A pinhole camera (60 degree horizontal field of view) at sphere_pose."""
+    pose = sphere_pose(rng, radius)
     f = f_scale * 0.5 * width / math.tan(math.radians(30.0))
-    return prepare_cam(look_at(eye, (0.0, 0.0, 0.0), up), width, height, f, f, width / 2.0, height / 2.0)
+    return prepare_cam(pose, width, height, f, f, width / 2.0, height / 2.0)
