@@ -119,10 +119,12 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     pa.radii = radii;
     pa.aabb = aabb;
     pa.n_tiles = n_tiles;
+    DepthScratch ds;
+    if (int r = ensure_depth_scratch(ctx, n, ds)) return r;
     ctx->timer.reset_marks();
     ctx->timer.mark(0, st);
     launch_project(pa, st);
-    scan_exclusive<int64_t>(n_tiles, offsets, n, d_total, scan_part, st);
+    launch_depth_offsets(n, splats, n_tiles, ds, offsets, d_total, scan_part, st);
     CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t n_isect = *ctx->h_total;
@@ -130,8 +132,8 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
         return fail(MSPLAT_CUDA_EOVERFLOW, "more than 2^31 tile intersections (%lld); lower the resolution",
                     (long long)n_isect);
     ctx->n_isect = n_isect;
-    ENSURE(ctx->keys[0], n_isect, uint64_t, k0);
-    ENSURE(ctx->keys[1], n_isect, uint64_t, k1);
+    ENSURE(ctx->keys[0], n_isect, uint32_t, k0);
+    ENSURE(ctx->keys[1], n_isect, uint32_t, k1);
     ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
     ENSURE(ctx->vals[1], n_isect, uint32_t, v1);
     ENSURE(ctx->emit_gid, n_isect, int32_t, emit_gid);
@@ -141,10 +143,9 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
 
     ctx->timer.mark(1, st);
     launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y, k0, v0, emit_gid, st);
-    uint64_t *kk[2] = {k0, k1};
+    uint32_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
-    const int key_bits = 32 + ceil_log2(std::max(T, 1));
-    const int cur = radix_sort_pairs(kk, vv, (int)n_isect, key_bits, rscratch, st);
+    const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);
     ctx->sorted = cur;
     launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
     launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
@@ -238,6 +239,8 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     ENSURE(ctx->tile_start, T, int32_t, tile_start);
     ENSURE(ctx->tile_end, T, int32_t, tile_end);
     if (!ctx->h_total) CUDA_TRY(cudaMallocHost(&ctx->h_total, sizeof(int64_t)));
+    DepthScratch ds;
+    if (int r = ensure_depth_scratch(ctx, n, ds)) return r;
 
     unsigned char *h = ctx->h_bdesc;
     ProjectArgs *hp = reinterpret_cast<ProjectArgs *>(h + o_proj);
@@ -289,7 +292,7 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     CUDA_TRY(cudaMemcpyAsync(d_desc, h, o_ras, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(d_desc + o_inst, h + o_inst, bytes - o_inst, cudaMemcpyHostToDevice, st));
     launch_project_batch(d, n, st);
-    scan_exclusive<int64_t>(n_tiles, offsets, n, d_total, scan_part, st);
+    launch_depth_offsets(n, splats, n_tiles, ds, offsets, d_total, scan_part, st);
     CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t n_isect = *ctx->h_total;
@@ -297,23 +300,22 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
         return fail(MSPLAT_CUDA_EOVERFLOW, "more than 2^31 tile intersections in the batch (%lld)",
                     (long long)n_isect);
     ctx->n_isect = n_isect;
-    ENSURE(ctx->keys[0], n_isect, uint64_t, k0);
-    ENSURE(ctx->keys[1], n_isect, uint64_t, k1);
+    ENSURE(ctx->keys[0], n_isect, uint32_t, k0);
+    ENSURE(ctx->keys[1], n_isect, uint32_t, k1);
     ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
     ENSURE(ctx->vals[1], n_isect, uint32_t, v1);
     ENSURE(ctx->emit_gid, n_isect, int32_t, emit_gid);
     ENSURE(ctx->isect_gid, n_isect, int32_t, isect_gid);
-    ENSURE(ctx->inv, n_isect, int32_t, inv);
     ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
 
     ctx->timer.mark(1, st);
     launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, d, k0, v0, emit_gid, st);
-    uint64_t *kk[2] = {k0, k1};
+    uint32_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
-    const int cur = radix_sort_pairs(kk, vv, (int)n_isect, 32 + ceil_log2(std::max(T, 1)), rscratch, st);
+    const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);
     ctx->sorted = cur;
     launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
-    launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
+    launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, nullptr, st);  // render only: no inverse map
 
     for (int v = 0; v < nv; v++) {
         const msplat_cuda_view &w = views[v];
@@ -877,7 +879,8 @@ int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
                         &ctx->d_scratch, &ctx->k_bounds, &ctx->k_sorted, &ctx->k_box, &ctx->k_md, &ctx->tstore,
                         &ctx->tcount, &ctx->bdesc, &ctx->bcounter, &ctx->tb.desc, &ctx->tb.pix_img,
                         &ctx->tb.pix_T, &ctx->tb.pix_idx, &ctx->tb.pix_v, &ctx->tb.partials, &ctx->tb.losses,
-                        &ctx->tb.counters};
+                        &ctx->tb.counters, &ctx->dkeys[0], &ctx->dkeys[1], &ctx->dvals[0], &ctx->dvals[1],
+                        &ctx->dcounts, &ctx->doff};
     int64_t total = 0;
     for (const Buf *b : all) total += (int64_t)b->bytes;
     return total;

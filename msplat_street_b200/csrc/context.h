@@ -172,6 +172,8 @@ struct msplat_cuda_ctx {
     // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
     int tstore_cap = 0;
     Buf tstore, tcount;
+    // depth order of the Gaussians (or batch instances) before key emission
+    Buf dkeys[2], dvals[2], dcounts, doff;
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
     int32_t *h_count = nullptr;  // pinned readback of the densified count
     // batched render: device view descriptors, their pinned staging copy, the
@@ -191,7 +193,8 @@ struct msplat_cuda_ctx {
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter};
+                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
+                      &dvals[0], &dvals[1], &dcounts, &doff};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);
             b->ptr = nullptr;
@@ -251,5 +254,24 @@ int check_camera(int num_points, unsigned H, unsigned W, int tx, int ty, unsigne
                  const float *viewmat, const float *projmat, const float *cam_pos, const float *bg);
 CamParams make_cam(const float *viewmat, const float *projmat, float fx, float fy, float cx, float cy, unsigned H,
                    unsigned W, int tx, int ty, float clip, unsigned degree, unsigned dtu, const float *cam_pos);
+
+// Depth-order scratch for n Gaussians (or batch instances) from the context's buffers.
+inline int ensure_depth_scratch(msplat_cuda_ctx *ctx, int64_t n, DepthScratch &s) {
+    ENSURE(ctx->dkeys[0], n, uint32_t, k0);
+    ENSURE(ctx->dkeys[1], n, uint32_t, k1);
+    ENSURE(ctx->dvals[0], n, uint32_t, v0);
+    ENSURE(ctx->dvals[1], n, uint32_t, v1);
+    ENSURE(ctx->dcounts, n, int32_t, counts);
+    ENSURE(ctx->doff, n, int64_t, off);
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)std::max<int64_t>(n, 1)), unsigned char, rs);
+    s.keys[0] = k0;
+    s.keys[1] = k1;
+    s.vals[0] = v0;
+    s.vals[1] = v1;
+    s.counts = counts;
+    s.off_sorted = off;
+    s.radix_scratch = rs;
+    return 0;
+}
 
 }  // namespace msplat

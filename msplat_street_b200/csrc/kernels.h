@@ -40,13 +40,26 @@ int scan_blocks(int n);
 template <typename TO>
 void scan_exclusive(const int32_t *in, TO *out, int n, TO *d_total, TO *partials, cudaStream_t st);
 
+// Depth order of n Gaussians (stable) and their emission offsets in that order:
+// offsets[g] = tiles of every Gaussian before g by (depth, index); *d_total = all.
+struct DepthScratch {
+    uint32_t *keys[2], *vals[2];  // n each
+    int32_t *counts;              // n
+    int64_t *off_sorted;          // n
+    void *radix_scratch;          // radix_scratch_bytes(n)
+};
+void launch_depth_offsets(int n, const Splat *splats, const int32_t *n_tiles, DepthScratch &s, int64_t *offsets,
+                          int64_t *d_total, int64_t *scan_part, cudaStream_t st);
+// Emission: key = tile id (global tile id in a batch), value = emission index.
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
-                      int tiles_x, int tiles_y, uint64_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
+                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
 size_t radix_scratch_bytes(int n);
 // d_n / d_T (optional): device-side counts capping the host-side capacities n / T
 int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
                      const int *d_n = nullptr);
-void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
+int radix_sort_pairs32(uint32_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
+                       const int *d_n = nullptr);
+void launch_tile_ranges(const uint32_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
                         const int *d_n = nullptr, const int *d_T = nullptr);
 void launch_isect_map(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid, int32_t *inv,
                       cudaStream_t st, const int *d_n = nullptr);
@@ -105,7 +118,7 @@ __device__ __forceinline__ int find_view(const int *off, int n_views, int g) {
 
 void launch_project_batch(const BatchDesc &d, int total, cudaStream_t st);
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                            const int64_t *offsets, const BatchDesc &d, uint64_t *keys, uint32_t *vals,
+                            const int64_t *offsets, const BatchDesc &d, uint32_t *keys, uint32_t *vals,
                             int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
 void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant = 0);
 

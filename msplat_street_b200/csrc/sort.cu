@@ -1,12 +1,13 @@
-// Tile-intersection binning: exclusive scan, key emission, stable LSD radix sort and
-// tile ranges.
+// Tile-intersection binning: exclusive scan, depth order, key emission, stable LSD
+// radix sort and tile ranges.
 //
 // The reference builds per-tile lists ordered by (depth bits, Gaussian index)
-// (bin_and_sort, core/cpu/msplat_cpu.cpp:505-567). Here every (Gaussian, tile) pair
-// gets one 64-bit key (tile id << 32) | depth bits, written in Gaussian order at
-// offsets from an exclusive scan of tiles-per-Gaussian. A STABLE radix sort over the
-// significant bits then yields, within each tile, ascending depth with ties in
-// Gaussian order -- exactly the reference's order -- without a per-tile sort or any
+// (bin_and_sort, core/cpu/msplat_cpu.cpp:505-567). Here the visible Gaussians are
+// sorted by depth bits once (stable, so ties keep index order); every (Gaussian, tile)
+// pair is then emitted in that order at offsets from an exclusive scan of
+// tiles-per-Gaussian, keyed by its tile id alone. A STABLE radix sort over the
+// ceil(log2 tiles) tile bits then yields, within each tile, ascending depth with ties
+// in Gaussian order -- exactly the reference's order -- without a per-tile sort or any
 // cap on a tile's list. The sort carries the emission index as its value; the map
 // kernel turns it into the Gaussian id per sorted slot and the inverse permutation
 // that the backward pass uses to reduce per-Gaussian gradients deterministically.
@@ -105,10 +106,42 @@ __global__ void scan_apply_kernel(const int32_t *in, int n, const TO *partials, 
 
 int scan_blocks(int n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 
+// Small inputs: one 1024-thread block walks the array in chunks of 4096 with a
+// running carry (one launch instead of three).
+constexpr int SCAN_SMALL = 16384, SMALL_ITEMS = 4;
+
+template <typename TO>
+__global__ void __launch_bounds__(1024) scan_small_kernel(const int32_t *in, int n, TO *out, TO *total) {
+    __shared__ TO ws[33];
+    TO carry = 0;
+    for (int base = 0; base < n; base += 1024 * SMALL_ITEMS) {
+        const int i0 = base + threadIdx.x * SMALL_ITEMS;
+        TO v[SMALL_ITEMS], s = 0;
+#pragma unroll
+        for (int j = 0; j < SMALL_ITEMS; j++) {
+            v[j] = i0 + j < n ? (TO)in[i0 + j] : TO(0);
+            s += v[j];
+        }
+        TO tot;
+        TO ex = block_exclusive_scan<TO>(s, ws, tot) + carry;
+#pragma unroll
+        for (int j = 0; j < SMALL_ITEMS; j++) {
+            if (i0 + j < n) out[i0 + j] = ex;
+            ex += v[j];
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
 template <typename TO>
 void scan_exclusive(const int32_t *in, TO *out, int n, TO *d_total, TO *partials, cudaStream_t st) {
     if (n <= 0) {
         if (d_total) cudaMemsetAsync(d_total, 0, sizeof(TO), st);
+        return;
+    }
+    if (n <= SCAN_SMALL) {
+        scan_small_kernel<TO><<<1, 1024, 0, st>>>(in, n, out, d_total);
         return;
     }
     const int nb = scan_blocks(n);
@@ -120,7 +153,47 @@ template void scan_exclusive<int32_t>(const int32_t *, int32_t *, int, int32_t *
 template void scan_exclusive<int64_t>(const int32_t *, int64_t *, int, int64_t *, int64_t *, cudaStream_t);
 
 // ---------------------------------------------------------------------------------
-// Key emission: one thread per Gaussian, tiles in row-major order of its rectangle.
+// Depth order and key emission.
+//
+// The reference orders each tile's list by (depth bits, Gaussian index). Here the
+// Gaussians are first sorted by depth bits, stably (ties keep index order), and each
+// one's intersections are emitted at offsets from a scan of tile counts taken in that
+// order; a stable sort of the emitted entries by tile id alone then leaves every tile's
+// entries in (depth, index) order. The per-intersection sort needs only ceil(log2
+// tiles) key bits (2 passes up to 65,536 tiles) instead of 32 more depth bits.
+
+// Depth keys: the float bits of the depth, which for the positive depths of visible
+// Gaussians order like the numbers; Gaussians with no tiles go last.
+__global__ void depth_keys_kernel(int n, const Splat *splats, const int32_t *n_tiles, uint32_t *keys, uint32_t *vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keys[i] = n_tiles[i] > 0 ? __float_as_uint(splats[i].depth) : 0xffffffffu;
+    vals[i] = (uint32_t)i;
+}
+
+__global__ void gather_counts_kernel(int n, const uint32_t *order, const int32_t *n_tiles, int32_t *cnt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) cnt[r] = n_tiles[order[r]];
+}
+
+__global__ void scatter_offsets_kernel(int n, const uint32_t *order, const int64_t *off_sorted, int64_t *offsets) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) offsets[order[r]] = off_sorted[r];
+}
+
+void launch_depth_offsets(int n, const Splat *splats, const int32_t *n_tiles, DepthScratch &s, int64_t *offsets,
+                          int64_t *d_total, int64_t *scan_part, cudaStream_t st) {
+    if (n <= 0) {
+        cudaMemsetAsync(d_total, 0, sizeof(int64_t), st);
+        return;
+    }
+    const int nb = (n + 255) / 256;
+    depth_keys_kernel<<<nb, 256, 0, st>>>(n, splats, n_tiles, s.keys[0], s.vals[0]);
+    const int cur = radix_sort_pairs32(s.keys, s.vals, n, 32, s.radix_scratch, st);
+    gather_counts_kernel<<<nb, 256, 0, st>>>(n, s.vals[cur], n_tiles, s.counts);
+    scan_exclusive<int64_t>(s.counts, s.off_sorted, n, d_total, scan_part, st);
+    scatter_offsets_kernel<<<nb, 256, 0, st>>>(n, s.vals[cur], s.off_sorted, offsets);
+}
 
 __device__ __forceinline__ void rect_of(const Splat &s, float ax, float ay, int tx, int ty, int &x0, int &y0, int &x1,
                                         int &y1) {
@@ -132,26 +205,65 @@ __device__ __forceinline__ void rect_of(const Splat &s, float ax, float ay, int 
     y1 = min(max(0, (int)(ccy + rry + 1)), ty);
 }
 
+// Emits the intersections of each thread's Gaussian: the tiles of its rectangle
+// [x0, x1) x [y0, y1) in row-major order at emission indices e0, e0 + 1, ..., key =
+// base + tile id, value = emission index. Rectangles of up to SMALL_RECT tiles are
+// written by their own thread; larger ones by the whole warp, lane l writing entries
+// l, l + 32, ..., so the stores of the big (near-camera) Gaussians coalesce. Every
+// lane of the warp must call it. cap: buffer capacity (entries at or past it dropped).
+constexpr int SMALL_RECT = 8;
+
+__device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y1, int tiles_x, uint32_t base,
+                                          int64_t e0, int gid, int64_t cap, uint32_t *keys, uint32_t *vals,
+                                          int32_t *emit_gid) {
+    const int w = x1 - x0, cnt = ok ? w * (y1 - y0) : 0;
+    if (cnt > 0 && cnt <= SMALL_RECT) {
+        int64_t e = e0;
+        for (int y = y0; y < y1; y++)
+            for (int x = x0; x < x1 && e < cap; x++, e++) {
+                keys[e] = base + (uint32_t)(y * tiles_x + x);
+                vals[e] = (uint32_t)e;
+                emit_gid[e] = gid;
+            }
+    }
+    unsigned big = __ballot_sync(0xffffffffu, cnt > SMALL_RECT);
+    const int lane = threadIdx.x & 31;
+    while (big) {  // warp-uniform
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int sw = __shfl_sync(0xffffffffu, w, src), sc = __shfl_sync(0xffffffffu, cnt, src);
+        const int sx0 = __shfl_sync(0xffffffffu, x0, src), sy0 = __shfl_sync(0xffffffffu, y0, src);
+        const int stx = __shfl_sync(0xffffffffu, tiles_x, src), sg = __shfl_sync(0xffffffffu, gid, src);
+        const uint32_t sb = __shfl_sync(0xffffffffu, base, src);
+        const int64_t se = __shfl_sync(0xffffffffu, (long long)e0, src);
+        for (int j = lane; j < sc; j += 32) {
+            const int64_t e = se + j;
+            if (e >= cap) break;
+            const int yy = sy0 + j / sw, xx = sx0 + j % sw;
+            keys[e] = sb + (uint32_t)(yy * stx + xx);
+            vals[e] = (uint32_t)e;
+            emit_gid[e] = sg;
+        }
+    }
+}
+
 __global__ void emit_keys_kernel(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                                 const int64_t *offsets, int tiles_x, int tiles_y, uint64_t *keys, uint32_t *vals,
+                                 const int64_t *offsets, int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals,
                                  int32_t *emit_gid) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || n_tiles[i] <= 0) return;
-    const Splat s = splats[i];
-    int x0, y0, x1, y1;
-    rect_of(s, aabb[2 * i], aabb[2 * i + 1], tiles_x, tiles_y, x0, y0, x1, y1);
-    const uint64_t db = (uint64_t)__float_as_uint(s.depth);
-    int64_t e = offsets[i];
-    for (int y = y0; y < y1; y++)
-        for (int x = x0; x < x1; x++, e++) {
-            keys[e] = ((uint64_t)(y * tiles_x + x) << 32) | db;
-            vals[e] = (uint32_t)e;
-            emit_gid[e] = i;
-        }
+    const bool ok = i < n && n_tiles[i] > 0;
+    int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+    int64_t e0 = 0;
+    if (ok) {
+        const Splat s = splats[i];
+        rect_of(s, aabb[2 * i], aabb[2 * i + 1], tiles_x, tiles_y, x0, y0, x1, y1);
+        e0 = offsets[i];
+    }
+    emit_rect(ok, x0, y0, x1, y1, tiles_x, 0u, e0, i, INT64_MAX, keys, vals, emit_gid);
 }
 
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
-                      int tiles_x, int tiles_y, uint64_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st) {
+                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st) {
     if (n <= 0) return;
     emit_keys_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, n_tiles, offsets, tiles_x, tiles_y, keys, vals,
                                                       emit_gid);
@@ -161,28 +273,26 @@ void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32
 // view's first global tile added, so one stable sort orders every view's tiles at
 // once and each tile's list is the one the single-view sort gives.
 __global__ void emit_keys_batch_kernel(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                                       const int64_t *offsets, const BatchDesc d, uint64_t *keys, uint32_t *vals,
+                                       const int64_t *offsets, const BatchDesc d, uint32_t *keys, uint32_t *vals,
                                        int32_t *emit_gid, int64_t cap) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n || n_tiles[g] <= 0) return;
-    const int v = find_view(d.inst_off, d.n_views, g);
-    const int tiles_x = d.tiles_x[v], tiles_y = d.tiles_y[v];
-    const uint64_t base = (uint64_t)d.tile_off[v];
-    const Splat s = splats[g];
-    int x0, y0, x1, y1;
-    rect_of(s, aabb[2 * g], aabb[2 * g + 1], tiles_x, tiles_y, x0, y0, x1, y1);
-    const uint64_t db = (uint64_t)__float_as_uint(s.depth);
-    int64_t e = offsets[g];
-    for (int y = y0; y < y1; y++)
-        for (int x = x0; x < x1 && e < cap; x++, e++) {  // cap: buffer capacity (graph mode)
-            keys[e] = ((base + (uint64_t)(y * tiles_x + x)) << 32) | db;
-            vals[e] = (uint32_t)e;
-            emit_gid[e] = g;
-        }
+    const bool ok = g < n && n_tiles[g] > 0;
+    int x0 = 0, y0 = 0, x1 = 0, y1 = 0, tiles_x = 0;
+    uint32_t base = 0;
+    int64_t e0 = 0;
+    if (ok) {
+        const int v = find_view(d.inst_off, d.n_views, g);
+        tiles_x = d.tiles_x[v];
+        base = (uint32_t)d.tile_off[v];
+        const Splat s = splats[g];
+        rect_of(s, aabb[2 * g], aabb[2 * g + 1], tiles_x, d.tiles_y[v], x0, y0, x1, y1);
+        e0 = offsets[g];
+    }
+    emit_rect(ok, x0, y0, x1, y1, tiles_x, base, e0, g, cap, keys, vals, emit_gid);
 }
 
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                            const int64_t *offsets, const BatchDesc &d, uint64_t *keys, uint32_t *vals,
+                            const int64_t *offsets, const BatchDesc &d, uint32_t *keys, uint32_t *vals,
                             int32_t *emit_gid, cudaStream_t st, int64_t cap) {
     if (n <= 0) return;
     emit_keys_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, n_tiles, offsets, d, keys, vals,
@@ -190,7 +300,8 @@ void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const
 }
 
 // ---------------------------------------------------------------------------------
-// Stable LSD radix sort of (u64 key, u32 value) by key bits [0, key_bits).
+// Stable LSD radix sort of (key, u32 value) pairs by key bits [0, key_bits), for
+// 32- and 64-bit keys.
 
 constexpr int RADIX = 256;
 constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32, SORT_ITEMS = 8;
@@ -200,49 +311,65 @@ constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per war
 int radix_blocks(int n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
 // d_n (may be null): a device-side count that caps n (capacity-bounded launches)
-__global__ void radix_hist_kernel(const uint64_t *keys, int n, const int *d_n, int shift, uint32_t mask,
-                                  uint32_t *counts, int nb) {
+template <typename K>
+__global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shift, uint32_t mask, uint32_t *counts,
+                                  int nb) {
     __shared__ uint32_t h[RADIX];
     if (d_n) n = min(n, *d_n);
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int base = blockIdx.x * SORT_TILE;
+    int dig[SORT_ITEMS];
+#pragma unroll
+    for (int j = 0; j < SORT_ITEMS; j++) {  // independent loads first
+        const int k = base + j * SORT_THREADS + threadIdx.x;
+        dig[j] = k < n ? (int)((keys[k] >> shift) & mask) : RADIX;
+    }
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
-        const int k = base + j * SORT_THREADS + threadIdx.x;
-        const bool ok = k < n;
-        const int d = ok ? (int)((keys[k] >> shift) & mask) : RADIX;
+        const int d = dig[j];
         const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+        if (d < RADIX && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
     }
     __syncthreads();
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) counts[(size_t)i * nb + blockIdx.x] = h[i];
 }
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
-__global__ void radix_scatter_kernel(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout, int n,
+template <typename K>
+__global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout, uint32_t *vout, int n,
                                      const int *d_n, int shift, uint32_t mask, const int32_t *offs, int nb) {
+    // The block's keys are first ranked and placed in shared memory in digit order
+    // (a block-local stable multisplit), then written out so that consecutive threads
+    // write consecutive entries of each digit's run: coalesced global stores.
     __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
-    __shared__ uint32_t gbase[RADIX];
+    __shared__ uint32_t gbase[RADIX], bstart[RADIX + 1];
+    __shared__ uint32_t ws[33];
+    __shared__ K skey[SORT_TILE];
+    __shared__ uint32_t sval[SORT_TILE];
     if (d_n) n = min(n, *d_n);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
-    __syncthreads();
-    uint64_t key[SORT_ITEMS];
+    K key[SORT_ITEMS];
     uint32_t val[SORT_ITEMS], rank[SORT_ITEMS];
     int dig[SORT_ITEMS];
     const int base = blockIdx.x * SORT_TILE + warp * WARP_KEYS;
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; r++) {  // independent loads first
+        const int k = base + r * 32 + lane;
+        const bool ok = k < n;
+        key[r] = ok ? kin[k] : K(0);
+        val[r] = ok ? vin[k] : 0u;
+        dig[r] = ok ? (int)((key[r] >> shift) & mask) : RADIX;
+    }
+    __syncthreads();
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; r++) {
-        const int k = base + r * 32 + lane;
-        const bool ok = k < n;
-        key[r] = ok ? kin[k] : 0ull;
-        val[r] = ok ? vin[k] : 0u;
-        const int d = ok ? (int)((key[r] >> shift) & mask) : RADIX;
-        dig[r] = d;
+        const int d = dig[r];
+        const bool ok = d < RADIX;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = ok ? wcnt[warp][d] : 0u;
         rank[r] = before + (uint32_t)__popc(peers & lt);
@@ -251,25 +378,39 @@ __global__ void radix_scatter_kernel(const uint64_t *kin, const uint32_t *vin, u
         __syncwarp();
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < RADIX; d += blockDim.x) {
-        uint32_t run = 0;
+    // per digit: exclusive prefix over warps, then over digits (block-local starts)
+    uint32_t tot = 0;
+    if (threadIdx.x < RADIX) {
+        const int d = threadIdx.x;
 #pragma unroll
         for (int w = 0; w < SORT_WARPS; w++) {
             const uint32_t t = wcnt[w][d];
-            wcnt[w][d] = run;
-            run += t;
+            wcnt[w][d] = tot;
+            tot += t;
         }
     }
+    uint32_t btot;
+    const uint32_t ex = block_exclusive_scan<uint32_t>(threadIdx.x < RADIX ? tot : 0u, ws, btot);
+    if (threadIdx.x < RADIX) bstart[threadIdx.x] = ex;
+    if (threadIdx.x == 0) bstart[RADIX] = btot;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; r++) {
-        const int k = base + r * 32 + lane;
-        if (k < n) {
-            const int d = dig[r];
-            const uint32_t pos = gbase[d] + wcnt[warp][d] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+        const int d = dig[r];
+        if (d < RADIX) {
+            const uint32_t lp = bstart[d] + wcnt[warp][d] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = val[r];
         }
+    }
+    __syncthreads();
+    const int valid = (int)bstart[RADIX];
+    for (int i = threadIdx.x; i < valid; i += blockDim.x) {
+        const K kk = skey[i];
+        const int d = (int)((kk >> shift) & mask);
+        const uint32_t pos = gbase[d] + ((uint32_t)i - bstart[d]);
+        kout[pos] = kk;
+        vout[pos] = sval[i];
     }
 }
 
@@ -282,8 +423,8 @@ size_t radix_scratch_bytes(int n) {
 // Sorts (k[0], v[0]) using (k[1], v[1]) as the ping-pong buffers; returns the index
 // (0 or 1) of the buffer pair holding the result. With d_n, n is a capacity and the
 // count is read on the device (no host round trip; every pass runs).
-int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
-                     const int *d_n) {
+template <typename K>
+int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
     if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
     const int nb = radix_blocks(n);
     const size_t cnt = (size_t)RADIX * nb;
@@ -294,21 +435,32 @@ int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *
     for (int shift = 0; shift < key_bits; shift += 8) {
         const int bits = key_bits - shift < 8 ? key_bits - shift : 8;  // digits above key_bits are ignored
         const uint32_t mask = (1u << bits) - 1u;
-        radix_hist_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
-                                                       reinterpret_cast<uint32_t *>(counts), nb);
+        radix_hist_kernel<K><<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
+                                                          reinterpret_cast<uint32_t *>(counts), nb);
         scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift, mask,
-                                                          offs, nb);
+        radix_scatter_kernel<K><<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift,
+                                                             mask, offs, nb);
         cur ^= 1;
     }
     return cur;
 }
 
-// ---------------------------------------------------------------------------------
-// Tile ranges by binary search (empty tiles get start == end == the running count,
-// as the reference's prefix sums give), and the per-slot Gaussian id / inverse map.
+int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
+                     const int *d_n) {
+    return radix_sort_impl<uint64_t>(k, v, n, key_bits, scratch, st, d_n);
+}
 
-__global__ void tile_ranges_kernel(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end,
+int radix_sort_pairs32(uint32_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
+                       const int *d_n) {
+    return radix_sort_impl<uint32_t>(k, v, n, std::min(key_bits, 32), scratch, st, d_n);
+}
+
+// ---------------------------------------------------------------------------------
+// Tile ranges by binary search over the sorted tile ids (empty tiles get start ==
+// end == the running count, as the reference's prefix sums give), and the per-slot
+// Gaussian id / inverse map.
+
+__global__ void tile_ranges_kernel(const uint32_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end,
                                    const int *d_n, const int *d_T) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (d_n) n = min(n, *d_n);
@@ -317,13 +469,15 @@ __global__ void tile_ranges_kernel(const uint64_t *keys, int n, int T, int32_t *
     int lo = 0, hi = n;  // first position whose tile id >= t
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if ((int)(keys[mid] >> 32) < t) lo = mid + 1;
+        if ((int)keys[mid] < t) lo = mid + 1;
         else hi = mid;
     }
     if (t < T) tile_start[t] = lo;
     if (t > 0) tile_end[t - 1] = lo;
 }
 
+// inv (may be null, render-only frames): emission index -> sorted position, for the
+// backward's per-Gaussian reduction
 __global__ void isect_map_kernel(const uint32_t *sorted_e, int n, const int32_t *emit_gid, int32_t *isect_gid,
                                  int32_t *inv, const int *d_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -331,10 +485,10 @@ __global__ void isect_map_kernel(const uint32_t *sorted_e, int n, const int32_t 
     if (k >= n) return;
     const uint32_t e = sorted_e[k];
     isect_gid[k] = emit_gid[e];
-    inv[e] = k;
+    if (inv) inv[e] = k;
 }
 
-void launch_tile_ranges(const uint64_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
+void launch_tile_ranges(const uint32_t *keys, int n, int T, int32_t *tile_start, int32_t *tile_end, cudaStream_t st,
                         const int *d_n, const int *d_T) {
     tile_ranges_kernel<<<(T + 1 + 255) / 256, 256, 0, st>>>(keys, n, T, tile_start, tile_end, d_n, d_T);
 }

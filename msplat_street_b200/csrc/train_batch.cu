@@ -82,7 +82,7 @@ struct StepPtrs {
     float *aabb;
     int64_t *offsets, *scan_part, *total;
     int32_t *tile_start, *tile_end;
-    uint64_t *k[2];
+    uint32_t *k[2];
     uint32_t *v[2];
     int32_t *emit_gid, *isect_gid, *inv;
     float *slots;
@@ -92,6 +92,7 @@ struct StepPtrs {
     double *partials;
     float *losses;
     int *counters;
+    DepthScratch depth;  // depth order of the instances
 };
 
 struct Sizes {
@@ -154,8 +155,8 @@ int ensure_buffers(msplat_cuda_ctx *ctx, const Sizes &sz, int64_t isect_cap, int
     ENSURE(ctx->total, 1, int64_t, total);
     ENSURE(ctx->tile_start, sz.tiles, int32_t, tile_start);
     ENSURE(ctx->tile_end, sz.tiles, int32_t, tile_end);
-    ENSURE(ctx->keys[0], isect_cap, uint64_t, k0);
-    ENSURE(ctx->keys[1], isect_cap, uint64_t, k1);
+    ENSURE(ctx->keys[0], isect_cap, uint32_t, k0);
+    ENSURE(ctx->keys[1], isect_cap, uint32_t, k1);
     ENSURE(ctx->vals[0], isect_cap, uint32_t, v0);
     ENSURE(ctx->vals[1], isect_cap, uint32_t, v1);
     ENSURE(ctx->emit_gid, isect_cap, int32_t, emit_gid);
@@ -171,15 +172,19 @@ int ensure_buffers(msplat_cuda_ctx *ctx, const Sizes &sz, int64_t isect_cap, int
     ENSURE(tb.losses, nv, float, losses);
     ENSURE(tb.counters, N_COUNTERS, int, counters);
     P = StepPtrs{desc, splats, radii, n_tiles, aabb, offsets, scan_part, total, tile_start, tile_end, {k0, k1},
-                 {v0, v1}, emit_gid, isect_gid, inv, slots, rscratch, img, T, v_img, idx, partials, losses, counters};
+                 {v0, v1}, emit_gid, isect_gid, inv, slots, rscratch, img, T, v_img, idx, partials, losses, counters,
+                 {}};
     // capacities as the buffers now stand (ENSURE keeps headroom)
-    const int64_t cap_k = (int64_t)std::min({ctx->keys[0].bytes / 8, ctx->keys[1].bytes / 8, ctx->vals[0].bytes / 4,
+    const int64_t cap_k = (int64_t)std::min({ctx->keys[0].bytes / 4, ctx->keys[1].bytes / 4, ctx->vals[0].bytes / 4,
                                              ctx->vals[1].bytes / 4, ctx->emit_gid.bytes / 4,
                                              ctx->isect_gid.bytes / 4, ctx->inv.bytes / 4, ctx->slots.bytes / 36});
     tb.isect_cap = std::min<int64_t>(cap_k, INT32_MAX / 2);
-    // the sort's scratch must cover the whole capacity (no reallocation when it already does)
-    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)tb.isect_cap), unsigned char, rs2);
+    // one sort scratch serves the depth sort and the tile sort, so it covers both sizes
+    // (no reallocation when it already does)
+    if (int r = ensure_depth_scratch(ctx, inst, P.depth)) return r;
+    ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)std::max<int64_t>(tb.isect_cap, inst)), unsigned char, rs2);
     P.rscratch = rs2;
+    P.depth.radix_scratch = rs2;
     tb.tile_cap = (int)std::min<size_t>(std::min(ctx->tile_start.bytes, ctx->tile_end.bytes) / 4, INT32_MAX);
     return MSPLAT_CUDA_OK;
 }
@@ -295,12 +300,14 @@ BatchDesc batch_desc(const StepPtrs &P, int nv) {
     return d;
 }
 
-// Projection and the scan of tiles per instance (total -> P.total).
+// Projection, the instances' depth order and the scan of their tile counts in that
+// order (emission offsets; total -> P.total).
 void enqueue_count(const StepArgs &a, const StepPtrs &P, cudaStream_t st) {
     const BatchDesc d = batch_desc(P, a.nv);
     const int inst = a.nv * a.n;
     launch_project_batch(d, inst, st);
-    scan_exclusive<int64_t>(P.n_tiles, P.offsets, inst, P.total, P.scan_part, st);
+    DepthScratch ds = P.depth;
+    launch_depth_offsets(inst, P.splats, P.n_tiles, ds, P.offsets, P.total, P.scan_part, st);
 }
 
 // Everything after the count: capacity check, emission, sort, ranges, forward,
@@ -316,10 +323,10 @@ void enqueue_rest(const StepArgs &a, const StepPtrs &P, int64_t isect_cap, int t
     launch_clamp_count(P.total, isect_cap, d_n, d_over, st);
     launch_emit_keys_batch(inst, P.splats, P.aabb, P.n_tiles, P.offsets, d, P.k[0], P.v[0], P.emit_gid, st,
                            isect_cap);
-    uint64_t *kk[2] = {P.k[0], P.k[1]};
+    uint32_t *kk[2] = {P.k[0], P.k[1]};
     uint32_t *vv[2] = {P.v[0], P.v[1]};
     const int cap = (int)isect_cap;
-    const int cur = radix_sort_pairs(kk, vv, cap, 32 + ceil_log2(std::max(tile_cap, 1)), P.rscratch, st, d_n);
+    const int cur = radix_sort_pairs32(kk, vv, cap, ceil_log2(std::max(tile_cap, 1)), P.rscratch, st, d_n);
     launch_tile_ranges(kk[cur], cap, tile_cap, P.tile_start, P.tile_end, st, d_n, d.tile_off + a.nv);
     launch_isect_map(vv[cur], cap, P.emit_gid, P.isect_gid, P.inv, st, d_n);
     if (tm) tm->mark(2, st);
@@ -387,7 +394,9 @@ std::vector<uint64_t> graph_key(const StepArgs &a, const StepPtrs &P, int64_t is
     u((uintptr_t)a.vis), u((uintptr_t)a.gn), u((uintptr_t)a.ms);
     const void *ptrs[] = {P.desc, P.splats, P.radii, P.n_tiles, P.aabb, P.offsets, P.scan_part, P.total,
                           P.tile_start, P.tile_end, P.k[0], P.k[1], P.v[0], P.v[1], P.emit_gid, P.isect_gid, P.inv,
-                          P.slots, P.rscratch, P.img, P.T, P.v_img, P.idx, P.partials, P.losses, P.counters};
+                          P.slots, P.rscratch, P.img, P.T, P.v_img, P.idx, P.partials, P.losses, P.counters,
+                          P.depth.keys[0], P.depth.keys[1], P.depth.vals[0], P.depth.vals[1], P.depth.counts,
+                          P.depth.off_sorted};
     for (const void *p : ptrs) u((uintptr_t)p);
     return k;
 }
