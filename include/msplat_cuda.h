@@ -215,6 +215,30 @@ int msplat_cuda_init_gaussians(msplat_cuda_ctx *ctx, const float *means, const u
                                uint32_t seed, float opacity_logit, float *scales, float *quats, float *features_dc,
                                float *opacities);
 
+/* Image pipeline, metrics, display (bindings.h:158-180). Image pointers are device
+ * pointers unless said otherwise; results equal the reference's bit for bit. */
+
+/* bindings.h:163 msplat_resize_area -- area (box) resample to (dh, dw, 3) float RGB;
+ * src is (sh, sw, 4) RGBA8 when src_is_u8, else (sh, sw, 3) float RGB. */
+int msplat_cuda_resize_area(msplat_cuda_ctx *ctx, const void *src, int src_is_u8, int sw, int sh, float *dst, int dw,
+                            int dh);
+/* bindings.h:167-168 msplat_undistort -- Brown-Conrady undistortion of (sh, sw, 3) into
+ * the (dh, dw, 3) crop at (roi_x, roi_y); intr (host) = fx fy cx cy, dist (host) =
+ * k1 k2 p1 p2 k3. */
+int msplat_cuda_undistort(msplat_cuda_ctx *ctx, const float *src, int sw, int sh, const float *intr,
+                          const float *dist, int roi_x, int roi_y, float *dst, int dw, int dh);
+/* bindings.h:172 msplat_image_metrics -- PSNR, SSIM (11-tap Gaussian, clamp-to-edge)
+ * and L1 of two (h, w, 3) images into out[3] (host). Synchronises. */
+int msplat_cuda_image_metrics(msplat_cuda_ctx *ctx, const float *rendered, const float *gt, int h, int w,
+                              double *out);
+/* bindings.h:175 msplat_pack_rgba8 -- float RGB (n, 3) to RGBA8 (n, 4) written to out
+ * (host or device). Synchronises. */
+int msplat_cuda_pack_rgba8(msplat_cuda_ctx *ctx, const float *img, uint32_t n, uint8_t *out);
+/* bindings.h:179-180 msplat_finalize_depth -- expected depth (depth_num / alpha *
+ * inv_scale, 0 where alpha <= 1e-4) and alpha = 1 - final_T. */
+int msplat_cuda_finalize_depth(msplat_cuda_ctx *ctx, const float *depth_num, const float *final_T, uint32_t n,
+                               float inv_scale, float *depth_out, float *alpha_out);
+
 /* Gradient-only backward of the last msplat_cuda_render on this context (same scene
  * and camera), for differentiable rendering (torch.autograd): given dL/d(image)
  * (H,W,3, device), writes dL/d(means, log-scales, quats, features_dc, features_rest,

@@ -103,6 +103,11 @@ _SIGS["msplat_cuda_train_batch"] = (i32, [vp, i32, vp, vp, f32, vp, vp, vp, vp, 
 _SIGS["msplat_cuda_train_batch_stats"] = (i32, [vp, C.POINTER(i64)])
 _SIGS["msplat_cuda_raster_variant"] = (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32)])
+_SIGS["msplat_cuda_resize_area"] = (i32, [vp, vp, i32, i32, i32, vp, i32, i32])
+_SIGS["msplat_cuda_undistort"] = (i32, [vp, vp, i32, i32, vp, vp, i32, i32, vp, i32, i32])
+_SIGS["msplat_cuda_image_metrics"] = (i32, [vp, vp, vp, i32, i32, vp])
+_SIGS["msplat_cuda_pack_rgba8"] = (i32, [vp, vp, C.c_uint32, vp])
+_SIGS["msplat_cuda_finalize_depth"] = (i32, [vp, vp, vp, C.c_uint32, f32, vp, vp])
 
 # entry points added later in the build; bound when the library exports them
 _OPTIONAL_SIGS: dict = {}

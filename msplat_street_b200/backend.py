@@ -258,6 +258,64 @@ class Context:
             C.byref(loss) if sync_loss else None))
         return float(loss.value) if sync_loss else None
 
+    # -- image pipeline, metrics, display (bindings.h:158-180) ------------------------
+    def resize_area(self, src: torch.Tensor, out_w: int, out_h: int) -> torch.Tensor:
+        """Area resample of an (H, W, 4) uint8 RGBA or (H, W, 3) float32 CUDA image to
+        (out_h, out_w, 3) float32."""
+        self.bind_stream()
+        u8 = src.dtype == torch.uint8
+        if not src.is_cuda or not src.is_contiguous() or src.dim() != 3 or src.shape[2] != (4 if u8 else 3) or \
+                (not u8 and src.dtype != torch.float32):
+            raise ValueError("src must be a contiguous CUDA (H, W, 4) uint8 or (H, W, 3) float32 image")
+        out = torch.empty((out_h, out_w, 3), dtype=torch.float32, device=src.device)
+        check(self._lib.msplat_cuda_resize_area(self.handle, ptr(src), int(u8), src.shape[1], src.shape[0], ptr(out),
+                                                out_w, out_h))
+        return out
+
+    def undistort(self, src: torch.Tensor, intr, dist, roi_x: int, roi_y: int, out_w: int,
+                  out_h: int) -> torch.Tensor:
+        """Brown-Conrady undistortion (intr = fx, fy, cx, cy; dist = k1, k2, p1, p2, k3)
+        of an (H, W, 3) float32 image into the (out_h, out_w) crop at (roi_x, roi_y)."""
+        self.bind_stream()
+        require_cuda(src, "src")
+        it, ds = _f32(intr), _f32(dist)
+        if it.size != 4 or ds.size != 5:
+            raise ValueError("intr needs 4 values and dist 5")
+        out = torch.empty((out_h, out_w, 3), dtype=torch.float32, device=src.device)
+        check(self._lib.msplat_cuda_undistort(self.handle, ptr(src), src.shape[1], src.shape[0], it.ctypes.data,
+                                              ds.ctypes.data, roi_x, roi_y, ptr(out), out_w, out_h))
+        return out
+
+    def image_metrics(self, rendered: torch.Tensor, gt: torch.Tensor):
+        """(PSNR, SSIM, L1) of two (H, W, 3) float32 CUDA images."""
+        self.bind_stream()
+        require_cuda(rendered, "rendered")
+        require_cuda(gt, "gt")
+        if rendered.shape != gt.shape:
+            raise ValueError("images differ in shape")
+        out = np.zeros(3, np.float64)
+        check(self._lib.msplat_cuda_image_metrics(self.handle, ptr(rendered), ptr(gt), rendered.shape[0],
+                                                  rendered.shape[1], out.ctypes.data))
+        return float(out[0]), float(out[1]), float(out[2])
+
+    def pack_rgba8(self, img: torch.Tensor) -> np.ndarray:
+        """(H, W, 3) float32 CUDA image to an (H, W, 4) uint8 host array."""
+        self.bind_stream()
+        require_cuda(img, "img")
+        out = np.empty(tuple(img.shape[:-1]) + (4,), np.uint8)
+        check(self._lib.msplat_cuda_pack_rgba8(self.handle, ptr(img), img.numel() // 3, out.ctypes.data))
+        return out
+
+    def finalize_depth(self, depth_num: torch.Tensor, final_T: torch.Tensor, inv_scale: float = 1.0):
+        """(expected depth, alpha) from the aux render's depth numerator and final T."""
+        self.bind_stream()
+        require_cuda(depth_num, "depth_num")
+        require_cuda(final_T, "final_T")
+        d, a = torch.empty_like(depth_num), torch.empty_like(final_T)
+        check(self._lib.msplat_cuda_finalize_depth(self.handle, ptr(depth_num), ptr(final_T), depth_num.numel(),
+                                                   inv_scale, ptr(d), ptr(a)))
+        return d, a
+
     def set_raster_variant(self, v: int) -> None:
         """Rasterizer staging variant (see raster_variants()); results do not depend on it."""
         check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"raster_variant", int(v)))

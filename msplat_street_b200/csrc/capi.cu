@@ -850,6 +850,74 @@ int msplat_cuda_init_gaussians(msplat_cuda_ctx *ctx, const float *means, const u
     return MSPLAT_CUDA_OK;
 }
 
+int msplat_cuda_resize_area(msplat_cuda_ctx *ctx, const void *src, int src_is_u8, int sw, int sh, float *dst, int dw,
+                            int dh) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (sw <= 0 || sh <= 0 || dw < 0 || dh < 0) return fail(MSPLAT_CUDA_EINVAL, "bad image sizes");
+    if (dw == 0 || dh == 0) return MSPLAT_CUDA_OK;
+    if (!src || !dst) return fail(MSPLAT_CUDA_EINVAL, "null image");
+    launch_resize_area(src, src_is_u8 ? 1 : 0, sw, sh, dst, dw, dh, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_undistort(msplat_cuda_ctx *ctx, const float *src, int sw, int sh, const float *intr,
+                          const float *dist, int roi_x, int roi_y, float *dst, int dw, int dh) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (sw <= 0 || sh <= 0 || dw < 0 || dh < 0) return fail(MSPLAT_CUDA_EINVAL, "bad image sizes");
+    if (dw == 0 || dh == 0) return MSPLAT_CUDA_OK;
+    if (!src || !dst || !intr || !dist) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    launch_undistort(src, sw, sh, intr, dist, roi_x, roi_y, dst, dw, dh, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_image_metrics(msplat_cuda_ctx *ctx, const float *rendered, const float *gt, int h, int w,
+                              double *out) {
+    if (!ctx || !out) return fail(MSPLAT_CUDA_EINVAL, "null context or output");
+    out[0] = out[1] = out[2] = 0.0;
+    if (h <= 0 || w <= 0) return MSPLAT_CUDA_OK;  // the reference returns zeros too
+    if (!rendered || !gt) return fail(MSPLAT_CUDA_EINVAL, "null image");
+    const size_t npix = (size_t)h * w;
+    MetricsScratch s;
+    ENSURE(ctx->img[0], npix * 15, float, hbuf);
+    ENSURE(ctx->img[1], npix * 3, float, ts);
+    ENSURE(ctx->img[2], npix * 3, float, tl);
+    ENSURE(ctx->img[3], npix * 3, double, tq);
+    ENSURE(ctx->img[4], (size_t)h * 3 + 3, double, rows);
+    s.hbuf = hbuf;
+    s.t_ssim = ts;
+    s.t_l1 = tl;
+    s.t_sq = tq;
+    s.rows = rows;
+    double *dout = rows + (size_t)h * 3;
+    launch_image_metrics(rendered, gt, h, w, s, dout, ctx->stream);
+    CUDA_TRY(cudaMemcpyAsync(out, dout, 3 * sizeof(double), cudaMemcpyDefault, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_pack_rgba8(msplat_cuda_ctx *ctx, const float *img, uint32_t n, uint8_t *out) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (n == 0) return MSPLAT_CUDA_OK;
+    if (!img || !out) return fail(MSPLAT_CUDA_EINVAL, "null image");
+    ENSURE(ctx->img[5], (size_t)n * 4, uint8_t, packed);
+    launch_pack_rgba8(img, n, packed, ctx->stream);
+    CUDA_TRY(cudaMemcpyAsync(out, packed, (size_t)n * 4, cudaMemcpyDefault, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_finalize_depth(msplat_cuda_ctx *ctx, const float *depth_num, const float *final_T, uint32_t n,
+                               float inv_scale, float *depth_out, float *alpha_out) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (n == 0) return MSPLAT_CUDA_OK;
+    if (!depth_num || !final_T || !depth_out || !alpha_out) return fail(MSPLAT_CUDA_EINVAL, "null buffer");
+    launch_finalize_depth(depth_num, final_T, n, inv_scale, depth_out, alpha_out, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
 int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
     if (!ctx || !loss) return fail(MSPLAT_CUDA_EINVAL, "null argument");
     if (!ctx->loss.ptr) return fail(MSPLAT_CUDA_EINVAL, "no train step has run on this context");
@@ -880,7 +948,8 @@ int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
                         &ctx->tcount, &ctx->bdesc, &ctx->bcounter, &ctx->tb.desc, &ctx->tb.pix_img,
                         &ctx->tb.pix_T, &ctx->tb.pix_idx, &ctx->tb.pix_v, &ctx->tb.partials, &ctx->tb.losses,
                         &ctx->tb.counters, &ctx->dkeys[0], &ctx->dkeys[1], &ctx->dvals[0], &ctx->dvals[1],
-                        &ctx->dcounts, &ctx->doff};
+                        &ctx->dcounts, &ctx->doff, &ctx->img[0], &ctx->img[1], &ctx->img[2], &ctx->img[3],
+                        &ctx->img[4], &ctx->img[5]};
     int64_t total = 0;
     for (const Buf *b : all) total += (int64_t)b->bytes;
     return total;

@@ -174,6 +174,8 @@ struct msplat_cuda_ctx {
     Buf tstore, tcount;
     // depth order of the Gaussians (or batch instances) before key emission
     Buf dkeys[2], dvals[2], dcounts, doff;
+    // image pipeline scratch: metrics (moments, terms, row sums) and RGBA8 packing
+    Buf img[6];
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
     int32_t *h_count = nullptr;  // pinned readback of the densified count
     // batched render: device view descriptors, their pinned staging copy, the
@@ -194,7 +196,7 @@ struct msplat_cuda_ctx {
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
                       &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
-                      &dvals[0], &dvals[1], &dcounts, &doff};
+                      &dvals[0], &dvals[1], &dcounts, &doff, &img[0], &img[1], &img[2], &img[3], &img[4], &img[5]};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);
             b->ptr = nullptr;

@@ -217,6 +217,22 @@ struct DensifyScratch {
 void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st);
 void launch_opacity_reset(float *o, float *m1, float *m2, int n, float reset_logit, cudaStream_t st);
 
+// Image pipeline, metrics and display (image.cu).
+struct MetricsScratch {
+    float *hbuf;            // h * w * 15
+    float *t_ssim, *t_l1;   // h * w * 3
+    double *t_sq;           // h * w * 3
+    double *rows;           // h * 3
+};
+void launch_resize_area(const void *src, int u8in, int sw, int sh, float *dst, int dw, int dh, cudaStream_t st);
+void launch_undistort(const float *src, int sw, int sh, const float *intr, const float *dist, int rx, int ry,
+                      float *dst, int dw, int dh, cudaStream_t st);
+void launch_image_metrics(const float *a, const float *b, int h, int w, const MetricsScratch &s, double *out,
+                          cudaStream_t st);
+void launch_pack_rgba8(const float *img, uint32_t n, uint8_t *out, cudaStream_t st);
+void launch_finalize_depth(const float *d, const float *t, uint32_t n, float inv_scale, float *od, float *oa,
+                           cudaStream_t st);
+
 struct KnnScratch {
     unsigned int *bounds;  // 6 ordered-bit floats: min xyz, max xyz
     uint64_t *keys[2];

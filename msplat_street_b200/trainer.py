@@ -268,10 +268,16 @@ class GaussianTrainer:
         return self.render_tensor(setup).cpu().numpy()
 
     def render_rgba8(self, cam_idx: int) -> np.ndarray:
-        img = self.render_tensor(self.ds.views[cam_idx].setup)
-        rgb = (img.clamp(0.0, 1.0) * 255.0).to(torch.uint8)
-        alpha = torch.full(rgb.shape[:-1] + (1,), 255, dtype=torch.uint8, device=rgb.device)
-        return torch.cat([rgb, alpha], dim=-1).cpu().numpy()
+        """(H, W, 4) uint8 render of a training camera (msplat_pack_rgba8's packing)."""
+        return self.ctx.pack_rgba8(self.render_tensor(self.ds.views[cam_idx].setup))
+
+    def evaluate(self, cam_idx: int):
+        """(PSNR, SSIM, L1) of a training camera's render against its target
+        (msplat_image_metrics)."""
+        gt = self._targets[cam_idx]
+        if gt is None:
+            raise ValueError(f"view {cam_idx} has no target image")
+        return self.ctx.image_metrics(self.render_tensor(self.ds.views[cam_idx].setup), gt)
 
     @property
     def splat_count(self) -> int:

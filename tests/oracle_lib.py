@@ -186,6 +186,22 @@ class Oracle:
         self.lib.orc_pack_rgba8(P(img), C.c_uint32(n), P(out))
         return out
 
+    def undistort(self, img, intr, dist, roi_x, roi_y, out_w, out_h):
+        img = np.ascontiguousarray(img, np.float32)
+        it = np.ascontiguousarray(intr, np.float32)
+        ds = np.ascontiguousarray(dist, np.float32)
+        out = np.zeros((out_h, out_w, 3), np.float32)
+        self.lib.orc_undistort(P(img), C.c_int(img.shape[1]), C.c_int(img.shape[0]), P(it), P(ds), C.c_int(roi_x),
+                               C.c_int(roi_y), P(out), C.c_int(out_w), C.c_int(out_h))
+        return out
+
+    def finalize_depth(self, depth_num, final_t, inv_scale):
+        d = np.ascontiguousarray(depth_num, np.float32)
+        t = np.ascontiguousarray(final_t, np.float32)
+        od, oa = np.zeros_like(d), np.zeros_like(t)
+        self.lib.orc_finalize_depth(P(d), P(t), C.c_uint32(d.size), C.c_float(inv_scale), P(od), P(oa))
+        return od, oa
+
 
 def new_adam_state(g, lrs, step: int, beta1=0.9, beta2=0.999, eps=1e-8):
     """Moments and the step sizes Model::fullIteration derives (core/src/model.cpp:638-651)."""

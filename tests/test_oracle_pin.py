@@ -227,7 +227,15 @@ def test_reference_image_ops(rest):
     assert np.array_equal(rest.resize_area(a, 20, 14), ref.resize_area(a, 20, 14))
     u8 = rng.integers(0, 256, (37, 53, 4)).astype(np.uint8)
     assert np.array_equal(rest.resize_area(u8, 53, 37), ref.resize_area(u8, 53, 37))
+    assert np.array_equal(rest.resize_area(u8, 17, 11), ref.resize_area(u8, 17, 11))
     assert np.array_equal(rest.pack_rgba8(a * 1.2 - 0.1), ref.pack_rgba8(a * 1.2 - 0.1))
+    intr, dist = [48.0, 46.0, 26.2, 18.7], [-0.12, 0.03, 0.001, -0.002, 0.004]
+    assert np.array_equal(rest.undistort(a, intr, dist, 2, 1, 49, 34), ref.undistort(a, intr, dist, 2, 1, 49, 34))
+    t = rng.random(500).astype(np.float32)
+    t[::7] = 1.0  # alpha 0 -> depth 0
+    dn = rng.random(500).astype(np.float32) * 3
+    for x, y in zip(rest.finalize_depth(dn, t, 0.5), ref.finalize_depth(dn, t, 0.5)):
+        assert np.array_equal(x, y)
 
 
 # ---- the oracle's gradients against float64 finite differences --------------------
