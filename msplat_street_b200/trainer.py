@@ -24,6 +24,7 @@ from typing import Callable, List, Optional, Sequence
 import numpy as np
 import torch
 
+from . import formats
 from .backend import AdamState, Context, GaussianParams
 from .camera import CameraSetup, prepare_cam
 
@@ -270,6 +271,41 @@ class GaussianTrainer:
     def render_rgba8(self, cam_idx: int) -> np.ndarray:
         """(H, W, 4) uint8 render of a training camera (msplat_pack_rgba8's packing)."""
         return self.ctx.pack_rgba8(self.render_tensor(self.ds.views[cam_idx].setup))
+
+    # -- files (python/bindings.cpp:372-386; core/src/model.cpp:256-496) ---------------
+    crs_scale: float = 1.0
+    crs_translation = (0.0, 0.0, 0.0)
+    keep_crs: bool = False
+
+    def export_ply(self, path: str) -> None:
+        formats.save_ply(path, self.params.numpy(), self.current_step, self.crs_scale, self.crs_translation,
+                         self.keep_crs)
+
+    def export_splat(self, path: str) -> None:
+        formats.save_splat(path, self.params.numpy(), self.crs_scale, self.crs_translation, self.keep_crs)
+
+    def save_checkpoint(self, path: str) -> None:
+        n = self.num_active
+        ck = formats.Checkpoint(self.current_step, self.cfg.sh_degree, self.adam_step,
+                                np.asarray(self.lrs, np.float32), LR_INIT[0], MEANS_LR_FINAL, self.params.numpy(),
+                                [b[:n].cpu().numpy() for b in self.m1], [b[:n].cpu().numpy() for b in self.m2])
+        formats.save_checkpoint(path, ck)
+
+    def load_checkpoint(self, path: str) -> int:
+        """Restores parameters, Adam state, learning rates and the step; returns the
+        step. Capacity becomes 4 N as Model::loadCheckpoint sets it (model.cpp:445-447)."""
+        ck = formats.load_checkpoint(path)
+        self._setup_buffers(GaussianParams(*[torch.from_numpy(a).to(self.device) for a in ck.params]))
+        for g in range(6):
+            self.m1[g][:ck.num_active] = torch.from_numpy(ck.exp_avg[g]).to(self.device).reshape(
+                self.m1[g][:ck.num_active].shape)
+            self.m2[g][:ck.num_active] = torch.from_numpy(ck.exp_avg_sq[g]).to(self.device).reshape(
+                self.m2[g][:ck.num_active].shape)
+        self.lrs = [float(x) for x in ck.lrs]
+        self.adam_step = ck.adam_step
+        self.current_step = ck.step
+        self.stats = None
+        return ck.step
 
     def evaluate(self, cam_idx: int):
         """(PSNR, SSIM, L1) of a training camera's render against its target

@@ -20,6 +20,7 @@ PATHS = {
     "restatement": os.path.join(ORACLE_DIR, "_build", "libmsplat_oracle.so"),
     "reference": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref.so"),
     "reference_fast": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_fast.so"),
+    "reference_formats": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_formats.so"),
 }
 
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
