@@ -325,8 +325,82 @@ struct State {
     std::vector<int32_t> final_idx;
     std::vector<float> v_rendered, isect_grad;
     std::vector<float> v_xy, v_conic, v_rgb, v_opacity, v_mean3d, v_scale, v_quat;
+    // prior-guided extras: expected-depth numerator, per-pixel background, dL/d(depth,
+    // alpha) per pixel, per-Gaussian depth gradient, exposure-adjusted image and its
+    // gradient
+    bool aux = false;
+    std::vector<float> out_depth, bg_img, v_aux, v_depth, out_adj, v_adj;
 };
 State g;
+bool g_has_prior = false;
+orc_prior g_prior;
+
+// ---- learned sky (core/cpu/msplat_cpu.cpp:329-402) --------------------------------
+
+struct Sky {
+    V3 up{0.f, 0.f, 0.f}, e1{0.f, 0.f, 0.f}, e2{0.f, 0.f, 0.f};
+    float fx = 1.f, fy = 1.f, cx = 0.f, cy = 0.f;
+    uint32_t w = 1, h = 1;
+    bool on = false;
+};
+
+Sky make_sky(const orc_prior *p, float fx, float fy, float cx, float cy) {
+    Sky s;
+    s.fx = fx;
+    s.fy = fy;
+    s.cx = cx;
+    s.cy = cy;
+    if (p && p->aux && p->sky && p->sky_tex) {
+        s.up = V3{p->sky_frame[0], p->sky_frame[1], p->sky_frame[2]};
+        s.e1 = V3{p->sky_frame[3], p->sky_frame[4], p->sky_frame[5]};
+        s.e2 = V3{p->sky_frame[6], p->sky_frame[7], p->sky_frame[8]};
+        s.w = (uint32_t)p->sky_w;
+        s.h = (uint32_t)p->sky_h;
+        s.on = true;
+    }
+    return s;
+}
+
+// world direction of the ray through pixel (px, py); vm is world-to-camera
+inline V3 ray_dir(float px, float py, const float *vm, const Sky &s) {
+    const float dx = (px + 0.5f - s.cx) / s.fx, dy = (py + 0.5f - s.cy) / s.fy;
+    return V3{vm[0] * dx + vm[4] * dy + vm[8], vm[1] * dx + vm[5] * dy + vm[9], vm[2] * dx + vm[6] * dy + vm[10]};
+}
+
+inline V2 sky_uv(V3 d, const Sky &s) {
+    const float pi = 3.14159265358979323846f;
+    d = scl(d, 1.f / std::sqrt(dot3(d, d)));
+    const float el = std::asin(std::min(std::max(dot3(d, s.up), -1.f), 1.f));
+    const float az = std::atan2(dot3(d, s.e2), dot3(d, s.e1));
+    return V2{(az * (0.5f / pi) + 0.5f) * (float)s.w - 0.5f, (0.5f - el / pi) * (float)s.h - 0.5f};
+}
+
+// bilinear taps: longitude wraps, latitude clamps
+struct Taps {
+    uint32_t idx[4];
+    float w[4];
+};
+inline Taps sky_taps(V2 uv, uint32_t w, uint32_t h) {
+    const float u0f = std::floor(uv.x), fu = uv.x - u0f;
+    int u0 = (int)u0f % (int)w;
+    if (u0 < 0) u0 += (int)w;
+    const int u1 = (u0 + 1) % (int)w;
+    const float vc = std::min(std::max(uv.y, 0.f), (float)h - 1.f);
+    const int v0 = (int)vc, v1 = std::min(v0 + 1, (int)h - 1);
+    const float fv = vc - (float)v0;
+    Taps t;
+    t.idx[0] = (uint32_t)(v0 * (int)w + u0); t.w[0] = (1.f - fu) * (1.f - fv);
+    t.idx[1] = (uint32_t)(v0 * (int)w + u1); t.w[1] = fu * (1.f - fv);
+    t.idx[2] = (uint32_t)(v1 * (int)w + u0); t.w[2] = (1.f - fu) * fv;
+    t.idx[3] = (uint32_t)(v1 * (int)w + u1); t.w[3] = fu * fv;
+    return t;
+}
+inline V3 sky_sample(const float *tex, V2 uv, uint32_t w, uint32_t h) {
+    const Taps t = sky_taps(uv, w, h);
+    V3 c{0.f, 0.f, 0.f};
+    for (int k = 0; k < 4; k++) c = add(scl(ld3(tex, t.idx[k]), t.w[k]), c);
+    return c;
+}
 
 // core/cpu/msplat_cpu.cpp:452-500
 void project(State &f, int N, const float *means, const float *scales, float gsc, const float *quats,
@@ -436,12 +510,19 @@ inline float sigma_of(V3 conic, V2 d) {
     return 0.5f * (conic.x * d.x * d.x + conic.z * d.y * d.y) + conic.y * d.x * d.y;
 }
 
-// core/cpu/msplat_cpu.cpp:574-626 (the non-aux path)
-void raster_fwd(State &f, const float *bg) {
+// core/cpu/msplat_cpu.cpp:574-626; with f.aux also the expected-depth numerator
+// sum_i z_i w_i and the per-pixel background (the learned sky when on)
+void raster_fwd(State &f, const float *bg, const float *sky_tex = nullptr, const Sky *sky = nullptr,
+                const float *vm = nullptr) {
     const int W = (int)f.W, H = (int)f.H, T = f.tx * f.ty;
     f.out_img.assign((size_t)W * H * 3, 0.f);
     f.final_Ts.assign((size_t)W * H, 0.f);
     f.final_idx.assign((size_t)W * H, 0);
+    if (f.aux) {
+        f.out_depth.assign((size_t)W * H, 0.f);
+        f.bg_img.assign((size_t)W * H * 3, 0.f);
+    }
+    const bool use_sky = f.aux && sky && sky->on && sky_tex;
     const V3 b{bg[0], bg[1], bg[2]};
 #pragma omp parallel for schedule(dynamic, 1)
     for (int t = 0; t < T; t++) {
@@ -452,6 +533,7 @@ void raster_fwd(State &f, const float *bg) {
                 const float px = (float)j, py = (float)i;
                 float Tr = 1.f;
                 V3 acc{0.f, 0.f, 0.f};
+                float depth = 0.f;
                 int last = s - 1;
                 for (int k = s; k < e; k++) {
                     V3 xyo = ld3(f.pk_xyo.data(), k);
@@ -468,13 +550,20 @@ void raster_fwd(State &f, const float *bg) {
                     V3 rgb = ld3(f.pk_rgb.data(), k);
                     V3 c{std::max(rgb.x + 0.5f, 0.f), std::max(rgb.y + 0.5f, 0.f), std::max(rgb.z + 0.5f, 0.f)};
                     acc = add(scl(c, vis), acc);
+                    if (f.aux) depth += f.depths[f.isect_gid[k]] * vis;
                     Tr = nT;
                     last = k;
                 }
                 const size_t pid = (size_t)i * W + j;
                 f.final_Ts[pid] = Tr;
                 f.final_idx[pid] = last;
-                V3 o = add(scl(b, Tr), acc);
+                V3 bp = b;
+                if (use_sky) bp = sky_sample(sky_tex, sky_uv(ray_dir(px, py, vm, *sky), *sky), sky->w, sky->h);
+                if (f.aux) {
+                    f.out_depth[pid] = depth;
+                    st3(f.bg_img.data(), (int64_t)pid, bp);
+                }
+                V3 o = add(scl(bp, Tr), acc);
                 f.out_img[3 * pid] = clamp01(o.x);
                 f.out_img[3 * pid + 1] = clamp01(o.y);
                 f.out_img[3 * pid + 2] = clamp01(o.z);
@@ -482,7 +571,7 @@ void raster_fwd(State &f, const float *bg) {
     }
 }
 
-// core/cpu/msplat_cpu.cpp:629-657 (no priors)
+// core/cpu/msplat_cpu.cpp:629-657
 void forward(State &f, int N, const float *means, const float *scales, float gsc, const float *quats,
              const float *vm, const float *P, float fx, float fy, float cx, float cy, unsigned H, unsigned W,
              int tx, int ty, float clip, unsigned degree, unsigned dtu, const float *cam, const float *dc,
@@ -492,9 +581,12 @@ void forward(State &f, int N, const float *means, const float *scales, float gsc
     f.H = H;
     f.tx = tx;
     f.ty = ty;
+    const orc_prior *pr = g_has_prior ? &g_prior : nullptr;
+    f.aux = pr && pr->aux;
     project(f, N, means, scales, gsc, quats, vm, P, fx, fy, cx, cy, clip, degree, dtu, cam, dc, rest);
     bin_sort(f, N, opac);
-    raster_fwd(f, bg);
+    const Sky sky = make_sky(pr, fx, fy, cx, cy);
+    raster_fwd(f, bg, sky.on ? pr->sky_tex : nullptr, &sky, vm);
 }
 
 // core/cpu/msplat_cpu.cpp:669-785 -- zero-padded separable SSIM + L1, forward and
@@ -604,8 +696,10 @@ constexpr int GS = 10;  // per-intersection slot: xy(2) conic(3) rgb(3) opacity 
 // which measures how far summation order alone moves the reference's gradients.
 bool g_reverse_sums = false;
 
-// core/cpu/msplat_cpu.cpp:959-1031 (non-aux) -- back to front, T recovered by
-// division; per-intersection slots accumulated over the tile's pixels
+// core/cpu/msplat_cpu.cpp:959-1031 -- back to front, T recovered by division;
+// per-intersection slots accumulated over the tile's pixels. With f.aux the pixel's
+// background is its own (bg_img) and the expected depth / alpha gradients (v_aux)
+// enter v_alpha and slot 9.
 void raster_bwd(State &f, const float *bg, const float *v_img) {
     const int W = (int)f.W, H = (int)f.H, T = f.tx * f.ty;
     const int64_t total = T ? f.tile_end[T - 1] : 0;
@@ -627,9 +721,11 @@ void raster_bwd(State &f, const float *bg, const float *v_img) {
                 const float Tf = f.final_Ts[pid];
                 float Tr = Tf;
                 V3 buf{0.f, 0.f, 0.f};
+                float buf_d = 0.f, buf_a = 0.f;
                 const int kf = f.final_idx[pid];
                 const V3 vo = ld3(v_img, pid);
-                const V3 Tbg = scl(Tf, b);
+                const float vd = f.aux ? f.v_aux[2 * pid] : 0.f, vaa = f.aux ? f.v_aux[2 * pid + 1] : 0.f;
+                const V3 Tbg = scl(Tf, f.aux ? ld3(f.bg_img.data(), (int64_t)pid) : b);
                 for (int k = std::min(kf, e - 1); k >= s; k--) {
                     V3 xyo = ld3(f.pk_xyo.data(), k);
                     V3 cn = ld3(f.pk_conic.data(), k);
@@ -648,11 +744,21 @@ void raster_bwd(State &f, const float *bg, const float *v_img) {
                     V3 inner = add(scl(nb, ra), scl(-ra, Tbg));
                     V3 outer = add(scl(rgb, Tr), inner);
                     float va = dot3(outer, vo);
+                    float z = 0.f;
+                    if (f.aux) {
+                        z = f.depths[f.isect_gid[k]];
+                        va += (z * Tr - buf_d * ra) * vd + (Tr - buf_a * ra) * vaa;
+                    }
                     buf = add(scl(rgb, fac), buf);
                     float *gg = lv + (size_t)(k - s) * GS;
                     if (raw.x + 0.5f >= 0.f) gg[5] += fac * vo.x;
                     if (raw.y + 0.5f >= 0.f) gg[6] += fac * vo.y;
                     if (raw.z + 0.5f >= 0.f) gg[7] += fac * vo.z;
+                    if (f.aux) {
+                        buf_d += z * fac;
+                        buf_a += fac;
+                        gg[9] += fac * vd;
+                    }
                     if (a < 0.999f) {
                         const float vs = -a * va;
                         gg[2] += 0.5f * vs * d.x * d.x;
@@ -682,6 +788,7 @@ void reduce_slots(State &f, int N) {
     f.v_conic.assign((size_t)N * 3, 0.f);
     f.v_rgb.assign((size_t)N * 3, 0.f);
     f.v_opacity.assign(N, 0.f);
+    f.v_depth.assign(N, 0.f);
 #pragma omp parallel for schedule(static)
     for (int gi = 0; gi < N; gi++) {
         float s[GS] = {0};
@@ -694,6 +801,7 @@ void reduce_slots(State &f, int N) {
         f.v_conic[3 * gi] = s[2]; f.v_conic[3 * gi + 1] = s[3]; f.v_conic[3 * gi + 2] = s[4];
         f.v_rgb[3 * gi] = s[5]; f.v_rgb[3 * gi + 1] = s[6]; f.v_rgb[3 * gi + 2] = s[7];
         f.v_opacity[gi] = s[8];
+        f.v_depth[gi] = s[9];
     }
 }
 
@@ -716,7 +824,7 @@ void proj_bwd_adam(State &f, int N, const float *means, const float *scales, flo
         if (f.radii[i] <= 0) continue;
         V3 pw = ld3(means, i);
         V3 vmn = center_vjp(P, pw, W, H, ld2(f.v_xy.data(), i));
-        vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, 0.f));  // v_depth is zero without priors
+        vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, f.v_depth[i]));  // zero without priors
         gm[0] = vmn.x; gm[1] = vmn.y; gm[2] = vmn.z;
         float gc2[3];
         conic_vjp(ld3(f.conics.data(), i), ld3(f.v_conic.data(), i), gc2);
@@ -762,6 +870,173 @@ void adam_dense(float *p, const float *gr, float *m1, float *m2, size_t n, float
                 float eps) {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; i++) adam(p[i], m1[i], m2[i], gr[i], ss, b1, b2, bc2, eps);
+}
+
+// ---- prior-guided extras (core/cpu/msplat_cpu.cpp:787-950, :1295-1309) ------------
+
+// prior depth, bilinear unless the four samples straddle a depth edge (then nearest)
+float prior_depth_at(const float *d, float x, float y, uint32_t w, uint32_t h) {
+    x = std::min(std::max(x, 0.f), (float)w - 1.f);
+    y = std::min(std::max(y, 0.f), (float)h - 1.f);
+    const uint32_t x0 = (uint32_t)x, y0 = (uint32_t)y;
+    const uint32_t x1 = std::min(x0 + 1, w - 1), y1 = std::min(y0 + 1, h - 1);
+    const float fx = x - (float)x0, fy = y - (float)y0;
+    const float d00 = d[y0 * w + x0], d01 = d[y0 * w + x1], d10 = d[y1 * w + x0], d11 = d[y1 * w + x1];
+    const float lo = std::min(std::min(d00, d01), std::min(d10, d11));
+    const float hi = std::max(std::max(d00, d01), std::max(d10, d11));
+    if (lo <= 0.f || hi > 1.05f * lo) return d[((fy < 0.5f) ? y0 : y1) * w + ((fx < 0.5f) ? x0 : x1)];
+    const float top = d00 + (d01 - d00) * fx, bot = d10 + (d11 - d10) * fx;
+    return top + (bot - top) * fy;
+}
+
+// Depth / sky / fill prior losses: per-pixel dL/d(depth numerator, alpha) into
+// f.v_aux, pixels outside `keep` removed from the photometric gradient, loss terms
+// summed per row in double and accumulated into p.loss_terms (:807-901).
+void prior_loss(State &f, const orc_prior &p, float *v_photo) {
+    const uint32_t W = f.W, H = f.H;
+    const bool has = p.prior_depth && p.prior_aux && p.prior_w > 0 && p.prior_h > 0;
+    const uint32_t pw = has ? (uint32_t)p.prior_w : 1u, ph = has ? (uint32_t)p.prior_h : 1u;
+    static const uint8_t dflt_aux[4] = {0, 0, 255, 0};  // keep everything, no sky, zero confidence
+    static const float dflt_depth[1] = {0.f};
+    const uint8_t *aux = has ? p.prior_aux : dflt_aux;
+    const float *pd = has ? p.prior_depth : dflt_depth;
+    const bool use_depth = has && p.has_depth, use_sky = has && p.has_sky_mask;
+    const float huber = std::max(p.huber_delta, 1e-6f);
+    const float inv_npix = 1.0f / (float)(W * H);
+    f.v_aux.assign((size_t)W * H * 2, 0.f);
+    std::vector<double> terms((size_t)H * 3, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int gy = 0; gy < (int)H; gy++) {
+        double ld = 0, ls = 0, lf = 0;
+        for (uint32_t gx = 0; gx < W; gx++) {
+            const size_t pix = (size_t)gy * W + gx;
+            const float sx = ((float)gx + 0.5f) * (float)pw / (float)W;
+            const float sy = ((float)gy + 0.5f) * (float)ph / (float)H;
+            const uint32_t q = std::min((uint32_t)sy, ph - 1) * pw + std::min((uint32_t)sx, pw - 1);
+            const float conf = (float)aux[4 * q] * (1.f / 255.f);
+            const bool sky = use_sky && aux[4 * q + 1] >= 128;
+            const bool keep = aux[4 * q + 2] >= 128;
+            float vd = 0.f, va = 0.f;
+            if (!keep) {
+                if (p.mask_photometric) st3(v_photo, (int64_t)pix, V3{0.f, 0.f, 0.f});
+            } else {
+                const float A = 1.f - f.final_Ts[pix];
+                if (sky) {
+                    ls += p.sky_weight * A;
+                    va = p.sky_weight * inv_npix;
+                } else {
+                    if (use_sky && p.fill_weight > 0.f) {
+                        lf += p.fill_weight * (1.f - A);
+                        va -= p.fill_weight * inv_npix;
+                    }
+                    const float D = f.out_depth[pix];
+                    if (use_depth && p.depth_weight > 0.f && conf > 0.f && A > p.min_alpha && D > 0.f) {
+                        const float dp = prior_depth_at(pd, sx - 0.5f, sy - 0.5f, pw, ph);
+                        if (dp > 0.f) {
+                            const float r = std::log(D / A) - std::log(dp);
+                            const float ar = std::fabs(r);
+                            float dr;
+                            if (ar < huber) {
+                                ld += p.depth_weight * conf * 0.5f * r * r / huber;
+                                dr = r / huber;
+                            } else {
+                                ld += p.depth_weight * conf * (ar - 0.5f * huber);
+                                dr = r > 0.f ? 1.f : (r < 0.f ? -1.f : 0.f);
+                            }
+                            const float s = p.depth_weight * conf * dr * inv_npix;
+                            vd = s / D;
+                            va -= s / A;
+                        }
+                    }
+                }
+            }
+            f.v_aux[2 * pix] = vd;
+            f.v_aux[2 * pix + 1] = va;
+        }
+        terms[3 * (size_t)gy] = ld;
+        terms[3 * (size_t)gy + 1] = ls;
+        terms[3 * (size_t)gy + 2] = lf;
+    }
+    if (p.loss_terms) {
+        double t[3] = {0, 0, 0};
+        for (uint32_t y = 0; y < H; y++)
+            for (int k = 0; k < 3; k++) t[k] += terms[3 * y + k];
+        for (int k = 0; k < 3; k++) p.loss_terms[k] += (float)(t[k] * inv_npix);
+    }
+}
+
+// per-image affine exposure: out = M c + t, M = P[0..8] row-major, t = P[9..11] (:904-913)
+void exposure_apply(const float *img, const float *P, size_t n, float *out) {
+    for (size_t i = 0; i < n; i++) {
+        const V3 c = ld3(img, (int64_t)i);
+        st3(out, (int64_t)i, V3{dot3(V3{P[0], P[1], P[2]}, c) + P[9], dot3(V3{P[3], P[4], P[5]}, c) + P[10],
+                                dot3(V3{P[6], P[7], P[8]}, c) + P[11]});
+    }
+}
+
+// exposure backward (gradient to the render, the 12 parameters' gradient summed in
+// double in pixel order) and Adam towards the identity-regularised parameters (:916-937)
+void exposure_backward_adam(const float *img, const orc_prior &p, size_t n, const float *v_adj, float *v_img,
+                            float b1, float b2, float eps) {
+    const uint32_t cam = (uint32_t)std::max(0, p.cam_index);
+    float *params = p.expo_params;
+    const float *P = params + 12 * cam;
+    double gg[12] = {0};
+    for (size_t i = 0; i < n; i++) {
+        const V3 c = ld3(img, (int64_t)i), v = ld3(v_adj, (int64_t)i);
+        st3(v_img, (int64_t)i, V3{P[0] * v.x + P[3] * v.y + P[6] * v.z, P[1] * v.x + P[4] * v.y + P[7] * v.z,
+                                  P[2] * v.x + P[5] * v.y + P[8] * v.z});
+        gg[0] += v.x * c.x; gg[1] += v.x * c.y; gg[2] += v.x * c.z;
+        gg[3] += v.y * c.x; gg[4] += v.y * c.y; gg[5] += v.y * c.z;
+        gg[6] += v.z * c.x; gg[7] += v.z * c.y; gg[8] += v.z * c.z;
+        gg[9] += v.x; gg[10] += v.y; gg[11] += v.z;
+    }
+    for (int k = 0; k < 12; k++) {
+        const uint32_t i = 12 * cam + k;
+        const float ident = (k == 0 || k == 4 || k == 8) ? 1.f : 0.f;
+        const float gk = (float)gg[k] + (p.expo_grad ? p.expo_grad[k] : 0.f) + p.expo_reg * (params[i] - ident);
+        if (p.expo_grad) p.expo_grad[k] = 0.f;
+        adam(params[i], p.expo_exp_avg[i], p.expo_exp_avg_sq[i], gk, p.expo_step_size, b1, b2, p.expo_bc2_sqrt, eps);
+    }
+}
+
+// sky texture gradient (each pixel still seeing the sky adds T dL/dC to its four
+// taps, in pixel order) and Adam over the texture (:940-964)
+void sky_backward_adam(State &f, const orc_prior &p, const Sky &sky, const float *vm, const float *v_img, float b1,
+                       float b2, float eps) {
+    float *grad = p.sky_grad;
+    for (uint32_t y = 0; y < f.H; y++)
+        for (uint32_t x = 0; x < f.W; x++) {
+            const size_t pix = (size_t)y * f.W + x;
+            const float T = f.final_Ts[pix];
+            if (T < 1e-4f) continue;
+            const V3 gv = scl(T, ld3(v_img, (int64_t)pix));
+            const Taps taps = sky_taps(sky_uv(ray_dir((float)x, (float)y, vm, sky), sky), sky.w, sky.h);
+            for (int k = 0; k < 4; k++) {
+                if (taps.w[k] == 0.f) continue;
+                float *t = grad + 3 * (size_t)taps.idx[k];
+                t[0] += taps.w[k] * gv.x;
+                t[1] += taps.w[k] * gv.y;
+                t[2] += taps.w[k] * gv.z;
+            }
+        }
+    const size_t n = (size_t)p.sky_w * p.sky_h * 3;
+    for (size_t i = 0; i < n; i++)
+        adam(p.sky_tex[i], p.sky_exp_avg[i], p.sky_exp_avg_sq[i], grad[i], p.sky_step_size, b1, b2, p.sky_bc2_sqrt,
+             eps);
+}
+
+// needle cap: the largest log-scale at most log_max above the middle one (:1295-1309)
+void needle_cap(float *s, int n, float log_max) {
+    for (int i = 0; i < n; i++) {
+        const float a = s[3 * i], b = s[3 * i + 1], c = s[3 * i + 2];
+        const float mx = std::max(a, std::max(b, c)), mn = std::min(a, std::min(b, c));
+        const float cap = (a + b + c - mx - mn) + log_max;
+        if (mx <= cap) continue;
+        if (a == mx) s[3 * i] = cap;
+        else if (b == mx) s[3 * i + 1] = cap;
+        else s[3 * i + 2] = cap;
+    }
 }
 
 // k-d tree with median splits for exact 3-NN (core/cpu/msplat_cpu.cpp:1498-1580)
@@ -844,7 +1119,14 @@ int orc_render(int n, const float *means, const float *scales, float gsc, const 
     return 0;
 }
 
-// core/cpu/msplat_cpu.cpp:1204-1327 (no priors, no needle cap)
+// Copies the prior (its pointers stay the caller's); NULL clears it.
+int orc_set_prior(const orc_prior *prior) {
+    g_has_prior = prior != nullptr;
+    if (prior) g_prior = *prior;
+    return 0;
+}
+
+// core/cpu/msplat_cpu.cpp:1204-1327, with the prior set by orc_set_prior
 float orc_train_step(int n, float *means, float *scales, float gsc, float *quats, const float *vm, const float *P,
                      float fx, float fy, float cx, float cy, unsigned H, unsigned W, int tx, int ty, float clip,
                      unsigned degree, unsigned dtu, const float *cam, float *dc, float *rest, float *opac,
@@ -852,10 +1134,29 @@ float orc_train_step(int n, float *means, float *scales, float gsc, float *quats
                      const int64_t *numel, const float *ss, const float *bc2, float b1, float b2, float eps,
                      float *vis, float *gn, float *ms, float inv_max_dim) {
     State &f = g;
+    const orc_prior *pr = g_has_prior ? &g_prior : nullptr;
+    const bool aux = pr && pr->aux;
+    const bool sky_on = aux && pr->sky && pr->sky_tex && pr->sky_grad;
+    const bool expo = pr && pr->exposure && pr->expo_params;
+    const size_t npix = (size_t)W * H;
     forward(f, n, means, scales, gsc, quats, vm, P, fx, fy, cx, cy, H, W, tx, ty, clip, degree, dtu, cam, dc, rest,
             opac, bg);
-    f.v_rendered.assign((size_t)W * H * 3, 0.f);
-    double loss = ssim_loss(f.out_img.data(), gt, W, H, ssim_w, inv_n, f.v_rendered.data());
+    if (aux && pr->loss_terms) std::fill(pr->loss_terms, pr->loss_terms + 4, 0.f);
+    if (sky_on) std::fill(pr->sky_grad, pr->sky_grad + (size_t)pr->sky_w * pr->sky_h * 3, 0.f);
+    f.v_rendered.assign(npix * 3, 0.f);
+    const float *loss_in = f.out_img.data();
+    float *loss_grad = f.v_rendered.data();
+    if (expo) {
+        f.out_adj.assign(npix * 3, 0.f);
+        f.v_adj.assign(npix * 3, 0.f);
+        exposure_apply(f.out_img.data(), pr->expo_params + 12 * std::max(0, pr->cam_index), npix, f.out_adj.data());
+        loss_in = f.out_adj.data();
+        loss_grad = f.v_adj.data();
+    }
+    double loss = ssim_loss(loss_in, gt, W, H, ssim_w, inv_n, loss_grad);
+    if (aux) prior_loss(f, *pr, loss_grad);
+    if (expo) exposure_backward_adam(f.out_img.data(), *pr, npix, f.v_adj.data(), f.v_rendered.data(), b1, b2, eps);
+    if (sky_on) sky_backward_adam(f, *pr, make_sky(pr, fx, fy, cx, cy), vm, f.v_rendered.data(), b1, b2, eps);
     raster_bwd(f, bg, f.v_rendered.data());
     reduce_slots(f, n);
     proj_bwd_adam(f, n, means, scales, gsc, quats, vm, P, fx, fy, degree, dtu, cam, dc, rest, m1[3], m2[3], m1[4],
@@ -867,6 +1168,7 @@ float orc_train_step(int n, float *means, float *scales, float gsc, float *quats
         if (gi == 3 || gi == 4 || numel[gi] == 0) continue;
         adam_dense(params[gi], grads[gi], m1[gi], m2[gi], (size_t)numel[gi], ss[gi], b1, b2, bc2[gi], eps);
     }
+    if (pr && pr->log_max_scale_ratio > 0.f) needle_cap(scales, n, pr->log_max_scale_ratio);
     for (int i = 0; i < n; i++) {
         if (f.radii[i] <= 0) continue;
         vis[i] += 1.0f;
@@ -903,6 +1205,12 @@ int64_t orc_frame(const char *name, void **ptr) {
     ORC_F("v_mean3d", g.v_mean3d, (int64_t)g.n * 3)
     ORC_F("v_scale", g.v_scale, (int64_t)g.n * 3)
     ORC_F("v_quat", g.v_quat, (int64_t)g.n * 4)
+    ORC_F("out_depth", g.out_depth, g.aux ? (int64_t)g.W * g.H : 0)
+    ORC_F("bg_img", g.bg_img, g.aux ? (int64_t)g.W * g.H * 3 : 0)
+    ORC_F("v_aux", g.v_aux, g.aux ? (int64_t)g.W * g.H * 2 : 0)
+    ORC_F("v_depth", g.v_depth, (int64_t)g.v_depth.size())
+    ORC_F("out_adj", g.out_adj, (int64_t)g.out_adj.size())
+    ORC_F("v_adj", g.v_adj, (int64_t)g.v_adj.size())
 #undef ORC_F
     *ptr = nullptr;
     return -1;

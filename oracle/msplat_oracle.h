@@ -28,6 +28,32 @@ extern "C" {
  * gradient sums in another float rounding order. Returns 0, or -1 if unknown. */
 int orc_set_option(const char *name, int value);
 
+/* Prior-guided extras (core/metal/bindings.h:43-76, PriorStep), host pointers. The
+ * prior set here applies to every later orc_render / orc_train_step until cleared with
+ * NULL (the reference takes it as their last argument). Arrays the step updates
+ * (sky texture, its gradient and moments, exposure parameters and moments, exposure
+ * gradient, loss terms) are updated in place. */
+typedef struct orc_prior {
+    int aux;                    /* expected depth + per-pixel background */
+    int sky;                    /* learned equirect sky behind the Gaussians */
+    float *sky_tex, *sky_grad, *sky_exp_avg, *sky_exp_avg_sq;  /* (sky_h, sky_w, 3) */
+    int sky_w, sky_h;
+    float sky_frame[9];         /* up, e1 (azimuth 0), e2 (azimuth 90 degrees) */
+    float sky_step_size, sky_bc2_sqrt;
+    const float *prior_depth;   /* (prior_h, prior_w), scene units, 0 = invalid */
+    const uint8_t *prior_aux;   /* (prior_h, prior_w, 4): confidence, sky, keep, - */
+    int prior_w, prior_h, has_depth, has_sky_mask;
+    float depth_weight, sky_weight, fill_weight, huber_delta, min_alpha;
+    int mask_photometric;
+    float *loss_terms;          /* [4]: depth, sky, fill, - (zeroed every step) */
+    int exposure, cam_index;
+    float *expo_params, *expo_exp_avg, *expo_exp_avg_sq;  /* (num_cams, 12) */
+    float *expo_grad;           /* [12] or NULL, zeroed after each update */
+    float expo_step_size, expo_bc2_sqrt, expo_reg;
+    float log_max_scale_ratio;  /* needle cap; <= 0 disables */
+} orc_prior;
+int orc_set_prior(const orc_prior *prior);
+
 /* core/metal/bindings.h:81-91 (msplat_render); writes the (H,W,3) image. */
 int orc_render(int num_points, const float *means, const float *scales, float glob_scale,
                const float *quats, const float *viewmat, const float *projmat,
@@ -54,6 +80,8 @@ float orc_train_step(int num_points, float *means, float *scales, float glob_sca
  *   xys depths conics colors aabb radii(i32) tile_start(i32) tile_end(i32)
  *   isect_gid(i32) out_img final_Ts final_idx(i32) v_rendered
  *   v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat
+ * and, with a prior set, out_depth bg_img v_aux (dL/d depth numerator, dL/d alpha per
+ * pixel) v_depth (per Gaussian) out_adj v_adj (exposure-adjusted image, its gradient)
  * Returns the element count and sets *ptr to the library's internal storage
  * (valid until the next call), or -1 for an unknown name. */
 int64_t orc_frame(const char *name, void **ptr);

@@ -12,6 +12,7 @@
 
 #include "msplat_oracle.h"
 
+#include <memory>
 #include <string>
 
 namespace {
@@ -40,9 +41,78 @@ struct Scene {
     }
 };
 
+bool g_has_prior = false;
+orc_prior g_prior;
+
+// The reference's PriorStep over MTensor copies of the host arrays of g_prior; the
+// arrays a train step updates are copied back by finish().
+struct Prior {
+    PriorStep ps;
+    MTensor sky_tex, sky_grad, sky_m1, sky_m2, depth, aux, terms, expo, expo_m1, expo_m2, expo_grad;
+    int64_t num_cams;
+    explicit Prior(int64_t num_cams_) : num_cams(num_cams_) {
+        const orc_prior &p = g_prior;
+        ps.aux = p.aux != 0;
+        ps.sky = p.sky != 0;
+        const std::vector<int64_t> tex{p.sky_h, p.sky_w, 3};
+        if (p.sky_tex) ps.sky_tex = &(sky_tex = host_tensor(tex, DType::Float32, p.sky_tex));
+        if (p.sky_grad) ps.sky_grad = &(sky_grad = host_tensor(tex, DType::Float32, p.sky_grad));
+        if (p.sky_exp_avg) ps.sky_exp_avg = &(sky_m1 = host_tensor(tex, DType::Float32, p.sky_exp_avg));
+        if (p.sky_exp_avg_sq) ps.sky_exp_avg_sq = &(sky_m2 = host_tensor(tex, DType::Float32, p.sky_exp_avg_sq));
+        ps.sky_w = p.sky_w;
+        ps.sky_h = p.sky_h;
+        std::memcpy(ps.sky_frame, p.sky_frame, sizeof ps.sky_frame);
+        ps.sky_step_size = p.sky_step_size;
+        ps.sky_bc2_sqrt = p.sky_bc2_sqrt;
+        if (p.prior_depth) ps.prior_depth = &(depth = host_tensor({p.prior_h, p.prior_w}, DType::Float32, p.prior_depth));
+        if (p.prior_aux) ps.prior_aux = &(aux = host_tensor({p.prior_h, p.prior_w, 4}, DType::UInt8, p.prior_aux));
+        ps.prior_w = p.prior_w;
+        ps.prior_h = p.prior_h;
+        ps.has_depth = p.has_depth != 0;
+        ps.has_sky_mask = p.has_sky_mask != 0;
+        ps.depth_weight = p.depth_weight;
+        ps.sky_weight = p.sky_weight;
+        ps.fill_weight = p.fill_weight;
+        ps.huber_delta = p.huber_delta;
+        ps.min_alpha = p.min_alpha;
+        ps.mask_photometric = p.mask_photometric != 0;
+        if (p.loss_terms) ps.loss_terms = &(terms = host_tensor({4}, DType::Float32, p.loss_terms));
+        ps.exposure = p.exposure != 0;
+        ps.cam_index = p.cam_index;
+        if (p.expo_params) ps.expo_params = &(expo = host_tensor({num_cams, 12}, DType::Float32, p.expo_params));
+        if (p.expo_exp_avg) ps.expo_exp_avg = &(expo_m1 = host_tensor({num_cams, 12}, DType::Float32, p.expo_exp_avg));
+        if (p.expo_exp_avg_sq)
+            ps.expo_exp_avg_sq = &(expo_m2 = host_tensor({num_cams, 12}, DType::Float32, p.expo_exp_avg_sq));
+        if (p.expo_grad) ps.expo_grad = &(expo_grad = host_tensor({12}, DType::Float32, p.expo_grad));
+        ps.expo_step_size = p.expo_step_size;
+        ps.expo_bc2_sqrt = p.expo_bc2_sqrt;
+        ps.expo_reg = p.expo_reg;
+        ps.log_max_scale_ratio = p.log_max_scale_ratio;
+    }
+    void finish() const {
+        const orc_prior &p = g_prior;
+        if (p.sky_tex) copy_out(sky_tex, p.sky_tex);
+        if (p.sky_grad) copy_out(sky_grad, p.sky_grad);
+        if (p.sky_exp_avg) copy_out(sky_m1, p.sky_exp_avg);
+        if (p.sky_exp_avg_sq) copy_out(sky_m2, p.sky_exp_avg_sq);
+        if (p.loss_terms) copy_out(terms, p.loss_terms);
+        if (p.expo_params) copy_out(expo, p.expo_params);
+        if (p.expo_exp_avg) copy_out(expo_m1, p.expo_exp_avg);
+        if (p.expo_exp_avg_sq) copy_out(expo_m2, p.expo_exp_avg_sq);
+        if (p.expo_grad) copy_out(expo_grad, p.expo_grad);
+    }
+};
+
 }  // namespace
 
 extern "C" {
+
+// The shim's exposure arrays hold cam_index + 1 cameras (the rows up to the one used).
+int orc_set_prior(const orc_prior *prior) {
+    g_has_prior = prior != nullptr;
+    if (prior) g_prior = *prior;
+    return 0;
+}
 
 int orc_render(int n, const float *means, const float *scales, float gsc, const float *quats, const float *vm,
                const float *P, float fx, float fy, float cx, float cy, unsigned H, unsigned W, int tx, int ty,
@@ -50,8 +120,11 @@ int orc_render(int n, const float *means, const float *scales, float gsc, const 
                const float *opac, const float *bg, float *out) {
     Scene s(n, means, scales, quats, vm, P, degree, dc, rest, opac, bg);
     float cp[3] = {cam[0], cam[1], cam[2]};
+    std::unique_ptr<Prior> pr;
+    if (g_has_prior) pr.reset(new Prior(std::max(0, g_prior.cam_index) + 1));
     MTensor img = msplat_render(n, s.means, s.scales, gsc, s.quats, s.vm, s.pm, fx, fy, cx, cy, H, W,
-                                std::make_tuple(tx, ty, 1), clip, degree, dtu, cp, s.dc, s.rest, s.opac, s.bg);
+                                std::make_tuple(tx, ty, 1), clip, degree, dtu, cp, s.dc, s.rest, s.opac, s.bg,
+                                pr ? &pr->ps : nullptr);
     copy_out(img, out);
     return 0;
 }
@@ -79,11 +152,14 @@ float orc_train_step(int n, float *means, float *scales, float gsc, float *quats
     MTensor tv = host_tensor({n}, DType::Float32, vis), tg = host_tensor({n}, DType::Float32, gn),
             tm = host_tensor({n}, DType::Float32, ms);
     float cp[3] = {cam[0], cam[1], cam[2]};
+    std::unique_ptr<Prior> pr;
+    if (g_has_prior) pr.reset(new Prior(std::max(0, g_prior.cam_index) + 1));
     auto [radii, loss] = msplat_train_step(
         n, s.means, s.scales, gsc, s.quats, s.vm, s.pm, fx, fy, cx, cy, H, W, std::make_tuple(tx, ty, 1), clip, degree,
         dtu, cp, s.dc, s.rest, s.opac, s.bg, gtt, win, ssim_w, inv_n, (int)(num_sh_bases(degree) - 1), 6, params, ea,
-        eas, ssz, b2s, b1, b2, eps, tv, tg, tm, inv_max_dim);
+        eas, ssz, b2s, b1, b2, eps, tv, tg, tm, inv_max_dim, pr ? &pr->ps : nullptr);
     (void)radii;
+    if (pr) pr->finish();
     for (int g = 0; g < 6; g++) {
         copy_out(params[g], host_params[g]);
         copy_out(ea[g], m1[g]);
@@ -106,6 +182,8 @@ int64_t orc_frame(const char *name, void **ptr) {
     if (s == nm) { *ptr = (void *)vec.data(); return (int64_t)(cnt); }
 #define REF_T(nm, ten, cnt) \
     if (s == nm) { *ptr = ten.defined() ? ten.data_ptr() : nullptr; return ten.defined() ? (int64_t)(cnt) : -1; }
+#define REF_T0(nm, ten, cnt) \
+    if (s == nm) { *ptr = ten.defined() ? ten.data_ptr() : nullptr; return ten.defined() ? (int64_t)(cnt) : 0; }
     REF_V("xys", f.xys, (int64_t)n * 2)
     REF_V("depths", f.depths, n)
     REF_V("conics", f.conics, (int64_t)n * 3)
@@ -126,8 +204,15 @@ int64_t orc_frame(const char *name, void **ptr) {
     REF_V("v_mean3d", f.v_mean3d, (int64_t)n * 3)
     REF_V("v_scale", f.v_scale, (int64_t)n * 3)
     REF_V("v_quat", f.v_quat, (int64_t)n * 4)
+    REF_T0("out_depth", f.out_depth, f.aux ? npix : 0)
+    REF_T0("bg_img", f.bg_img, f.aux ? npix * 3 : 0)
+    REF_V("v_aux", f.v_aux, f.aux ? npix * 2 : 0)
+    REF_V("v_depth", f.v_depth, (int64_t)f.v_depth.size())
+    REF_T0("out_adj", f.out_adj, f.out_adj.defined() ? f.out_adj.numel() : 0)
+    REF_T0("v_adj", f.v_adj, f.v_adj.defined() ? f.v_adj.numel() : 0)
 #undef REF_V
 #undef REF_T
+#undef REF_T0
     *ptr = nullptr;
     return -1;
 }

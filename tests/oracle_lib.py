@@ -222,3 +222,44 @@ def set_option(oracle: "Oracle", name: str, value: int) -> None:
     fn = getattr(oracle.lib, "orc_set_option", None)
     if fn is None or fn(name.encode(), C.c_int(value)) != 0:
         raise KeyError(f"{oracle.kind} oracle has no option {name}")
+
+
+class OrcPrior(C.Structure):
+    """oracle/msplat_oracle.h orc_prior (core/metal/bindings.h:43-77, PriorStep)."""
+    _fields_ = [("aux", C.c_int), ("sky", C.c_int),
+                ("sky_tex", C.c_void_p), ("sky_grad", C.c_void_p), ("sky_exp_avg", C.c_void_p),
+                ("sky_exp_avg_sq", C.c_void_p), ("sky_w", C.c_int), ("sky_h", C.c_int),
+                ("sky_frame", C.c_float * 9), ("sky_step_size", C.c_float), ("sky_bc2_sqrt", C.c_float),
+                ("prior_depth", C.c_void_p), ("prior_aux", C.c_void_p), ("prior_w", C.c_int), ("prior_h", C.c_int),
+                ("has_depth", C.c_int), ("has_sky_mask", C.c_int), ("depth_weight", C.c_float),
+                ("sky_weight", C.c_float), ("fill_weight", C.c_float), ("huber_delta", C.c_float),
+                ("min_alpha", C.c_float), ("mask_photometric", C.c_int), ("loss_terms", C.c_void_p),
+                ("exposure", C.c_int), ("cam_index", C.c_int), ("expo_params", C.c_void_p),
+                ("expo_exp_avg", C.c_void_p), ("expo_exp_avg_sq", C.c_void_p), ("expo_grad", C.c_void_p),
+                ("expo_step_size", C.c_float), ("expo_bc2_sqrt", C.c_float), ("expo_reg", C.c_float),
+                ("log_max_scale_ratio", C.c_float)]
+
+
+_PRIOR_ARRAYS = ("sky_tex", "sky_grad", "sky_exp_avg", "sky_exp_avg_sq", "prior_depth", "prior_aux", "loss_terms",
+                 "expo_params", "expo_exp_avg", "expo_exp_avg_sq", "expo_grad")
+
+
+def orc_prior(pr: dict) -> OrcPrior:
+    """An OrcPrior over the numpy arrays of a prior dict (the arrays must outlive it)."""
+    s = OrcPrior()
+    for name, _ in OrcPrior._fields_:
+        if name in _PRIOR_ARRAYS:
+            a = pr.get(name)
+            setattr(s, name, None if a is None else a.ctypes.data)
+        elif name == "sky_frame":
+            s.sky_frame[:] = [float(v) for v in np.asarray(pr.get("sky_frame", np.zeros(9)), np.float32)]
+        elif name in pr:
+            setattr(s, name, pr[name])
+    return s
+
+
+def set_prior(oracle: "Oracle", pr) -> None:
+    """orc_set_prior: ``pr`` (a dict as tests/prior_util.py builds, or None) applies to
+    every later render / train step of this oracle."""
+    oracle._prior = None if pr is None else orc_prior(pr)
+    oracle.lib.orc_set_prior(None if pr is None else C.byref(oracle._prior))

@@ -14,8 +14,14 @@ import pytest
 
 from msplat_street_b200 import scenes
 from msplat_street_b200.camera import look_at, prepare_cam
-from oracle_lib import Oracle, available, new_adam_state
+from oracle_lib import Oracle, available, new_adam_state, set_prior
 from parity_util import BACKGROUND, C1_LRS
+from prior_util import ALL, copy_prior, make_prior, restep
+
+PRIOR_ARRAYS = ("sky_tex", "sky_exp_avg", "sky_exp_avg_sq", "sky_grad", "loss_terms", "expo_params",
+                "expo_exp_avg", "expo_exp_avg_sq", "expo_grad")
+PRIOR_FRAMES = ("out_depth", "bg_img", "final_Ts", "v_aux", "v_depth", "out_adj", "v_adj")
+GRADS = ("v_rendered", "v_xy", "v_conic", "v_rgb", "v_opacity", "v_mean3d", "v_scale", "v_quat")
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -128,6 +134,42 @@ def test_knn_matches_bruteforce(rest):
         np.testing.assert_allclose(rest.knn3_mean_dist(pts), want, rtol=1e-4, atol=1e-6, err_msg=name)
 
 
+def test_golden_prior_steps(rest):
+    """Learned sky, depth / sky / fill priors, exposure and needle cap together
+    (core/cpu/msplat_cpu.cpp:787-964, 1204-1327)."""
+    gv = _load("prior.npz")
+    g = _golden_scene(10)
+    cam = _golden_camera()
+    pr = make_prior(70, 46, 3, ALL)
+    try:
+        set_prior(rest, pr)
+        assert np.array_equal(rest.render(g, cam, BACKGROUND), gv["image"])
+        for k in ("out_depth", "bg_img", "final_Ts"):
+            assert np.array_equal(rest.frame(k), gv["render_" + k]), k
+        m1 = [np.zeros_like(a) for a in g.arrays()]
+        m2 = [np.zeros_like(a) for a in g.arrays()]
+        st = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+        for step in (1, 2):
+            set_prior(rest, restep(pr, step))
+            ad = new_adam_state(g, C1_LRS, step)
+            ad["m1"], ad["m2"] = m1, m2
+            assert np.float32(rest.train_step(g, cam, BACKGROUND, gv["gt"], ad, st)) == gv[f"step{step}_loss"]
+            for k in GRADS + PRIOR_FRAMES:
+                assert np.array_equal(rest.frame(k), gv[f"step{step}_{k}"]), (step, k)
+            for name, a in zip(("means", "scales", "quats", "dc", "rest", "opac"), g.arrays()):
+                assert np.array_equal(a, gv[f"step{step}_param_{name}"]), (step, name)
+            for k in PRIOR_ARRAYS:
+                assert np.array_equal(pr[k], gv[f"step{step}_prior_{k}"]), (step, k)
+        # the extras were exercised: sky seen, priors and exposure moved, needles capped
+        assert gv["step1_prior_loss_terms"][:3].min() > 0
+        assert not np.array_equal(gv["step2_prior_sky_tex"], make_prior(70, 46, 3, ALL)["sky_tex"])
+        ls = gv["step2_param_scales"]
+        spread = ls.max(1) - np.median(ls, 1)
+        assert spread.max() <= 0.7 + 1e-6
+    finally:
+        set_prior(rest, None)
+
+
 # ---- against the reference build itself (where it was compiled) ------------------
 
 needs_ref = pytest.mark.skipif(not available("reference"), reason="reference CPU backend not built here")
@@ -160,6 +202,53 @@ def test_reference_render_and_steps(rest, deg):
             assert np.array_equal(rest.frame(k), ref.frame(k)), (step, k)
         for a, b in zip(ga.arrays(), gb.arrays()):
             assert np.array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("modes", [("aux",), ("aux", "sky"), ("aux", "depth"), ("exposure",), ("needle",), ALL],
+                         ids=lambda m: "+".join(m))
+def test_reference_prior_steps(rest, modes):
+    """Each prior-guided extra alone and all together, against the reference, on a
+    150x110 view: render frames, three training steps, every updated array."""
+    ref = Oracle("reference")
+    cam = prepare_cam(look_at((0.5, 0.4, 2.8), (0, 0, 0)), 150, 110, 170.0, 160.0, 74.0, 56.0)
+    g = scenes.random_gaussians(3000, 50, sh_degree=2)
+    set_prior(ref, None)
+    gt = ref.render(scenes.random_gaussians(3000, 51, sh_degree=2), cam, BACKGROUND)
+    pr = make_prior(150, 110, 8, modes)
+    pa, pb = copy_prior(pr), copy_prior(pr)
+    try:
+        set_prior(rest, pa)
+        set_prior(ref, pb)
+        assert np.array_equal(rest.render(g, cam, BACKGROUND), ref.render(g, cam, BACKGROUND))
+        for k in ("out_depth", "bg_img", "final_Ts"):
+            assert np.array_equal(rest.frame(k), ref.frame(k)), k
+        ga, gb = g.copy(), g.copy()
+        ma = [[np.zeros_like(a) for a in g.arrays()] for _ in range(2)]
+        mb = [[np.zeros_like(a) for a in g.arrays()] for _ in range(2)]
+        sa = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+        sb = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+        for step in (1, 2, 3):
+            set_prior(rest, restep(pa, step))
+            set_prior(ref, restep(pb, step))
+            aa = new_adam_state(ga, C1_LRS, step)
+            aa["m1"], aa["m2"] = ma
+            ab = new_adam_state(gb, C1_LRS, step)
+            ab["m1"], ab["m2"] = mb
+            assert rest.train_step(ga, cam, BACKGROUND, gt, aa, sa) == ref.train_step(gb, cam, BACKGROUND, gt, ab, sb)
+            # frames a mode does not write keep whatever an earlier call left there
+            frames = [k for k in PRIOR_FRAMES if ("aux" in modes or k in ("final_Ts", "v_depth"))
+                      and ("exposure" in modes or k not in ("out_adj", "v_adj"))]
+            for k in GRADS + tuple(frames):
+                assert np.array_equal(rest.frame(k), ref.frame(k)), (step, k)
+            for a, b in zip(ga.arrays(), gb.arrays()):
+                assert np.array_equal(a, b)
+            for k in PRIOR_ARRAYS:
+                if k in pa:
+                    assert np.array_equal(pa[k], pb[k]), (step, k)
+    finally:
+        set_prior(rest, None)
+        set_prior(ref, None)
 
 
 @needs_ref
