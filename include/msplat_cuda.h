@@ -167,6 +167,54 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
                            float *vis_counts, float *xys_grad_norm, float *max_2d_size, float inv_max_dim,
                            const int32_t **radii_out, float *loss_out);
 
+/* bindings.h:43-77 PriorStep, the last argument of msplat_render (bindings.h:90) and
+ * msplat_train_step (bindings.h:126): prior-guided extras for street captures. Device
+ * pointers; the step updates in place the arrays it trains (sky texture and its
+ * moments and gradient, exposure parameters and moments, exposure gradient, loss
+ * terms).
+ *   aux          rasterize the expected-depth numerator and a per-pixel background
+ *                (required by the sky and by every prior loss)
+ *   sky          learned equirect sky (sky_h, sky_w, 3) composited behind the Gaussians
+ *   prior_*      per-camera depth prior (prior_h, prior_w; 0 = invalid) and aux map
+ *                (prior_h, prior_w, 4 bytes: confidence, sky >= 128, keep >= 128, -)
+ *                at their own resolution; loss weights; loss_terms[4] = depth, sky,
+ *                fill, - (zeroed by every train step, then accumulated)
+ *   exposure     affine colour transform per camera (num_cams, 12: row-major M, then
+ *                b) applied to the render before the photometric loss, trained by
+ *                Adam with an L2 pull towards identity; expo_grad[12] (may be NULL)
+ *                is added to its gradient and zeroed
+ *   log_max_scale_ratio  needle cap after the update: largest log-scale <= middle one
+ *                + this (<= 0 disables). */
+typedef struct msplat_cuda_prior {
+    int32_t aux, sky;
+    float *sky_tex, *sky_grad, *sky_exp_avg, *sky_exp_avg_sq;
+    int32_t sky_w, sky_h;
+    float sky_frame[9]; /* up, e1 (azimuth 0), e2 (azimuth 90 degrees) */
+    float sky_step_size, sky_bc2_sqrt;
+    const float *prior_depth;
+    const uint8_t *prior_aux;
+    int32_t prior_w, prior_h, has_depth, has_sky_mask;
+    float depth_weight, sky_weight, fill_weight, huber_delta, min_alpha;
+    int32_t mask_photometric;
+    float *loss_terms;
+    int32_t exposure, cam_index;
+    float *expo_params, *expo_exp_avg, *expo_exp_avg_sq, *expo_grad;
+    float expo_step_size, expo_bc2_sqrt, expo_reg;
+    float log_max_scale_ratio;
+    int32_t expo_num_cams; /* rows of expo_params: cam_index is checked against it (0 = unchecked) */
+} msplat_cuda_prior;
+/* Sets the PriorStep of this context's later msplat_cuda_render and
+ * msplat_cuda_train_step calls (NULL restores the plain pipeline, the reference's
+ * default). The struct is copied; the arrays it points to must stay valid while it
+ * is set. Fails on inconsistent fields (a sky without its texture or moments,
+ * exposure without its moments or with cam_index outside expo_num_cams, a prior_aux
+ * map not 4-byte aligned). */
+int msplat_cuda_set_prior(msplat_cuda_ctx *ctx, const msplat_cuda_prior *prior);
+/* bindings.h:93-96 msplat_render_aux_outputs: after a render or train step with aux
+ * set, device pointers to the expected-depth numerator sum_i w_i z_i (H, W) and the
+ * final transmittance (H, W) in the frame cache. */
+int msplat_cuda_render_aux_outputs(msplat_cuda_ctx *ctx, const float **depth, const float **final_T);
+
 /* bindings.h:120-135 msplat_densify. The 18 buffers are capacity-sized (buf_capacity
  * rows): params[6] = means, scales, quats, features_dc, features_rest (fr_stride
  * floats per row), opacities; exp_avg[6] / exp_avg_sq[6] likewise. Requires
@@ -267,8 +315,11 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
  * the reference's _gpu_* hooks, python/bindings.cpp:655-738). Names: splats (N x 12
  * floats: x y conic_a conic_b | conic_c sigmoid(opacity) r g | b depth - -), radii,
  * aabb, tile_start, tile_end, isect_gid, out_img, final_Ts, final_idx, v_rendered and,
- * with option keep_grads, v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat.
- * *count is the element count (floats or int32). Device pointers. */
+ * with option keep_grads, v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat; with a
+ * prior (msplat_cuda_set_prior): out_depth bg_img v_aux (dL/d depth numerator, dL/d
+ * alpha per pixel) out_adj v_adj (exposure-adjusted render and its gradient) and,
+ * with keep_grads, v_depth. *count is the element count (floats or int32). Device
+ * pointers. */
 int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count);
 /* Number of tile intersections of the last frame. */
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx);

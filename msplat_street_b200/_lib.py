@@ -109,6 +109,28 @@ _SIGS["msplat_cuda_image_metrics"] = (i32, [vp, vp, vp, i32, i32, vp])
 _SIGS["msplat_cuda_pack_rgba8"] = (i32, [vp, vp, C.c_uint32, vp])
 _SIGS["msplat_cuda_finalize_depth"] = (i32, [vp, vp, vp, C.c_uint32, f32, vp, vp])
 
+
+class Prior(C.Structure):
+    """msplat_cuda_prior (include/msplat_cuda.h; PriorStep, core/metal/bindings.h:43-77)."""
+    _fields_ = [
+        ("aux", C.c_int32), ("sky", C.c_int32),
+        ("sky_tex", vp), ("sky_grad", vp), ("sky_exp_avg", vp), ("sky_exp_avg_sq", vp),
+        ("sky_w", C.c_int32), ("sky_h", C.c_int32), ("sky_frame", f32 * 9),
+        ("sky_step_size", f32), ("sky_bc2_sqrt", f32),
+        ("prior_depth", vp), ("prior_aux", vp),
+        ("prior_w", C.c_int32), ("prior_h", C.c_int32), ("has_depth", C.c_int32), ("has_sky_mask", C.c_int32),
+        ("depth_weight", f32), ("sky_weight", f32), ("fill_weight", f32), ("huber_delta", f32), ("min_alpha", f32),
+        ("mask_photometric", C.c_int32), ("loss_terms", vp),
+        ("exposure", C.c_int32), ("cam_index", C.c_int32),
+        ("expo_params", vp), ("expo_exp_avg", vp), ("expo_exp_avg_sq", vp), ("expo_grad", vp),
+        ("expo_step_size", f32), ("expo_bc2_sqrt", f32), ("expo_reg", f32),
+        ("log_max_scale_ratio", f32), ("expo_num_cams", C.c_int32),
+    ]
+
+
+_SIGS["msplat_cuda_set_prior"] = (i32, [vp, C.POINTER(Prior)])
+_SIGS["msplat_cuda_render_aux_outputs"] = (i32, [vp, PP, PP])
+
 # entry points added later in the build; bound when the library exports them
 _OPTIONAL_SIGS: dict = {}
 

@@ -125,6 +125,74 @@ class BatchItem:
     clip_thresh: float = 0.01
 
 
+_PRIOR_TENSORS = {"sky_tex": torch.float32, "sky_grad": torch.float32, "sky_exp_avg": torch.float32,
+                  "sky_exp_avg_sq": torch.float32, "prior_depth": torch.float32, "prior_aux": torch.uint8,
+                  "loss_terms": torch.float32, "expo_params": torch.float32, "expo_exp_avg": torch.float32,
+                  "expo_exp_avg_sq": torch.float32, "expo_grad": torch.float32}
+
+
+@dataclass
+class PriorStep:
+    """Prior-guided extras of a render / train step (core/metal/bindings.h:43-77), over
+    CUDA tensors the step reads and, for the trained ones, updates in place: the
+    learned sky (texture, gradient, Adam moments), the loss terms and the exposure
+    parameters, moments and gradient. Defaults are the reference's."""
+    aux: bool = False
+    sky: bool = False
+    sky_tex: Optional[torch.Tensor] = None          # (sky_h, sky_w, 3)
+    sky_grad: Optional[torch.Tensor] = None
+    sky_exp_avg: Optional[torch.Tensor] = None
+    sky_exp_avg_sq: Optional[torch.Tensor] = None
+    sky_frame: Sequence[float] = (0.0,) * 9         # up, e1 (azimuth 0), e2 (azimuth 90 degrees)
+    sky_step_size: float = 0.0
+    sky_bc2_sqrt: float = 1.0
+    prior_depth: Optional[torch.Tensor] = None      # (prior_h, prior_w) float32, 0 = invalid
+    prior_aux: Optional[torch.Tensor] = None        # (prior_h, prior_w, 4) uint8: confidence, sky, keep, -
+    has_depth: bool = False
+    has_sky_mask: bool = False
+    depth_weight: float = 0.0
+    sky_weight: float = 0.0
+    fill_weight: float = 0.0
+    huber_delta: float = 0.05
+    min_alpha: float = 0.25
+    mask_photometric: bool = True
+    loss_terms: Optional[torch.Tensor] = None       # [4]: depth, sky, fill, - (zeroed each step)
+    exposure: bool = False
+    cam_index: int = 0
+    expo_params: Optional[torch.Tensor] = None      # (num_cams, 12)
+    expo_exp_avg: Optional[torch.Tensor] = None
+    expo_exp_avg_sq: Optional[torch.Tensor] = None
+    expo_grad: Optional[torch.Tensor] = None        # [12], zeroed after each update
+    expo_step_size: float = 0.0
+    expo_bc2_sqrt: float = 1.0
+    expo_reg: float = 0.0
+    log_max_scale_ratio: float = 0.0                # needle cap, <= 0 disables
+
+    def to_c(self) -> "_lib.Prior":
+        c = _lib.Prior()
+        for name, dt in _PRIOR_TENSORS.items():
+            t = getattr(self, name)
+            if t is not None and (not t.is_cuda or t.dtype != dt or not t.is_contiguous()):
+                raise ValueError(f"PriorStep.{name} must be a contiguous {dt} CUDA tensor")
+            setattr(c, name, _addr(t))
+        c.aux, c.sky, c.exposure = int(self.aux), int(self.sky), int(self.exposure)
+        c.has_depth, c.has_sky_mask = int(self.has_depth), int(self.has_sky_mask)
+        c.mask_photometric, c.cam_index = int(self.mask_photometric), int(self.cam_index)
+        if self.sky_tex is not None:
+            c.sky_h, c.sky_w = int(self.sky_tex.shape[0]), int(self.sky_tex.shape[1])
+        if self.prior_depth is not None:
+            c.prior_h, c.prior_w = int(self.prior_depth.shape[0]), int(self.prior_depth.shape[1])
+        elif self.prior_aux is not None:
+            c.prior_h, c.prior_w = int(self.prior_aux.shape[0]), int(self.prior_aux.shape[1])
+        if self.expo_params is not None:
+            c.expo_num_cams = int(self.expo_params.shape[0])
+        c.sky_frame[:] = [float(v) for v in np.asarray(self.sky_frame, np.float32).reshape(9)]
+        for name in ("sky_step_size", "sky_bc2_sqrt", "depth_weight", "sky_weight", "fill_weight", "huber_delta",
+                     "min_alpha", "expo_step_size", "expo_bc2_sqrt", "expo_reg", "log_max_scale_ratio"):
+            setattr(c, name, float(getattr(self, name)))
+        return c
+
+
 class Context:
     """One msplat_cuda context: a frame cache plus the stream it works on."""
 
@@ -462,6 +530,28 @@ class Context:
         if cnt.value:
             check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out), src, int(cnt.value) * 4))
         return out
+
+    # -- prior-guided extras (bindings.h:43-96) ---------------------------------------
+    def set_prior(self, prior: Optional[PriorStep]) -> None:
+        """The PriorStep of later render / train_step calls (None: the plain pipeline).
+        The tensors must stay alive while it is set; the context keeps a reference."""
+        self._prior = prior
+        if prior is None:
+            check(self._lib.msplat_cuda_set_prior(self.handle, None))
+            return
+        self._prior_c = prior.to_c()
+        check(self._lib.msplat_cuda_set_prior(self.handle, C.byref(self._prior_c)))
+
+    def render_aux_outputs(self):
+        """msplat_render_aux_outputs: copies of the expected-depth numerator and the
+        final transmittance of the last aux-mode render or step, flat (H * W,)."""
+        d, t = C.c_void_p(), C.c_void_p()
+        check(self._lib.msplat_cuda_render_aux_outputs(self.handle, C.byref(d), C.byref(t)))
+        npix = self.frame("final_Ts").numel()
+        out = torch.empty((2, npix), dtype=torch.float32, device="cuda")
+        check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out[0]), d, npix * 4))
+        check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out[1]), t, npix * 4))
+        return out[0], out[1]
 
     def num_isects(self) -> int:
         return int(self._lib.msplat_cuda_num_isects(self.handle))

@@ -117,22 +117,27 @@ __device__ __forceinline__ void cov3d_vjp(V3 sc, float gs, Q4 q, const float *gc
 // slots, in sorted (tile) order. A Gaussian may cover hundreds of tiles, so the warp
 // sums each of its visible Gaussians together: lane l takes the intersections l,
 // l+32, ... and a fixed butterfly combines the lanes. g0 = index of the warp's first
-// Gaussian in offsets / n_tiles; s9 is zero for invisible Gaussians.
+// Gaussian in offsets / n_tiles; s9 is zero for invisible Gaussians. With
+// slots_depth (aux mode) the depth slots are summed the same way into *sd.
 __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64_t *offsets, const int32_t *n_tiles,
-                                               const int32_t *inv, const float *slots, float s9[9]) {
+                                               const int32_t *inv, const float *slots, float s9[9],
+                                               const float *slots_depth = nullptr, float *sd = nullptr) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int c = 0; c < 9; c++) s9[c] = 0.f;
+    if (sd) *sd = 0.f;
     const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
     for (int gl = 0; gl < 32; gl++) {
         if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
         const int64_t e0 = offsets[g0 + gl];
         const int cnt = n_tiles[g0 + gl];
-        float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, pd = 0.f;
         for (int j = lane; j < cnt; j += 32) {
-            const float *sl = slots + (size_t)inv[e0 + j] * 9;
+            const int32_t k = inv[e0 + j];
+            const float *sl = slots + (size_t)k * 9;
 #pragma unroll
             for (int c = 0; c < 9; c++) p[c] += sl[c];
+            if (slots_depth) pd += slots_depth[k];
         }
 #pragma unroll
         for (int c = 0; c < 9; c++) {
@@ -140,19 +145,26 @@ __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64
             for (int o = 16; o > 0; o >>= 1) p[c] += __shfl_xor_sync(0xffffffffu, p[c], o);
             if (lane == gl) s9[c] = p[c];
         }
+        if (slots_depth) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) pd += __shfl_xor_sync(0xffffffffu, pd, o);
+            if (lane == gl) *sd = pd;
+        }
     }
 }
 
 // Projection, EWA and covariance VJPs of one visible Gaussian i seen by camera cam
 // (core/cpu/msplat_cpu.cpp:1068-1110): mean, scale and quaternion gradients from its
 // summed xy / conic gradients, and its unit view direction for the SH gradients.
+// v_depth: dL/d(view-space depth), from the aux mode's expected-depth loss (else 0).
 __device__ __forceinline__ void projection_vjp(const CamParams &cam, const float *means, const float *scales,
                                                const float *quats, float glob_scale, const Splat *sp, int i,
-                                               const float s9[9], float gm[3], float gsv[3], float gq[4], V3 &dir) {
+                                               const float s9[9], float gm[3], float gsv[3], float gq[4], V3 &dir,
+                                               float v_depth = 0.f) {
     const float *vm = cam.viewmat;
     V3 pw = ld3(means, i);
     V3 vmn = center_vjp(cam.projmat, pw, cam.width, cam.height, s9[0], s9[1]);
-    vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, 0.f));  // no expected-depth term without priors
+    vmn = add(vmn, scl(V3{vm[8], vm[9], vm[10]}, v_depth));
     gm[0] = vmn.x;
     gm[1] = vmn.y;
     gm[2] = vmn.z;
@@ -216,9 +228,9 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
     const float b1 = a.beta1, b2 = a.beta2, eps = a.eps;
 
     // 1. per-Gaussian sums of the intersection slots
-    float s9[9];
+    float s9[9], sd = 0.f;
     warp_slot_sums(vis, (int64_t)blockIdx.x * BWD_THREADS + (threadIdx.x - lane), a.offsets, a.n_tiles, a.inv,
-                   a.slots, s9);
+                   a.slots, s9, a.slots_depth, a.slots_depth ? &sd : nullptr);
     if (valid) {  // s9 is zero for invisible Gaussians
         if (a.v_xy) {
             a.v_xy[2 * i] = s9[0];
@@ -235,12 +247,14 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
             a.v_rgb[3 * i + 2] = s9[7];
         }
         if (a.v_opacity) a.v_opacity[i] = s9[8];
+        if (a.v_depth) a.v_depth[i] = sd;
     }
 
     // 2. projection VJPs
     float gm[3] = {0.f, 0.f, 0.f}, gsv[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f};
     V3 dir{0.f, 0.f, 1.f};
-    if (vis) projection_vjp(a.cam, a.means, a.scales, a.quats, a.glob_scale, a.splats + i, i, s9, gm, gsv, gq, dir);
+    if (vis)
+        projection_vjp(a.cam, a.means, a.scales, a.quats, a.glob_scale, a.splats + i, i, s9, gm, gsv, gq, dir, sd);
     if (valid && a.v_mean3d) {
         for (int c = 0; c < 3; c++) {
             a.v_mean3d[3 * i + c] = gm[c];
@@ -267,6 +281,18 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs
             adam_step(a.p[2][k], a.m1[2][k], a.m2[2][k], gq[c], a.ss[2], b1, b2, a.bc2[2], eps);
         }
         if (a.m1[5]) adam_step(a.p[5][i], a.m1[5][i], a.m2[5][i], s9[8], a.ss[5], b1, b2, a.bc2[5], eps);
+        // needle cap after the scale update (scale_ratio_cap, core/cpu/msplat_cpu.cpp:1295-1309)
+        if (a.log_max_scale_ratio > 0.f) {
+            float *sc = a.p[1] + 3 * (size_t)i;
+            const float x = sc[0], y = sc[1], z = sc[2];
+            const float mx = fmaxf(x, fmaxf(y, z)), mn = fminf(x, fminf(y, z));
+            const float cap = (x + y + z - mx - mn) + a.log_max_scale_ratio;
+            if (mx > cap) {
+                if (x == mx) sc[0] = cap;
+                else if (y == mx) sc[1] = cap;
+                else sc[2] = cap;
+            }
+        }
         // DC for visible Gaussians
         if (vis) {
 #pragma unroll

@@ -74,9 +74,27 @@ CamParams msplat::make_cam(const float *viewmat, const float *projmat, float fx,
 
 namespace {
 
+// The sky sampling parameters of a prior for one camera (make_sky_params,
+// core/cpu/msplat_cpu.cpp:338-350).
+SkyArgs sky_args(const msplat_cuda_prior &p, const CamParams &cam) {
+    SkyArgs s;
+    s.tex = p.sky_tex;
+    s.tex_w = p.sky_w;
+    s.tex_h = p.sky_h;
+    std::memcpy(s.frame, p.sky_frame, sizeof s.frame);
+    s.fx = cam.fx;
+    s.fy = cam.fy;
+    s.cx = cam.cx;
+    s.cy = cam.cy;
+    std::memcpy(s.viewmat, cam.viewmat, sizeof s.viewmat);
+    return s;
+}
+
 // Projection, binning and forward rasterization: the shared forward of render and
 // train (core/cpu/msplat_cpu.cpp:629-657). One host synchronisation reads the
-// intersection count, which sizes the sort.
+// intersection count, which sizes the sort. With a prior whose aux flag is set, the
+// aux rasterizer also writes the expected-depth numerator and the per-pixel
+// background, sampled from the learned sky when one is set.
 int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales, float glob_scale,
             const float *quats, const CamParams &cam, const float *dc, const float *rest, const float *opac,
             const float *bg) {
@@ -103,6 +121,17 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ENSURE(ctx->final_T, npix, float, final_T);
     ENSURE(ctx->final_idx, npix, int32_t, final_idx);
     if (!ctx->h_total) CUDA_TRY(cudaMallocHost(&ctx->h_total, sizeof(int64_t)));
+    const msplat_cuda_prior *pr = ctx->has_prior ? &ctx->prior : nullptr;
+    const bool aux = pr && pr->aux;
+    const bool sky = aux && pr->sky && pr->sky_tex;
+    ctx->aux_frame = aux;
+    float *out_depth = nullptr, *bg_img = nullptr;
+    if (aux) {
+        ENSURE(ctx->pri[PB_DEPTH], npix, float, od);
+        ENSURE(ctx->pri[PB_BG], npix * 3, float, bi);
+        out_depth = od;
+        bg_img = bi;
+    }
 
     ProjectArgs pa;
     pa.n = n;
@@ -150,7 +179,7 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
     launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
 
-    RasterArgs ra;
+    RasterArgs ra{};
     ra.W = (int)cam.width;
     ra.H = (int)cam.height;
     ra.tiles_x = cam.tiles_x;
@@ -173,8 +202,16 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
         ra.tcount = tc;
         ra.tcap = ctx->tstore_cap;
     }
+    ra.out_depth = out_depth;
+    ra.bg_img = bg_img;
+    ra.sky_bg = sky ? 1 : 0;
     ctx->timer.mark(2, st);
-    launch_raster_fwd(ra, st, ctx->raster_variant);
+    if (aux) {
+        if (sky) launch_sky_background(sky_args(*pr, cam), (int)cam.width, (int)cam.height, bg_img, st);
+        launch_raster_fwd_aux(ra, st);
+    } else {
+        launch_raster_fwd(ra, st, ctx->raster_variant);
+    }
     ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
@@ -473,8 +510,48 @@ int msplat_cuda_render(msplat_cuda_ctx *ctx, int num_points, const float *means3
 
 int msplat_cuda_render_batch(msplat_cuda_ctx *ctx, int32_t n_views, const msplat_cuda_view *views) {
     if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (ctx->has_prior)
+        return fail(MSPLAT_CUDA_EUNSUPPORTED, "a prior (msplat_cuda_set_prior) applies to msplat_cuda_render only; "
+                                              "clear it before msplat_cuda_render_batch");
     if (int r = forward_batch(ctx, n_views, views)) return r;
     ctx->timer.collect();
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_set_prior(msplat_cuda_ctx *ctx, const msplat_cuda_prior *prior) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (!prior) {
+        ctx->has_prior = false;
+        return MSPLAT_CUDA_OK;
+    }
+    const msplat_cuda_prior &p = *prior;
+    if (p.aux && p.sky) {
+        if (!p.sky_tex) return fail(MSPLAT_CUDA_EINVAL, "prior: sky set without sky_tex");
+        if (p.sky_w < 1 || p.sky_h < 1)
+            return fail(MSPLAT_CUDA_EINVAL, "prior: sky texture size %dx%d", (int)p.sky_w, (int)p.sky_h);
+        if (p.sky_grad && (!p.sky_exp_avg || !p.sky_exp_avg_sq))
+            return fail(MSPLAT_CUDA_EINVAL, "prior: sky_grad set without the sky's Adam moments");
+    }
+    if ((p.prior_depth || p.prior_aux) && (p.prior_w < 0 || p.prior_h < 0))
+        return fail(MSPLAT_CUDA_EINVAL, "prior: negative prior size %dx%d", (int)p.prior_w, (int)p.prior_h);
+    if (p.prior_aux && reinterpret_cast<uintptr_t>(p.prior_aux) % 4 != 0)
+        return fail(MSPLAT_CUDA_EINVAL, "prior: prior_aux must be 4-byte aligned (one RGBA pixel per load)");
+    if (p.exposure && p.expo_params && (!p.expo_exp_avg || !p.expo_exp_avg_sq))
+        return fail(MSPLAT_CUDA_EINVAL, "prior: exposure set without its Adam moments");
+    if (p.exposure && p.expo_num_cams > 0 && std::max(0, (int)p.cam_index) >= p.expo_num_cams)
+        return fail(MSPLAT_CUDA_EINVAL, "prior: cam_index %d outside the %d exposure rows", (int)p.cam_index,
+                    (int)p.expo_num_cams);
+    ctx->prior = p;
+    ctx->has_prior = true;
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_render_aux_outputs(msplat_cuda_ctx *ctx, const float **depth, const float **final_T) {
+    if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (!ctx->aux_frame || !ctx->pri[PB_DEPTH].ptr)
+        return fail(MSPLAT_CUDA_EINVAL, "no aux outputs: the last render / train step ran without prior->aux");
+    if (depth) *depth = reinterpret_cast<const float *>(ctx->pri[PB_DEPTH].ptr);
+    if (final_T) *final_T = reinterpret_cast<const float *>(ctx->final_T.ptr);
     return MSPLAT_CUDA_OK;
 }
 
@@ -512,21 +589,137 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     ENSURE(ctx->loss_part, ssim_blocks((int)img_width, (int)img_height), double, loss_part);
     ENSURE(ctx->loss, 1, float, d_loss);
     ENSURE(ctx->slots, (size_t)ctx->n_isect * 9, float, slots);
+    const float *out_img = reinterpret_cast<const float *>(ctx->out_img.ptr);
+    const float *final_T = reinterpret_cast<const float *>(ctx->final_T.ptr);
+
+    // prior-guided extras (core/cpu/msplat_cpu.cpp:1225-1271)
+    const msplat_cuda_prior *pr = ctx->has_prior ? &ctx->prior : nullptr;
+    const bool aux = pr && pr->aux;
+    const bool sky = aux && pr->sky && pr->sky_tex && pr->sky_grad;
+    const bool expo = pr && pr->exposure && pr->expo_params;
+    if (aux && pr->loss_terms) CUDA_TRY(cudaMemsetAsync(pr->loss_terms, 0, 4 * sizeof(float), st));
+    const float *loss_in = out_img;
+    float *loss_grad = v_rendered;
+    float *out_adj = nullptr, *v_adj = nullptr;
+    if (expo) {
+        ENSURE(ctx->pri[PB_ADJ], npix * 3, float, adj);
+        ENSURE(ctx->pri[PB_VADJ], npix * 3, float, vadj);
+        out_adj = adj;
+        v_adj = vadj;
+        launch_exposure_apply(out_img, pr->expo_params + 12 * (size_t)std::max(0, pr->cam_index), (int64_t)npix,
+                              out_adj, st);
+        loss_in = out_adj;
+        loss_grad = v_adj;
+    }
 
     SsimArgs sa;
     sa.W = (int)img_width;
     sa.H = (int)img_height;
-    sa.img = reinterpret_cast<const float *>(ctx->out_img.ptr);
+    sa.img = loss_in;
     sa.gt = gt;
     sa.ssim_weight = ssim_weight;
     sa.inv_n = loss_inv_n;
-    sa.v_out = v_rendered;
+    sa.v_out = loss_grad;
     sa.partials = loss_part;
     sa.loss = d_loss;
     launch_ssim_loss(sa, st);
+
+    float *v_aux = nullptr, *slots_depth = nullptr;
+    if (aux) {
+        ENSURE(ctx->pri[PB_VAUX], npix * 2, float, va);
+        ENSURE(ctx->pri[PB_SLOTS_D], ctx->n_isect, float, sd);
+        v_aux = va;
+        slots_depth = sd;
+        PriorLossArgs pl;
+        pl.W = (int)img_width;
+        pl.H = (int)img_height;
+        pl.final_T = final_T;
+        pl.out_depth = reinterpret_cast<const float *>(ctx->pri[PB_DEPTH].ptr);
+        pl.prior_depth = pr->prior_depth;
+        pl.prior_aux = pr->prior_aux;
+        pl.pw = pr->prior_w;
+        pl.ph = pr->prior_h;
+        pl.use_depth = pr->has_depth;
+        pl.use_sky = pr->has_sky_mask;
+        pl.mask_photometric = pr->mask_photometric;
+        pl.depth_weight = pr->depth_weight;
+        pl.sky_weight = pr->sky_weight;
+        pl.fill_weight = pr->fill_weight;
+        pl.huber = std::max(pr->huber_delta, 1e-6f);
+        pl.min_alpha = pr->min_alpha;
+        pl.inv_npix = 1.0f / (float)(img_width * img_height);
+        pl.v_photo = loss_grad;
+        pl.v_aux = v_aux;
+        pl.terms = nullptr;
+        double *rows = nullptr;
+        if (pr->loss_terms) {
+            ENSURE(ctx->pri[PB_TERMS], npix * 3, float, terms);
+            ENSURE(ctx->pri[PB_ROWS], (size_t)img_height * 3, double, rw);
+            pl.terms = terms;
+            rows = rw;
+        }
+        launch_prior_loss(pl, rows, pr->loss_terms, st);
+    }
+    if (expo) {
+        ENSURE(ctx->pri[PB_EXPO], (size_t)exposure_blocks((int64_t)npix) * 12, double, part);
+        ExposureArgs e;
+        e.params = pr->expo_params;
+        e.exp_avg = pr->expo_exp_avg;
+        e.exp_avg_sq = pr->expo_exp_avg_sq;
+        e.grad = pr->expo_grad;
+        e.cam = std::max(0, pr->cam_index);
+        e.step_size = pr->expo_step_size;
+        e.bc2 = pr->expo_bc2_sqrt;
+        e.reg = pr->expo_reg;
+        e.beta1 = adam_beta1;
+        e.beta2 = adam_beta2;
+        e.eps = adam_eps;
+        launch_exposure_backward_adam(out_img, v_adj, (int64_t)npix, v_rendered, part, e, st);
+    }
+    if (sky) {
+        if (4 * npix > (size_t)INT32_MAX)
+            return fail(MSPLAT_CUDA_EINVAL, "learned sky: image too large for the sky backward (%zu pixels)", npix);
+        SkyScratch sc;
+        ENSURE(ctx->pri[PB_SKY_IDX], npix, uint4, tidx);
+        ENSURE(ctx->pri[PB_SKY_W], npix, float4, tw);
+        ENSURE(ctx->pri[PB_SKY_G], npix, float4, tg);
+        ENSURE(ctx->pri[PB_SKY_COUNT], npix, int32_t, cnt);
+        ENSURE(ctx->pri[PB_SKY_OFF], npix, int32_t, off);
+        ENSURE(ctx->pri[PB_SKY_PART], scan_blocks((int)npix) + 1, int32_t, spart);
+        ENSURE(ctx->pri[PB_SKY_TOTAL], 1, int32_t, stotal);
+        ENSURE(ctx->pri[PB_SKY_K0], 4 * npix, uint32_t, k0);
+        ENSURE(ctx->pri[PB_SKY_K1], 4 * npix, uint32_t, k1);
+        ENSURE(ctx->pri[PB_SKY_V0], 4 * npix, uint32_t, v0);
+        ENSURE(ctx->pri[PB_SKY_V1], 4 * npix, uint32_t, v1);
+        ENSURE(ctx->pri[PB_SKY_RS], radix_scratch_bytes((int)(4 * npix)), unsigned char, rs);
+        sc.tap_idx = tidx;
+        sc.tap_w = tw;
+        sc.tap_g = tg;
+        sc.count = cnt;
+        sc.off = off;
+        sc.scan_part = spart;
+        sc.d_total = stotal;
+        sc.keys[0] = k0;
+        sc.keys[1] = k1;
+        sc.vals[0] = v0;
+        sc.vals[1] = v1;
+        sc.radix_scratch = rs;
+        SkyAdamArgs sk;
+        sk.tex = pr->sky_tex;
+        sk.grad = pr->sky_grad;
+        sk.exp_avg = pr->sky_exp_avg;
+        sk.exp_avg_sq = pr->sky_exp_avg_sq;
+        sk.step_size = pr->sky_step_size;
+        sk.bc2 = pr->sky_bc2_sqrt;
+        sk.beta1 = adam_beta1;
+        sk.beta2 = adam_beta2;
+        sk.eps = adam_eps;
+        launch_sky_backward_adam(sky_args(*pr, cam), (int)img_width, (int)img_height, final_T, v_rendered, sk, sc,
+                                 st);
+    }
     ctx->timer.mark(4, st);
 
-    RasterBwdArgs rb;
+    RasterBwdArgs rb{};
     rb.W = (int)img_width;
     rb.H = (int)img_height;
     rb.tiles_x = tiles_x;
@@ -542,11 +735,20 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     rb.slots = slots;
     rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
     rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
-    launch_raster_bwd(rb, st, ctx->raster_variant);
+    if (aux) {
+        rb.bg_img = reinterpret_cast<const float *>(ctx->pri[PB_BG].ptr);
+        rb.v_aux = v_aux;
+        rb.slots_depth = slots_depth;
+        launch_raster_bwd_aux(rb, st);
+    } else {
+        launch_raster_bwd(rb, st, ctx->raster_variant);
+    }
     ctx->timer.mark(5, st);
 
     BackwardArgs ba;
     std::memset(&ba, 0, sizeof ba);
+    ba.slots_depth = slots_depth;
+    ba.log_max_scale_ratio = pr ? pr->log_max_scale_ratio : 0.f;
     ba.n = n;
     ba.means = means3d;
     ba.scales = scales;
@@ -574,6 +776,10 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
         ba.v_mean3d = vm3;
         ba.v_scale = vsc;
         ba.v_quat = vq;
+        if (aux) {
+            ENSURE(ctx->pri[PB_VDEPTH], n, float, vdep);
+            ba.v_depth = vdep;
+        }
     }
     ba.do_adam = adam ? 1 : 0;
     float *params[6] = {means3d, scales, quats, features_dc, features_rest, opacities};
@@ -601,6 +807,8 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
     if (vis_counts && (!xys_grad_norm || !max_2d_size))
         return fail(MSPLAT_CUDA_EINVAL, "densification statistics need all three buffers");
     launch_backward_adam(ba, st);
+    // without Adam the fused kernel leaves the scales alone; the cap still applies
+    if (!adam && ba.log_max_scale_ratio > 0.f) launch_needle_cap(scales, n, ba.log_max_scale_ratio, st);
     ctx->timer.mark(6, st);
     CUDA_TRY(cudaGetLastError());
     ctx->timer.collect();
@@ -627,6 +835,9 @@ int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const floa
         return fail(MSPLAT_CUDA_EINVAL, "render_backward must follow msplat_cuda_render of the same scene and camera "
                                         "on this context");
     if (!v_img) return fail(MSPLAT_CUDA_EINVAL, "null image gradient");
+    if (ctx->aux_frame)
+        return fail(MSPLAT_CUDA_EUNSUPPORTED, "render_backward of a render with a prior (aux mode) is not supported; "
+                                              "clear the prior with msplat_cuda_set_prior(ctx, NULL) first");
     if (num_points > 0 && (!means3d || !scales || !quats || !v_means || !v_scales || !v_quats || !v_features_dc ||
                            !v_opacities || (degree > 0 && !v_features_rest)))
         return fail(MSPLAT_CUDA_EINVAL, "null parameter or gradient pointer");
@@ -952,6 +1163,7 @@ int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
                         &ctx->img[4], &ctx->img[5]};
     int64_t total = 0;
     for (const Buf *b : all) total += (int64_t)b->bytes;
+    for (const Buf &b : ctx->pri) total += (int64_t)b.bytes;
     return total;
 }
 
@@ -998,6 +1210,12 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         {"v_mean3d", &ctx->v_mean3d, n * 3},
         {"v_scale", &ctx->v_scale, n * 3},
         {"v_quat", &ctx->v_quat, n * 4},
+        {"out_depth", &ctx->pri[PB_DEPTH], npix},
+        {"bg_img", &ctx->pri[PB_BG], npix * 3},
+        {"v_aux", &ctx->pri[PB_VAUX], npix * 2},
+        {"v_depth", &ctx->pri[PB_VDEPTH], n},
+        {"out_adj", &ctx->pri[PB_ADJ], npix * 3},
+        {"v_adj", &ctx->pri[PB_VADJ], npix * 3},
     };
     for (const Entry &e : table)
         if (!std::strcmp(e.name, name)) {

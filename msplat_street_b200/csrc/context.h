@@ -150,6 +150,24 @@ struct TrainBatchState {
     }
 };
 
+// Buffers of the prior-guided extras (msplat_cuda_set_prior), by index into
+// msplat_cuda_ctx::pri.
+enum PriBuf {
+    PB_DEPTH,     // expected-depth numerator (H, W)
+    PB_BG,        // per-pixel background (H, W, 3)
+    PB_VAUX,      // dL/d(depth numerator, alpha) (H, W, 2)
+    PB_SLOTS_D,   // depth gradient per intersection
+    PB_VDEPTH,    // dL/d(view depth) per Gaussian (keep_grads)
+    PB_TERMS,     // per-pixel loss terms (3, H, W)
+    PB_ROWS,      // per-row loss-term sums (H, 3) double
+    PB_ADJ,       // exposure-adjusted render (H, W, 3)
+    PB_VADJ,      // its gradient (H, W, 3)
+    PB_EXPO,      // exposure-gradient block partials (double)
+    PB_SKY_IDX, PB_SKY_W, PB_SKY_G, PB_SKY_COUNT, PB_SKY_OFF, PB_SKY_PART, PB_SKY_TOTAL,  // sky backward
+    PB_SKY_K0, PB_SKY_K1, PB_SKY_V0, PB_SKY_V1, PB_SKY_RS,
+    PB_COUNT
+};
+
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
     int raster_variant = 0;  // option "raster_variant": index into RASTER_VARIANTS
@@ -176,6 +194,11 @@ struct msplat_cuda_ctx {
     Buf dkeys[2], dvals[2], dcounts, doff;
     // image pipeline scratch: metrics (moments, terms, row sums) and RGBA8 packing
     Buf img[6];
+    // prior-guided extras: the prior in force, whether the last frame ran in aux
+    // mode, and their buffers
+    bool has_prior = false, aux_frame = false;
+    msplat_cuda_prior prior{};
+    Buf pri[PB_COUNT];
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
     int32_t *h_count = nullptr;  // pinned readback of the densified count
     // batched render: device view descriptors, their pinned staging copy, the
@@ -202,6 +225,12 @@ struct msplat_cuda_ctx {
             b->ptr = nullptr;
             b->bytes = 0;
         }
+        for (Buf &b : pri) {
+            if (b.ptr) cudaFree(b.ptr);
+            b.ptr = nullptr;
+            b.bytes = 0;
+        }
+        aux_frame = false;
         tb.release();  // its graph refers to the buffers just freed
         if (h_total) cudaFreeHost(h_total);
         h_total = nullptr;

@@ -77,6 +77,11 @@ struct RasterArgs {
     float *tstore;
     int32_t *tcount;
     int tcap;
+    // prior-guided aux mode (launch_raster_fwd_aux): expected-depth numerator
+    // sum_i z_i w_i per pixel, and the per-pixel background -- read from bg_img when
+    // a sky pass filled it (sky_bg = 1), else bg written there
+    float *out_depth, *bg_img;
+    int sky_bg;
 };
 // Rasterizer staging variants, chosen at run time (an autotuner times them): the
 // Gaussians staged in shared memory per forward round and per backward round, and
@@ -91,6 +96,7 @@ constexpr RasterVariant RASTER_VARIANTS[N_RASTER_VARIANTS] = {
 inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v : 0; }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
+void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st);
 
 // A batch of views rendered by one projection, one sort and one persistent raster
 // launch. Instances (view, Gaussian) and tiles (view, tile) are numbered globally,
@@ -133,8 +139,13 @@ struct RasterBwdArgs {
     float *slots;  // 9 floats per sorted intersection
     const float *tstore;  // stored-transmittance mode, as RasterArgs (null = divide)
     const int32_t *tcount;
+    // aux mode (launch_raster_bwd_aux): per-pixel background, dL/d(depth numerator,
+    // alpha) per pixel, and the depth-gradient slot of each intersection
+    const float *bg_img, *v_aux;
+    float *slots_depth;
 };
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant = 0);
+void launch_raster_bwd_aux(const RasterBwdArgs &a, cudaStream_t st);
 
 struct SsimArgs {
     int W, H;
@@ -156,8 +167,9 @@ struct BackwardArgs {
     const int32_t *radii, *n_tiles, *inv;
     const int64_t *offsets;
     const float *slots;
+    const float *slots_depth;  // aux mode: one depth-gradient value per intersection (else null)
     // optional per-Gaussian gradient outputs (null to skip)
-    float *v_xy, *v_conic, *v_rgb, *v_opacity, *v_mean3d, *v_scale, *v_quat;
+    float *v_xy, *v_conic, *v_rgb, *v_opacity, *v_mean3d, *v_scale, *v_quat, *v_depth;
     float *g_dc, *g_rest;  // SH gradients as arrays (gradient-only mode, no Adam)
     // Adam: groups means, scales, quats, dc, rest, opacity
     int do_adam;
@@ -168,6 +180,7 @@ struct BackwardArgs {
     // densification statistics (null to skip)
     float *vis_counts, *xys_grad_norm, *max_2d_size;
     float inv_max_dim;
+    float log_max_scale_ratio;  // needle cap after the scale update; <= 0 disables
 };
 void launch_backward_adam(const BackwardArgs &a, cudaStream_t st);
 
@@ -232,6 +245,53 @@ void launch_image_metrics(const float *a, const float *b, int h, int w, const Me
 void launch_pack_rgba8(const float *img, uint32_t n, uint8_t *out, cudaStream_t st);
 void launch_finalize_depth(const float *d, const float *t, uint32_t n, float inv_scale, float *od, float *oa,
                            cudaStream_t st);
+
+// Prior-guided extras (prior.cu; core/metal/bindings.h:43-77).
+struct SkyArgs {
+    const float *tex;     // (tex_h, tex_w, 3), device
+    int tex_w, tex_h;
+    float frame[9];       // up, e1 (azimuth 0), e2 (azimuth 90 degrees)
+    float fx, fy, cx, cy;
+    float viewmat[16];    // row-major world-to-camera
+};
+struct PriorLossArgs {
+    int W, H;
+    const float *final_T, *out_depth;
+    const float *prior_depth;     // (ph, pw) or null
+    const uint8_t *prior_aux;     // (ph, pw, 4) or null
+    int pw, ph, use_depth, use_sky, mask_photometric;
+    float depth_weight, sky_weight, fill_weight, huber, min_alpha, inv_npix;
+    float *v_photo;  // (H, W, 3): pixels outside "keep" are zeroed
+    float *v_aux;    // (H, W, 2): dL/d(depth numerator), dL/d(alpha)
+    float *terms;    // (3, H, W) per-pixel loss terms, null to skip them
+};
+struct ExposureArgs {
+    float *params, *exp_avg, *exp_avg_sq;  // (num_cams, 12)
+    float *grad;                           // [12] or null
+    int cam;
+    float step_size, bc2, reg, beta1, beta2, eps;
+};
+struct SkyAdamArgs {
+    float *tex, *grad, *exp_avg, *exp_avg_sq;  // (tex_h, tex_w, 3)
+    float step_size, bc2, beta1, beta2, eps;
+};
+struct SkyScratch {
+    uint4 *tap_idx;      // per pixel
+    float4 *tap_w, *tap_g;
+    int32_t *count, *off, *scan_part, *d_total;
+    uint32_t *keys[2], *vals[2];  // 4 per pixel
+    void *radix_scratch;          // radix_scratch_bytes(4 * pixels)
+};
+void launch_sky_background(const SkyArgs &s, int W, int H, float *bg_img, cudaStream_t st);
+// rows: 3 * H doubles (only with a.terms and loss_terms)
+void launch_prior_loss(const PriorLossArgs &a, double *rows, float *loss_terms, cudaStream_t st);
+void launch_exposure_apply(const float *img, const float *P, int64_t n, float *out, cudaStream_t st);
+int exposure_blocks(int64_t n);  // partials: 12 doubles per block
+void launch_exposure_backward_adam(const float *img, const float *v_adj, int64_t n, float *v_img, double *partials,
+                                   const ExposureArgs &e, cudaStream_t st);
+void launch_sky_backward_adam(const SkyArgs &s, int W, int H, const float *final_T, const float *v_img,
+                              const SkyAdamArgs &a, SkyScratch &sc, cudaStream_t st);
+void launch_needle_cap(float *scales, int n, float log_max, cudaStream_t st);
 
 struct KnnScratch {
     unsigned int *bounds;  // 6 ordered-bit floats: min xyz, max xyz

@@ -38,7 +38,9 @@ constexpr int BWD_WARPS = TILE_PIX / 32;
 // One 16x16 tile: `tile` indexes tile_start / tile_end (a global tile id in a batch),
 // (tx, ty) is its position in its view. Every thread of the block must call it.
 // FB: Gaussians staged in shared memory per round (at most one per thread).
-template <int FB>
+// AUX: also the expected-depth numerator and a per-pixel background
+// (rasterize_forward_aux, core/cpu/msplat_cpu.cpp:574-626 with f.aux).
+template <int FB, bool AUX = false>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
                                                 float4 *s1, float4 *s2) {
     int lx, ly;
@@ -51,7 +53,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     const int w = threadIdx.x >> 5;
     const float bx0 = (float)(tx * TILE + ((w & 1) << 3)), bx1 = bx0 + 7.f;
     const float by0 = (float)(ty * TILE + ((w >> 1) << 2)), by1 = by0 + 3.f;
-    float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f;
+    float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f, depth = 0.f;
     int last = start - 1;
     bool done = !inside;
     const size_t npix = (size_t)a.W * a.H;
@@ -91,6 +93,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
             cr = fmaxf(B.z + 0.5f, 0.f) * vis + cr;
             cg = fmaxf(B.w + 0.5f, 0.f) * vis + cg;
             cb = fmaxf(C.x + 0.5f, 0.f) * vis + cb;
+            if (AUX) depth += C.y * vis;
             T = nT;
             last = b0 + j;
         }
@@ -100,16 +103,34 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     if (a.final_idx) a.final_idx[pid] = last;
     if (a.tcount) a.tcount[pid] = stored <= a.tcap ? stored : -1;
     float *o = a.out_img + 3 * (size_t)pid;
+    if (AUX) {
+        float *bp = a.bg_img + 3 * (size_t)pid;
+        float br = a.bg[0], bgg = a.bg[1], bb = a.bg[2];
+        if (a.sky_bg) {
+            br = bp[0];
+            bgg = bp[1];
+            bb = bp[2];
+        } else {
+            bp[0] = br;
+            bp[1] = bgg;
+            bp[2] = bb;
+        }
+        a.out_depth[pid] = depth;
+        o[0] = clamp01(br * T + cr);
+        o[1] = clamp01(bgg * T + cg);
+        o[2] = clamp01(bb * T + cb);
+        return;
+    }
     o[0] = clamp01(a.bg[0] * T + cr);
     o[1] = clamp01(a.bg[1] * T + cg);
     o[2] = clamp01(a.bg[2] * T + cb);
 }
 
-template <int FB>
+template <int FB, bool AUX = false>
 __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     const int tile = blockIdx.x;
-    raster_fwd_tile<FB>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
+    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
@@ -174,22 +195,27 @@ void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter,
 // Gaussians are staged in shared memory per round.
 constexpr int PB_STRIDE = 36;  // floats per row: 32 lanes + pad, keeps float4 rows conflict-free
 
-template <int BB, int SB>
+// NG: gradient values per intersection, 9 (xy conic rgb opacity) or 10 with the
+// aux mode's depth gradient
+template <int BB, int SB, int NG = 9>
 constexpr size_t raster_bwd_smem() {
-    return sizeof(float4) * 3 * BB + sizeof(float) * BWD_WARPS * BB * 9 + sizeof(float) * BWD_WARPS * SB * 9 * PB_STRIDE +
-           16;
+    return sizeof(float4) * 3 * BB + sizeof(float) * BWD_WARPS * BB * NG +
+           sizeof(float) * BWD_WARPS * SB * NG * PB_STRIDE + 16;
 }
 
 // One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
 // global tile id in a batch), (tx, ty) is its position in its view. Every thread of
-// the block calls it; it ends with the block's shared memory free for reuse.
-template <int BB, int SB>
+// the block calls it; it ends with the block's shared memory free for reuse. AUX: the
+// per-pixel background is the pixel's own, and the expected-depth / alpha cotangents
+// enter v_alpha and a tenth value per intersection (the aux branch of :959-1031).
+template <int BB, int SB, bool AUX = false>
 __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
                                                 int &kmax) {
-    constexpr int BWD_BATCH = BB, SUB = SB, SUB_OUT = SB * 9;
+    constexpr int NG = AUX ? 10 : 9;
+    constexpr int BWD_BATCH = BB, SUB = SB, SUB_OUT = SB * NG;
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
-    float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][9]
-    float *pbuf = red + BWD_WARPS * BWD_BATCH * 9;            // [BWD_WARPS][SUB_OUT][PB_STRIDE]
+    float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][NG]
+    float *pbuf = red + BWD_WARPS * BWD_BATCH * NG;           // [BWD_WARPS][SUB_OUT][PB_STRIDE]
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -200,7 +226,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     const float bx0 = (float)(tx * TILE + ((warp & 1) << 3)), bx1 = bx0 + 7.f;
     const float by0 = (float)(ty * TILE + ((warp >> 1) << 2)), by1 = by0 + 3.f;
     const int pid = py * a.W + px;
-    float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f;
+    float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f, vd = 0.f, vaa = 0.f;
+    float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
     int kf = start - 1;
     if (inside) {
         Tf = a.final_T[pid];
@@ -210,6 +237,15 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         vr = v[0];
         vg = v[1];
         vb = v[2];
+        if (AUX) {
+            const float2 va2 = reinterpret_cast<const float2 *>(a.v_aux)[pid];
+            vd = va2.x;
+            vaa = va2.y;
+            const float *bp = a.bg_img + 3 * (size_t)pid;
+            bgr = bp[0];
+            bgg = bp[1];
+            bgb = bp[2];
+        }
     }
     if (threadIdx.x == 0) kmax = start - 1;
     __syncthreads();
@@ -217,8 +253,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     __syncthreads();
     const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
     // T_final * bg, then the -ra * (T_final * bg) term of the reference's v_alpha
-    const float tbr = Tf * a.bg[0], tbg = Tf * a.bg[1], tbb = Tf * a.bg[2];
+    const float tbr = Tf * bgr, tbg = Tf * bgg, tbb = Tf * bgb;
     float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
+    float bd = 0.f, ba = 0.f;             // aux: accumulated depth and alpha behind
     const float fpx = (float)px, fpy = (float)py;
     float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
     // stored-transmittance mode: contributions left to pop, -1 = recover T by division
@@ -241,7 +278,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                 const int k = b_start + j;
                 const float4 A = s0[j], C = s2[j];
                 if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
-                float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                float g[NG];
+#pragma unroll
+                for (int c = 0; c < NG; c++) g[c] = 0.f;
                 bool hit = false;
                 if (inside && k <= kf) {
                     const float4 B = s1[j];
@@ -277,7 +316,14 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                                         ib = __fmaf_rn(-bb, ra, nra * tbb);
                             const float orr = __fmaf_rn(cr, T, ir), og = __fmaf_rn(cg, T, ig),
                                         ob = __fmaf_rn(cb, T, ib);
-                            const float va = __fmaf_rn(orr, vr, __fmaf_rn(og, vg, ob * vb));
+                            float va = __fmaf_rn(orr, vr, __fmaf_rn(og, vg, ob * vb));
+                            if (AUX) {
+                                const float z = C.y;
+                                va += __fmaf_rn(__fmaf_rn(-bd, ra, z * T), vd, __fmaf_rn(-ba, ra, T) * vaa);
+                                bd = __fmaf_rn(z, fac, bd);
+                                ba += fac;
+                                g[9] = fac * vd;
+                            }
                             br = __fmaf_rn(cr, fac, br);
                             bgc = __fmaf_rn(cg, fac, bgc);
                             bb = __fmaf_rn(cb, fac, bb);
@@ -299,15 +345,15 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                 }
                 if (__ballot_sync(0xffffffffu, hit)) {
                     any |= 1u << (j - jlo);
-                    float *row = mypb + (j - jlo) * 9 * PB_STRIDE + lane;
-    #pragma unroll
-                    for (int c = 0; c < 9; c++) row[c * PB_STRIDE] = g[c];
+                    float *row = mypb + (j - jlo) * NG * PB_STRIDE + lane;
+#pragma unroll
+                    for (int c = 0; c < NG; c++) row[c * PB_STRIDE] = g[c];
                 }
             }
             __syncwarp();
             // this warp's sums for the sub-batch: output o = jj * 9 + c
             for (int o = lane; o < SUB_OUT; o += 32) {
-                const int jj = o / 9, c = o - jj * 9;
+                const int jj = o / NG, c = o - jj * NG;
                 if (jlo + jj > jhi) continue;
                 float s = 0.f;
                 if ((any >> jj) & 1u) {
@@ -321,32 +367,35 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                         s += v.w;
                     }
                 }
-                red[(warp * BWD_BATCH + jlo + jj) * 9 + c] = s;
+                red[(warp * BWD_BATCH + jlo + jj) * NG + c] = s;
             }
             __syncwarp();
         }
         __syncthreads();
-        for (int idx = threadIdx.x; idx < cnt * 9; idx += blockDim.x) {
-            const int j = idx / 9, c = idx - j * 9;
+        for (int idx = threadIdx.x; idx < cnt * NG; idx += blockDim.x) {
+            const int j = idx / NG, c = idx - j * NG;
             float s = 0.f;
 #pragma unroll
-            for (int w = 0; w < BWD_WARPS; w++) s += red[(w * BWD_BATCH + j) * 9 + c];
-            a.slots[(size_t)(b_start + j) * 9 + c] = s;
+            for (int w = 0; w < BWD_WARPS; w++) s += red[(w * BWD_BATCH + j) * NG + c];
+            if (c < 9) a.slots[(size_t)(b_start + j) * 9 + c] = s;
+            else a.slots_depth[b_start + j] = s;
         }
         __syncthreads();
     }
     // intersections above every pixel's last contributor get zero slots
-    for (int k = kend + threadIdx.x; k < end; k += blockDim.x)
+    for (int k = kend + threadIdx.x; k < end; k += blockDim.x) {
 #pragma unroll
         for (int c = 0; c < 9; c++) a.slots[(size_t)k * 9 + c] = 0.f;
+        if (AUX) a.slots_depth[k] = 0.f;
+    }
 }
 
-template <int BB, int SB>
+template <int BB, int SB, bool AUX = false>
 __global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_kernel(RasterBwdArgs a) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
     const int tile = blockIdx.x;
-    raster_bwd_tile<BB, SB>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
+    raster_bwd_tile<BB, SB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
 }
 
 // Persistent backward over the tiles of a batch of views, pulling global tile ids
@@ -380,6 +429,14 @@ __global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_batch_kernel(const Ras
 template <int FB>
 void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
     raster_fwd_kernel<FB><<<T, TILE_PIX, 0, st>>>(a);
+}
+
+// The aux forward runs the default staging only (the reference too forces one
+// rasterizer in this mode, core/metal/bindings.h:44-46).
+void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    raster_fwd_kernel<128, true><<<T, TILE_PIX, 0, st>>>(a);
 }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
@@ -431,6 +488,19 @@ void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
     MSPLAT_BWD_VARIANTS(X)
 #undef X
     bwd_launch<64, 4>(a, T, st);
+}
+
+// The aux backward, default staging only (as launch_raster_fwd_aux).
+void launch_raster_bwd_aux(const RasterBwdArgs &a, cudaStream_t st) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    constexpr size_t smem = raster_bwd_smem<64, 4, 10>();
+    static const bool attr = [] {
+        cudaFuncSetAttribute(raster_bwd_kernel<64, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return true;
+    }();
+    (void)attr;
+    raster_bwd_kernel<64, 4, true><<<T, TILE_PIX, smem, st>>>(a);
 }
 
 void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,

@@ -551,6 +551,9 @@ extern "C" int msplat_cuda_train_batch(msplat_cuda_ctx *ctx, int num_points, flo
                                        float adam_eps, float *vis_counts, float *xys_grad_norm, float *max_2d_size,
                                        float *const *grads_out, float *losses_out) {
     if (!ctx) return fail(MSPLAT_CUDA_EINVAL, "null context");
+    if (ctx->has_prior)
+        return fail(MSPLAT_CUDA_EUNSUPPORTED, "a prior (msplat_cuda_set_prior) applies to msplat_cuda_train_step only; "
+                                              "clear it before msplat_cuda_train_batch");
     StepArgs a;
     a.n = num_points;
     a.nv = n_views;

@@ -207,7 +207,7 @@ int64_t orc_frame(const char *name, void **ptr) {
     REF_T0("out_depth", f.out_depth, f.aux ? npix : 0)
     REF_T0("bg_img", f.bg_img, f.aux ? npix * 3 : 0)
     REF_V("v_aux", f.v_aux, f.aux ? npix * 2 : 0)
-    REF_V("v_depth", f.v_depth, (int64_t)f.v_depth.size())
+    REF_V("v_depth", f.v_depth, std::min<int64_t>((int64_t)f.v_depth.size(), n))
     REF_T0("out_adj", f.out_adj, f.out_adj.defined() ? f.out_adj.numel() : 0)
     REF_T0("v_adj", f.v_adj, f.v_adj.defined() ? f.v_adj.numel() : 0)
 #undef REF_V
