@@ -11,8 +11,10 @@ Restates core/src/model.cpp's training-side host code over the C-ABI:
  * SH degree ramp degrees_to_use = min(step // sh_degree_interval, sh_degree) (:535).
 The camera set-up (prepareCam) is msplat_street_b200.camera.prepare_cam. The public
 surface mirrors the reference's TrainingConfig / TrainingStats / GaussianTrainer
-(python/msplat/_core.pyi:157-267) for in-memory datasets; file loaders and the
-prior-guided "street" extras are outside this backend.
+(python/msplat/_core.pyi:157-267) for in-memory datasets. Prior-guided training
+(depth / sky / mask priors, learned sky, exposure, needle cap) follows
+Model::configurePriors and the per-step PriorStep (model.cpp:548-625, 811-858), with
+the prior maps built by msplat_street_b200.priors.
 """
 from __future__ import annotations
 
@@ -25,7 +27,8 @@ import numpy as np
 import torch
 
 from . import formats
-from .backend import AdamState, Context, GaussianParams
+from . import priors as _priors
+from .backend import AdamState, Context, GaussianParams, PriorStep
 from .camera import CameraSetup, prepare_cam
 
 LR_INIT = (0.00016, 0.005, 0.001, 0.0025, 0.000125, 0.05)  # model.cpp:100
@@ -133,6 +136,13 @@ class GaussianTrainer:
         self.last_loss = None
         self.radii_ready = False
         self.max_dim = max(max(v.width, v.height) for v in dataset.views) if dataset.views else 1
+        # prior-guided training (configure_priors)
+        self.prior_opts: Optional[_priors.PriorOptions] = None
+        self.cam_priors: List[Optional[_priors.CameraPrior]] = [None] * len(dataset.views)
+        self._prior_maps: List[Optional[tuple]] = [None] * len(dataset.views)
+        self.sky: Optional[dict] = None
+        self.exposure: Optional[dict] = None
+        self.prior_loss_terms: Optional[torch.Tensor] = None
 
     # -- capacity buffers (model.cpp:81-193) ------------------------------------------
     def _setup_buffers(self, p: GaussianParams):
@@ -213,6 +223,125 @@ class GaussianTrainer:
             self.ctx.opacity_reset(self.buf[5][:n], self.m1[5][:n], self.m2[5][:n], n, RESET_LOGIT)
         self.stats = None
 
+    # -- prior-guided training (model.cpp:548-625, 811-858) ------------------------------
+    def configure_priors(self, opts: "_priors.PriorOptions",
+                         cam_priors: Optional[Sequence[Optional["_priors.CameraPrior"]]] = None) -> None:
+        """Model::configurePriors: per-camera prior maps (CameraPrior, e.g. from
+        priors.load_camera_prior; None where a camera has none), the learned sky's
+        frame and initial texture, per-camera exposure at identity, the loss terms."""
+        if self.batched and opts.active():
+            raise ValueError("prior-guided training runs one view per step (views_per_step = 1, no graph)")
+        self.prior_opts = opts
+        n = len(self.ds.views)
+        cps = list(cam_priors) if cam_priors is not None else [None] * n
+        if len(cps) != n:
+            raise ValueError(f"{len(cps)} camera priors for {n} views")
+        self.cam_priors = cps if opts.wants_prior_files() else [None] * n
+        self._prior_maps = [None if cp is None else
+                            (torch.from_numpy(np.ascontiguousarray(cp.depth, np.float32)).to(self.device),
+                             torch.from_numpy(np.ascontiguousarray(cp.aux, np.uint8)).to(self.device))
+                            for cp in self.cam_priors]
+        self.sky = None
+        if opts.learn_sky:
+            if opts.sky_width < 4 or opts.sky_height < 2:
+                raise ValueError("sky texture must be at least 4x2")
+            frame = _priors.compute_sky_frame([v.cam_to_world for v in self.ds.views])
+            tex = _priors.init_sky_texture(self.ds.views, self.cam_priors, frame, opts.sky_width, opts.sky_height)
+            t = torch.from_numpy(tex).to(self.device)
+            self.sky = {"frame": frame, "steps": 0, "tex": t, "grad": torch.zeros_like(t),
+                        "exp_avg": torch.zeros_like(t), "exp_avg_sq": torch.zeros_like(t)}
+        self.exposure = None
+        if opts.exposure and n:
+            params = torch.zeros((n, 12), dtype=torch.float32, device=self.device)
+            params[:, 0] = params[:, 4] = params[:, 8] = 1.0
+            self.exposure = {"params": params, "exp_avg": torch.zeros_like(params),
+                             "exp_avg_sq": torch.zeros_like(params),
+                             "grad": torch.zeros(12, dtype=torch.float32, device=self.device), "steps": [0] * n}
+        self.prior_loss_terms = torch.zeros(4, dtype=torch.float32, device=self.device)
+
+    def _priors_active(self) -> bool:
+        return self.prior_opts is not None and self.prior_opts.active()
+
+    def _render_prior(self, force_aux: bool = False) -> Optional[PriorStep]:
+        """renderPriorStep (model.cpp:549-561): the learned sky, or aux for depth renders."""
+        ps = PriorStep(aux=force_aux)
+        if self.prior_opts is not None and self.prior_opts.learn_sky and self.sky is not None:
+            ps.aux = ps.sky = True
+            ps.sky_tex = self.sky["tex"]
+            ps.sky_frame = tuple(float(x) for x in self.sky["frame"])
+        return ps if ps.aux else None
+
+    def _train_prior(self, ci: int, step: int, adam: AdamState) -> PriorStep:
+        """trainPriorStep (model.cpp:576-625) for camera ci at training step ``step``;
+        advances the sky's and the camera's exposure Adam step counts."""
+        o = self.prior_opts
+        f = np.float32
+        ps = self._render_prior(False) or PriorStep()
+        cp, maps = self.cam_priors[ci], self._prior_maps[ci]
+        depth_w = _priors.depth_weight_at(o, step, self.cfg.iterations) if cp is not None and cp.has_depth else 0.0
+        sky_terms = cp is not None and cp.has_sky and (o.sky_alpha_weight > 0 or o.fill_weight > 0)
+        masks = cp is not None and cp.has_mask and o.use_masks
+        ps.aux = ps.aux or depth_w > 0 or sky_terms or masks
+
+        def bias(lr, t):
+            return float(f(lr) / (f(1) - np.power(f(adam.beta1), f(t)))), float(
+                np.sqrt(f(1) - np.power(f(adam.beta2), f(t))))
+
+        if ps.sky:
+            self.sky["steps"] += 1
+            ps.sky_grad, ps.sky_exp_avg, ps.sky_exp_avg_sq = self.sky["grad"], self.sky["exp_avg"], self.sky[
+                "exp_avg_sq"]
+            ps.sky_step_size, ps.sky_bc2_sqrt = bias(o.sky_lr, self.sky["steps"])
+        if cp is not None:
+            ps.prior_depth, ps.prior_aux = maps
+            ps.has_depth, ps.has_sky_mask = cp.has_depth, cp.has_sky
+        ps.depth_weight = depth_w
+        ps.sky_weight = o.sky_alpha_weight
+        ps.fill_weight = o.fill_weight
+        ps.huber_delta = o.depth_huber_delta
+        ps.min_alpha = o.depth_min_alpha
+        ps.mask_photometric = o.use_masks
+        ps.loss_terms = self.prior_loss_terms
+        if o.exposure and self.exposure is not None and 0 <= ci < len(self.exposure["steps"]):
+            self.exposure["steps"][ci] += 1
+            ps.exposure = True
+            ps.cam_index = ci
+            e = self.exposure
+            ps.expo_params, ps.expo_exp_avg, ps.expo_exp_avg_sq, ps.expo_grad = (e["params"], e["exp_avg"],
+                                                                                 e["exp_avg_sq"], e["grad"])
+            ps.expo_step_size, ps.expo_bc2_sqrt = bias(o.exposure_lr, e["steps"][ci])
+            ps.expo_reg = o.exposure_reg
+        if o.max_scale_ratio > 1.0:
+            ps.log_max_scale_ratio = float(f(math.log(f(o.max_scale_ratio))))
+        return ps
+
+    def prior_losses(self) -> dict:
+        """Mean prior losses of the last step (GaussianTrainer::prior_losses,
+        python/bindings.cpp:402-406). Synchronises."""
+        if self.prior_loss_terms is None:
+            return {"depth": 0.0, "sky": 0.0, "fill": 0.0}
+        t = self.prior_loss_terms.cpu().numpy()
+        return {"depth": float(t[0]), "sky": float(t[1]), "fill": float(t[2])}
+
+    def render_depth(self, cam_idx: int):
+        """Expected depth (dataset units) and alpha of a training camera
+        (Model::renderDepth, model.cpp:860-877): an aux render, then
+        msplat_finalize_depth. Returns two (H, W) float32 arrays."""
+        v = self.ds.views[cam_idx]
+        self.ctx.set_prior(self._render_prior(True))
+        self.ctx.render(self.params, v.setup, self.bg, degrees_to_use=self.degrees_to_use())
+        d, t = self.ctx.render_aux_outputs()
+        depth, alpha = self.ctx.finalize_depth(d, t, 1.0 / self.crs_scale)
+        return (depth.reshape(v.height, v.width).cpu().numpy(), alpha.reshape(v.height, v.width).cpu().numpy())
+
+    def save_sky(self, path: str) -> None:
+        """The learned sky texture as an 8-bit image (Model::saveSky, model.cpp:887-896)."""
+        if self.sky is None:
+            raise RuntimeError("No learned sky (enable learn_sky)")
+        from PIL import Image
+        tex = self.sky["tex"].cpu().numpy()
+        Image.fromarray(np.clip(tex * np.float32(255.0), 0.0, 255.0).astype(np.uint8)).save(path)
+
     # -- public API -----------------------------------------------------------------
     def step(self, sync_loss: bool = False, target: Optional[torch.Tensor] = None) -> TrainingStats:
         """One training iteration (GaussianTrainer::step, python/bindings.cpp:261-284)."""
@@ -224,6 +353,9 @@ class GaussianTrainer:
         if self.batched:
             if target is not None:
                 raise ValueError("a batched step takes its targets from the dataset")
+            if self._priors_active():
+                raise ValueError("prior-guided training runs one view per step")
+            self.ctx.set_prior(None)
             views = []
             for _ in range(self.views_per_step):
                 ci = self._next_camera()
@@ -240,6 +372,7 @@ class GaussianTrainer:
             gt = target if target is not None else self._targets[ci]
             if gt is None:
                 raise ValueError(f"view {ci} has no target image")
+            self.ctx.set_prior(self._train_prior(ci, self.current_step + 1, adam) if self._priors_active() else None)
             self.last_loss = self.ctx.train_step(self.params, adam, view.setup, self.bg, gt, self.stats,
                                                  ssim_weight=self.cfg.ssim_weight,
                                                  degrees_to_use=self.degrees_to_use(), sync_loss=sync_loss)
@@ -256,6 +389,7 @@ class GaussianTrainer:
                 callback(st)
 
     def render_tensor(self, setup: CameraSetup) -> torch.Tensor:
+        self.ctx.set_prior(self._render_prior(False))
         return self.ctx.render(self.params, setup, self.bg, degrees_to_use=self.degrees_to_use())
 
     def render(self, cam_idx: int) -> np.ndarray:
@@ -289,6 +423,14 @@ class GaussianTrainer:
         ck = formats.Checkpoint(self.current_step, self.cfg.sh_degree, self.adam_step,
                                 np.asarray(self.lrs, np.float32), LR_INIT[0], MEANS_LR_FINAL, self.params.numpy(),
                                 [b[:n].cpu().numpy() for b in self.m1], [b[:n].cpu().numpy() for b in self.m2])
+        if self.sky is not None:
+            ck.sky = {"frame": self.sky["frame"], "steps": self.sky["steps"], "tex": self.sky["tex"].cpu().numpy(),
+                      "exp_avg": self.sky["exp_avg"].cpu().numpy(),
+                      "exp_avg_sq": self.sky["exp_avg_sq"].cpu().numpy()}
+        if self.exposure is not None:
+            e = self.exposure
+            ck.exposure = {"params": e["params"].cpu().numpy(), "exp_avg": e["exp_avg"].cpu().numpy(),
+                           "exp_avg_sq": e["exp_avg_sq"].cpu().numpy(), "steps": np.asarray(e["steps"], np.int32)}
         formats.save_checkpoint(path, ck)
 
     def load_checkpoint(self, path: str) -> int:
@@ -305,6 +447,18 @@ class GaussianTrainer:
         self.adam_step = ck.adam_step
         self.current_step = ck.step
         self.stats = None
+        # the learned sky and exposure are adopted only when this trainer uses them with
+        # the same shapes (Model::loadCheckpoint, model.cpp:409-441)
+        if ck.sky is not None and self.sky is not None and ck.sky["tex"].shape == tuple(self.sky["tex"].shape):
+            for k in ("tex", "exp_avg", "exp_avg_sq"):
+                self.sky[k].copy_(torch.from_numpy(np.ascontiguousarray(ck.sky[k])))
+            self.sky["frame"] = np.asarray(ck.sky["frame"], np.float32).reshape(9)
+            self.sky["steps"] = int(ck.sky["steps"])
+        if (ck.exposure is not None and self.exposure is not None
+                and ck.exposure["params"].shape == tuple(self.exposure["params"].shape)):
+            for k in ("params", "exp_avg", "exp_avg_sq"):
+                self.exposure[k].copy_(torch.from_numpy(np.ascontiguousarray(ck.exposure[k])))
+            self.exposure["steps"] = [int(x) for x in ck.exposure["steps"]]
         return ck.step
 
     def evaluate(self, cam_idx: int):

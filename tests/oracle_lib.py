@@ -21,6 +21,7 @@ PATHS = {
     "reference": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref.so"),
     "reference_fast": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_fast.so"),
     "reference_formats": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_formats.so"),
+    "reference_priors": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_priors.so"),
 }
 
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")

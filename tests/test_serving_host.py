@@ -188,7 +188,7 @@ def test_server_continuous_batching_overlaps_slots():
 
     log = []
     srv = serving.RenderServer(st, [0.0] * 3, slots=3, max_batch=4,
-                               renderer_factory=lambda: Slow(log, delay=0.02))
+                               renderer_factory=lambda: Slow(log, delay=0.05))
     res = srv.run(_requests(40, 4, spacing=0.002), realtime=True)
     assert len(res) == 40
     assert peak[0] >= 2  # two or more batches were in flight together
