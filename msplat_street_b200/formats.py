@@ -3,8 +3,9 @@
 * Checkpoint v2 (``.msplat``; core/src/model.cpp:282-496): magic "MSPL", version, the
   step / active count / SH degree / Adam step, the six learning rates and the means
   schedule, the six parameter arrays, both Adam moments per group, then the learned
-  sky and per-image exposure sections (present flags; this backend has neither, so it
-  writes them absent and skips them on load, as a model without those features does).
+  sky and per-image exposure sections (present flags; written when the trainer uses
+  them, adopted on load only by a trainer configured with the same shapes, as
+  Model::loadCheckpoint does).
   Every array is ndim (u32), shape (i64 each), byte count (u64), float32 data.
 * PLY (core/src/loaders/save_gaussians.cpp:10-53 writer, :112-190 reader): the 3DGS
   layout -- xyz, zero normals, f_dc, f_rest transposed to (3, bases), opacity logit,
@@ -60,8 +61,8 @@ class Checkpoint:
     params: List[np.ndarray]  # means (N,3), scales (N,3), quats (N,4), dc (N,3), rest (N,B-1,3), opacities (N,1)
     exp_avg: List[np.ndarray]
     exp_avg_sq: List[np.ndarray]
-    sky: Optional[dict] = None  # frame (9,), steps, tex, exp_avg, exp_avg_sq (read, never produced here)
-    exposure: Optional[dict] = None  # params, exp_avg, exp_avg_sq, steps (read, never produced here)
+    sky: Optional[dict] = None  # frame (9,), steps, tex, exp_avg, exp_avg_sq
+    exposure: Optional[dict] = None  # params, exp_avg, exp_avg_sq, steps
 
     @property
     def num_active(self) -> int:

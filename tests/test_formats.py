@@ -168,7 +168,7 @@ def test_checkpoint_version1_and_optional_sections(tmp_path):
     got = formats.load_checkpoint(tmp_path / "v1.msplat")
     assert got.num_active == 10 and np.array_equal(got.params[4], ck.params[4])
     # a v2 file with a learned sky and exposure (written by models that use them) loads;
-    # the sections are kept for the caller, this backend does not use them
+    # the sections are kept for the caller (the trainer adopts them when it uses them)
     sky = {"frame": np.arange(9, dtype=np.float32), "steps": 77, "tex": np.ones((2, 4, 3), np.float32),
            "exp_avg": np.zeros((2, 4, 3), np.float32), "exp_avg_sq": np.zeros((2, 4, 3), np.float32)}
     expo = {"params": np.ones((5, 4), np.float32), "exp_avg": np.zeros((5, 4), np.float32),
