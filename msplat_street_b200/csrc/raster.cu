@@ -2,7 +2,10 @@
 //
 // One 256-thread CTA per tile, one pixel per thread. The tile's depth-sorted list is
 // walked in batches whose splat records are staged in shared memory; every thread
-// reads each record as a broadcast.
+// reads each record as a broadcast. Staging also clamps the colours once and marks
+// which of the tile's eight warp blocks (8x4 pixels each) the splat can reach at all
+// (its box and its ellipse's diagonal extents), so a warp passes over the splats that
+// miss its pixels with one bit test; the forward walks its splats by ballot.
 //
 // Forward: rasterize_forward (core/cpu/msplat_cpu.cpp:574-626): sigma < 0 or >= 5.55
 // skips, alpha = min(0.999, o * exp(-sigma)) with alpha < 1/255 skipped, and the pixel
@@ -10,7 +13,8 @@
 // leaves its loop when __syncthreads_count says all 256 pixels are done.
 //
 // Backward: rasterize_backward (:959-1031): back to front from final_idx, T recovered
-// by multiplying with 1/(1 - alpha), colour gradients gated on raw + 0.5 >= 0 and the
+// by multiplying with 1/(1 - alpha) (the hardware reciprocal: no decision depends on
+// T there), colour gradients gated on raw + 0.5 >= 0 and the
 // sigma gradients only for alpha < 0.999. Each (tile, Gaussian) pair -- one sorted
 // intersection -- gets one 9-float slot: xy(2) conic(3) rgb(3) opacity-logit(1),
 // reduced over the tile's pixels in a fixed order (lanes through a transposed
@@ -35,6 +39,55 @@ namespace msplat {
 
 constexpr int BWD_WARPS = TILE_PIX / 32;
 
+// A splat's colour channel as the rasterizers use it, max(raw + 0.5, 0), computed once
+// at staging. A channel clamped to zero is stored as -0.0, so its sign bit carries the
+// backward's gate (the gradient passes where raw + 0.5 >= 0): -0.0 * x + y == y and
+// +0.0 * x + y == y for every y the compositing sums take, so images do not change.
+__device__ __forceinline__ float staged_colour(float raw) {
+    const float c = raw + 0.5f;
+    return c >= 0.f ? c : -0.f;
+}
+
+// Which of a tile's eight 8x4 warp blocks (warp w covers columns 8 (w % 2) .. +7 and
+// rows 4 (w / 2) .. +3) a splat can reach with alpha >= 1/255: bit w set unless the
+// block lies outside the splat's box (x + ex < block x0 || x - ex > x1 || y + ey < y0
+// || y - ey > y1) or outside the ellipse's extent along either diagonal, x + y and
+// x - y (separating axes; rotated, elongated splats have boxes much larger than
+// themselves). The diagonal half-extents sqrt(2 L u^T C^-1 u), L = min(5.55,
+// ln(255 o)), are evaluated in double with margins (as the box is), so a block is
+// dropped only when no pixel in it can take part. Computed once per staged splat.
+__device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4 B, const float4 C, int tx,
+                                                    int ty) {
+    const float xr = A.x + C.z, xl = A.x - C.z, yb = A.y + C.w, yt = A.y - C.w;
+    uint32_t cols = 0u, mask = 0u;
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const float bx0 = (float)(tx * TILE + (c << 3)), bx1 = bx0 + 7.f;
+        if (!(xr < bx0 || xl > bx1)) cols |= 1u << c;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const float by0 = (float)(ty * TILE + (r << 2)), by1 = by0 + 3.f;
+        if (!(yb < by0 || yt > by1)) mask |= cols << (2 * r);
+    }
+    if (!mask) return 0u;
+    const double ca = A.z, cb = A.w, cc = B.x;  // conic
+    const double det = ca * cc - cb * cb;
+    const double L = fmin(5.55, log(255.0 * (double)B.y)) + 1e-2;
+    if (!(det > 0.0 && ca > 0.0 && cc > 0.0 && L > 0.0)) return mask;  // box only
+    const float hp = (float)(sqrt(2.0 * L * fmax(ca + cc - 2.0 * cb, 0.0) / det) * 1.001 + 0.5);
+    const float hm = (float)(sqrt(2.0 * L * fmax(ca + cc + 2.0 * cb, 0.0) / det) * 1.001 + 0.5);
+    const float sp = A.x + A.y, sd = A.x - A.y;
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+        const float bx0 = (float)(tx * TILE + ((w & 1) << 3)), bx1 = bx0 + 7.f;
+        const float by0 = (float)(ty * TILE + ((w >> 1) << 2)), by1 = by0 + 3.f;
+        if (sp + hp < bx0 + by0 || sp - hp > bx1 + by1 || sd + hm < bx0 - by1 || sd - hm > bx1 - by0)
+            mask &= ~(1u << w);
+    }
+    return mask;
+}
+
 // One 16x16 tile: `tile` indexes tile_start / tile_end (a global tile id in a batch),
 // (tx, ty) is its position in its view. Every thread of the block must call it.
 // FB: Gaussians staged in shared memory per round (at most one per thread).
@@ -42,17 +95,14 @@ constexpr int BWD_WARPS = TILE_PIX / 32;
 // (rasterize_forward_aux, core/cpu/msplat_cpu.cpp:574-626 with f.aux).
 template <int FB, bool AUX = false>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
-                                                float4 *s1, float4 *s2) {
+                                                float4 *s1, float4 *s2, uint8_t *sm) {
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
     const int start = a.tile_start[tile], end = a.tile_end[tile];
     const float fpx = (float)px, fpy = (float)py;
-    // this warp's 8x4 pixel block, for skipping Gaussians whose box misses it
-    const int w = threadIdx.x >> 5;
-    const float bx0 = (float)(tx * TILE + ((w & 1) << 3)), bx1 = bx0 + 7.f;
-    const float by0 = (float)(ty * TILE + ((w >> 1) << 2)), by1 = by0 + 3.f;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f, depth = 0.f;
     int last = start - 1;
     bool done = !inside;
@@ -64,38 +114,45 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
         const int k = b0 + threadIdx.x;
         if (threadIdx.x < FB && k < end) {
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
-            s0[threadIdx.x] = rec[0];
-            s1[threadIdx.x] = rec[1];
-            s2[threadIdx.x] = rec[2];
+            const float4 A = rec[0], B = rec[1], C = rec[2];
+            s0[threadIdx.x] = A;
+            s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
+            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
+            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, B, C, tx, ty);
         }
         __syncthreads();
         const int cnt = min(FB, end - b0);
-        for (int j = 0; j < cnt && !done; j++) {
-            const float4 A = s0[j], C = s2[j];
-            if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
-            const float4 B = s1[j];
-            const float dx = A.x - fpx, dy = A.y - fpy;
-            const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
-            if (sigma < 0.f || sigma >= 5.55f) continue;
-            const float alpha = fminf(0.999f, B.y * exp_ref(-sigma));
-            if (alpha < 1.f / 255.f) continue;
-            const float nT = T * (1.f - alpha);
-            if (nT <= 1e-4f) {
-                last = b0 + j - 1;
-                done = true;
-                break;
+        // this warp's splats in list order: 32 mask bits per ballot, then one per hit
+        for (int base = 0; base < cnt; base += 32) {
+            const int jl = base + lane;
+            unsigned bits = __ballot_sync(0xffffffffu, jl < cnt && ((sm[jl] >> w) & 1u));
+            while (bits && !done) {
+                const int j = base + __ffs(bits) - 1;
+                bits &= bits - 1u;
+                const float4 A = s0[j], B = s1[j], C = s2[j];
+                const float dx = A.x - fpx, dy = A.y - fpy;
+                const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
+                if (sigma < 0.f || sigma >= 5.55f) continue;
+                const float alpha = fminf(0.999f, B.y * exp_ref(-sigma));
+                if (alpha < 1.f / 255.f) continue;
+                const float nT = T * (1.f - alpha);
+                if (nT <= 1e-4f) {
+                    last = b0 + j - 1;
+                    done = true;
+                    break;
+                }
+                if (a.tstore) {
+                    if (stored < a.tcap) a.tstore[(size_t)stored * npix + pid] = T;
+                    stored++;
+                }
+                const float vis = alpha * T;
+                cr = B.z * vis + cr;  // staged colours: max(raw + 0.5, 0)
+                cg = B.w * vis + cg;
+                cb = C.x * vis + cb;
+                if (AUX) depth += C.y * vis;
+                T = nT;
+                last = b0 + j;
             }
-            if (a.tstore) {
-                if (stored < a.tcap) a.tstore[(size_t)stored * npix + pid] = T;
-                stored++;
-            }
-            const float vis = alpha * T;
-            cr = fmaxf(B.z + 0.5f, 0.f) * vis + cr;
-            cg = fmaxf(B.w + 0.5f, 0.f) * vis + cg;
-            cb = fmaxf(C.x + 0.5f, 0.f) * vis + cb;
-            if (AUX) depth += C.y * vis;
-            T = nT;
-            last = b0 + j;
         }
     }
     if (!inside) return;
@@ -129,8 +186,9 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
 template <int FB, bool AUX = false>
 __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
+    __shared__ uint8_t sm[FB];
     const int tile = blockIdx.x;
-    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2);
+    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
@@ -140,6 +198,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
 template <int FB>
 __global__ void __launch_bounds__(TILE_PIX) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
+    __shared__ uint8_t sm[FB];
     __shared__ int s_tile, s_lt;
     __shared__ RasterArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
     const int total_tiles = d.tile_off[d.n_views];  // read on the device: the launch is graph-capturable
@@ -157,7 +216,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_batch_kernel(const BatchD
         __syncthreads();
         const int t = s_tile, lt = s_lt;
         if (t >= total_tiles) break;
-        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2);
+        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2, sm);
     }
 }
 
@@ -200,7 +259,7 @@ constexpr int PB_STRIDE = 36;  // floats per row: 32 lanes + pad, keeps float4 r
 template <int BB, int SB, int NG = 9>
 constexpr size_t raster_bwd_smem() {
     return sizeof(float4) * 3 * BB + sizeof(float) * BWD_WARPS * BB * NG +
-           sizeof(float) * BWD_WARPS * SB * NG * PB_STRIDE + 16;
+           sizeof(float) * BWD_WARPS * SB * NG * PB_STRIDE + BB + 16;
 }
 
 // One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
@@ -216,6 +275,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
     float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][NG]
     float *pbuf = red + BWD_WARPS * BWD_BATCH * NG;           // [BWD_WARPS][SUB_OUT][PB_STRIDE]
+    uint8_t *sm = reinterpret_cast<uint8_t *>(pbuf + BWD_WARPS * SUB_OUT * PB_STRIDE);  // [BWD_BATCH] warp masks
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -223,8 +283,6 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     const int start = a.tile_start[tile], end = a.tile_end[tile];
     if (end <= start) return;  // block-uniform
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const float bx0 = (float)(tx * TILE + ((warp & 1) << 3)), bx1 = bx0 + 7.f;
-    const float by0 = (float)(ty * TILE + ((warp >> 1) << 2)), by1 = by0 + 3.f;
     const int pid = py * a.W + px;
     float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f, vd = 0.f, vaa = 0.f;
     float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
@@ -266,18 +324,20 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         const int cnt = b_end - b_start;
         if (threadIdx.x < cnt) {
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[b_start + threadIdx.x]);
-            s0[threadIdx.x] = rec[0];
-            s1[threadIdx.x] = rec[1];
-            s2[threadIdx.x] = rec[2];
+            const float4 A = rec[0], B = rec[1], C = rec[2];
+            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, B, C, tx, ty);
+            s0[threadIdx.x] = A;
+            s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
+            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
         }
         __syncthreads();
         for (int sb = (cnt - 1) / SUB; sb >= 0; sb--) {
             const int jlo = sb * SUB, jhi = min(cnt - 1, jlo + SUB - 1);
             unsigned any = 0u;  // bit jj: some lane of this warp touched Gaussian jlo + jj
             for (int j = jhi; j >= jlo; j--) {
+                if (!((sm[j] >> warp) & 1u)) continue;  // the splat cannot reach this warp's block
                 const int k = b_start + j;
                 const float4 A = s0[j], C = s2[j];
-                if (A.x + C.z < bx0 || A.x - C.z > bx1 || A.y + C.w < by0 || A.y - C.w > by1) continue;
                 float g[NG];
 #pragma unroll
                 for (int c = 0; c < NG; c++) g[c] = 0.f;
@@ -297,7 +357,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                             alpha = fminf(0.999f, op * exp_ref(-sigma));
                         if (alpha >= 1.f / 255.f) {
                             hit = true;
-                            const float ra = __frcp_rn(1.f - alpha);  // == 1.f / (1.f - alpha), IEEE
+                            // no decision depends on T here: the hardware reciprocal (within
+                            // an ulp or two) recovers it within the gradient tolerance
+                            const float ra = __fdividef(1.f, 1.f - alpha);
                             if (tj > 0) {
                                 tj--;
                                 T = a.tstore[(size_t)tj * npix + pid];  // T before this Gaussian, as stored
@@ -305,9 +367,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                                 T *= ra;  // recovered by division (core/cpu/msplat_cpu.cpp:996-997)
                             }
                             const float fac = alpha * T;
-                            const float rawr = B.z, rawg = B.w, rawb = C.x;
-                            const float cr = fmaxf(rawr + 0.5f, 0.f), cg = fmaxf(rawg + 0.5f, 0.f),
-                                        cb = fmaxf(rawb + 0.5f, 0.f);
+                            const float cr = B.z, cg = B.w, cb = C.x;  // staged colours
                             // gradient arithmetic (no decision depends on it) uses fused
                             // multiply-adds; the reference's values are met within the
                             // gradient tolerance, not bit for bit
@@ -327,9 +387,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                             br = __fmaf_rn(cr, fac, br);
                             bgc = __fmaf_rn(cg, fac, bgc);
                             bb = __fmaf_rn(cb, fac, bb);
-                            if (rawr + 0.5f >= 0.f) g[5] = fac * vr;
-                            if (rawg + 0.5f >= 0.f) g[6] = fac * vg;
-                            if (rawb + 0.5f >= 0.f) g[7] = fac * vb;
+                            if (!signbit(cr)) g[5] = fac * vr;  // raw + 0.5 >= 0
+                            if (!signbit(cg)) g[6] = fac * vg;
+                            if (!signbit(cb)) g[7] = fac * vb;
                             if (alpha < 0.999f) {
                                 const float vs = -alpha * va;
                                 const float hv = 0.5f * vs;
