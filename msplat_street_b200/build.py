@@ -81,6 +81,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+GRADCHECK = os.path.join(BUILD, "gradcheck_cuda")
+
+
+def build_reference_gradcheck(ref_root: str, force: bool = False) -> str:
+    """Links the reference's own gradient check (tests/gradcheck.cpp, read where the
+    reference sources lie) against this library through integration/bindings_cuda.cpp,
+    the bindings.h implementation over the C-ABI. Needs g++ and the reference tree;
+    the result runs without either."""
+    src = os.path.join(ref_root, "tests", "gradcheck.cpp")
+    shim = os.path.join(PKG, "integration", "bindings_cuda.cpp")
+    lib = build(force)
+    deps = [src, shim, lib, os.path.join(ROOT, "include", "msplat_cuda.h")]
+    if force or _stale(GRADCHECK, deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ref_root, "core", "metal"), "-I",
+               os.path.join(ref_root, "core", "include"), "-I", os.path.join(ROOT, "include"), "-o", GRADCHECK, src,
+               shim, "-L", PKG, "-lmsplat_cuda", "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"gradcheck build failed:\n{r.stdout}\n{r.stderr}")
+    return GRADCHECK
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")

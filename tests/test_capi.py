@@ -57,3 +57,16 @@ def test_argument_errors_are_status_codes():
     st = lib.msplat_cuda_ctx_set_option(ctx, b"no_such_option", 1)
     assert st == 1 and b"unknown option" in lib.msplat_cuda_last_error()
     lib.msplat_cuda_ctx_destroy(ctx)
+
+
+REF = os.environ.get("MSPLAT_REFERENCE_ROOT", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "core", "metal", "bindings.h")),
+                    reason="reference headers not present here")
+def test_bindings_shim_links_the_reference_gradcheck():
+    """integration/bindings_cuda.cpp implements every bindings.h function the
+    reference's callers use: its own gradient check links against it unchanged."""
+    from msplat_street_b200 import build
+    path = build.build_reference_gradcheck(REF)
+    assert os.path.exists(path) and os.access(path, os.X_OK)
