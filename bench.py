@@ -12,7 +12,9 @@ densification that falls in the window inside the timed step.
 value: iterations/s with the targets resident in HBM, device-timed with CUDA events
 per step (L2 flushed by a 256 MB write between steps, outside the events); e2e: the
 same schedule replayed through the public API with each step's target copied from
-pinned host memory and the loss read back, wall-clock timed. Training does not
+pinned host memory (on a copy stream, one step ahead, overlapping the previous
+step's kernels) and each step's loss read back into pinned memory (waited for once
+the next step is queued), wall-clock timed. Training does not
 shard without a gradient exchange, so N GPUs run N independent replicas ("replicas
 only", weak scaling); value is the sum over ranks of K / max-over-ranks time.
 
@@ -260,14 +262,28 @@ def run_ours(args, world, rank, local):
     host_targets = [t.cpu().pin_memory() for t in targets2]
     del targets2
     trainer2._targets = [None] * len(host_targets)
+    prefetch = TargetPrefetch(trainer2, host_targets, dev)
     for _ in range(args.warmup):
-        trainer2.step(target=_upload(trainer2, host_targets, dev), sync_loss=True)
+        trainer2.step(target=prefetch.next(), sync_loss=True)
+    # every step's loss is read back into pinned memory; the host waits for step i's
+    # value after queueing step i + 1, so reading it does not leave the GPU idle
+    loss_host = torch.zeros(2, dtype=torch.float32).pin_memory()
+    losses = []
     barrier(world, dev)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        trainer2.step(target=_upload(trainer2, host_targets, dev), sync_loss=True)
+    prev = None
+    for i in range(args.steps):
+        trainer2.step(target=prefetch.next())
+        ev = ctx2.read_loss_async(loss_host[i % 2:i % 2 + 1])
+        if prev is not None:
+            prev[0].synchronize()
+            losses.append(float(loss_host[prev[1]]))
+        prev = (ev, i % 2)
+    prev[0].synchronize()
+    losses.append(float(loss_host[prev[1]]))
     torch.cuda.synchronize()
+    assert len(losses) == args.steps and np.isfinite(losses).all(), "a step's loss was not read back"
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     barrier(world, dev)
     e2e = world * args.steps / e2e_s
@@ -506,13 +522,43 @@ def differentiation_report(dev):
     return out
 
 
-def _upload(trainer, host_targets, dev):
-    """Copy the next view's target from pinned host memory (the step's input)."""
-    import torch
-    if not trainer._order:
-        trainer._order = list(trainer._rng.permutation(len(trainer.ds.views)))
-    ci = trainer._order[-1]
-    return host_targets[ci].to(dev, non_blocking=True)
+class TargetPrefetch:
+    """Each step's target copied from pinned host memory on a copy stream, one step
+    ahead, so the upload of step i + 1 overlaps step i's kernels (a production input
+    pipeline). The camera schedule is the trainer's own: permutations are drawn from
+    its generator in the same sequence, only earlier."""
+
+    def __init__(self, trainer, host_targets, dev):
+        import torch
+        self.tr, self.host, self.dev = trainer, host_targets, dev
+        self.stream = torch.cuda.Stream(device=dev)
+        self.pending = self._issue(1)
+
+    def _camera(self, ahead: int) -> int:
+        tr = self.tr
+        while len(tr._order) < ahead:  # the permutation the trainer would draw next
+            tr._order = list(tr._rng.permutation(len(tr.ds.views))) + tr._order
+        return tr._order[-ahead]
+
+    def _issue(self, ahead: int):
+        import torch
+        ci = self._camera(ahead)
+        with torch.cuda.stream(self.stream):
+            t = self.host[ci].to(self.dev, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        return t, ev
+
+    def next(self):
+        """The next step's target, ready on the current stream; starts the following
+        step's upload."""
+        import torch
+        t, ev = self.pending
+        cur = torch.cuda.current_stream(self.dev)
+        cur.wait_event(ev)
+        t.record_stream(cur)
+        self.pending = self._issue(2)
+        return t
 
 
 def launches_per_step(n_isect: float) -> float:

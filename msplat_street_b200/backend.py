@@ -458,6 +458,21 @@ class Context:
         check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out), src, 4))
         return out
 
+    def read_loss_async(self, out: torch.Tensor) -> torch.cuda.Event:
+        """Enqueues a copy of the last train step's loss into ``out`` (a one-element
+        pinned host float32 tensor) behind the step's kernels and returns an event that
+        completes with the copy: the loss is read without stalling the host, so the next
+        step can be queued first."""
+        if out.is_cuda or out.dtype != torch.float32 or out.numel() < 1 or not out.is_pinned():
+            raise ValueError("out must be a pinned host float32 tensor")
+        self.bind_stream()
+        src = C.c_void_p()
+        check(self._lib.msplat_cuda_loss_device(self.handle, C.byref(src)))
+        check(self._lib.msplat_cuda_copy_buffer(self.handle, ptr(out), src, 4))
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream())
+        return ev
+
     # -- bindings.h:120-155 ----------------------------------------------------------
     def densify(self, n: int, buffers: List[torch.Tensor], exp_avg: List[torch.Tensor],
                 exp_avg_sq: List[torch.Tensor], grad_norm: torch.Tensor, vis_counts: torch.Tensor,

@@ -22,7 +22,8 @@ namespace msplat {
 constexpr int ST = 32;                     // output tile edge
 constexpr int SH_IN = ST + 20;             // input rows / cols with the 10-pixel halo
 constexpr int SH_F = ST + 10;              // derivative-field rows / cols (5-pixel halo)
-constexpr int SSIM_THREADS = 256;
+constexpr int SSIM_THREADS = 512;
+constexpr int SSIM_PPT = ST * ST / SSIM_THREADS;  // output pixels per thread
 __constant__ float kWin[11] = {0.0010283801f, 0.0075987581f, 0.0360007721f, 0.1093606895f,
                                0.2130055377f, 0.2660117249f, 0.2130055377f, 0.1093606895f,
                                0.0360007721f, 0.0075987581f, 0.0010283801f};
@@ -43,8 +44,10 @@ __device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, in
     const int W = a.W, H = a.H;
     const int x0 = bx * ST, y0 = by * ST;
     const float w = a.ssim_weight;
-    // each thread owns output pixels tid, tid+256, ... of the 32x32 tile
-    float ssim_acc[4] = {0.f, 0.f, 0.f, 0.f}, l1_acc[4] = {0.f, 0.f, 0.f, 0.f};
+    // each thread owns output pixels tid, tid + SSIM_THREADS, ... of the 32x32 tile
+    float ssim_acc[SSIM_PPT], l1_acc[SSIM_PPT];
+#pragma unroll
+    for (int u = 0; u < SSIM_PPT; u++) ssim_acc[u] = l1_acc[u] = 0.f;
     for (int c = 0; c < 3; c++) {
         // 1. inputs, zero outside the image
         for (int i = threadIdx.x; i < SH_IN * SH_IN; i += SSIM_THREADS) {
@@ -121,7 +124,7 @@ __device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, in
         // SSIM and L1 per owned pixel, channel by channel in order (the reference adds
         // channel 0, 1, 2 into ssim_pix / l1_pix)
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < SSIM_PPT; u++) {
             const int p = threadIdx.x + u * SSIM_THREADS;
             const int oy = p / ST, ox = p - oy * ST;
             const int gy = y0 + oy, gx = x0 + ox;
@@ -149,7 +152,7 @@ __device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, in
         __syncthreads();
         // 5. vertical back-convolution and the pixel gradient (:760-785)
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < SSIM_PPT; u++) {
             const int p = threadIdx.x + u * SSIM_THREADS;
             const int oy = p / ST, ox = p - oy * ST;
             const int gy = y0 + oy, gx = x0 + ox;
@@ -174,7 +177,7 @@ __device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, in
     // per-pixel loss in float, summed in double over the block in a fixed order
     double sum = 0.0;
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < SSIM_PPT; u++) {
         const int p = threadIdx.x + u * SSIM_THREADS;
         const int oy = p / ST, ox = p - oy * ST;
         if (y0 + oy < H && x0 + ox < W) sum += (double)(w * (1.0f - ssim_acc[u] / 3.0f) + (1.0f - w) * l1_acc[u] / 3.0f);
@@ -190,7 +193,7 @@ __device__ __forceinline__ void ssim_block(const SsimArgs &a, int bx, int by, in
     }
 }
 
-__global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_kernel(SsimArgs a) {
+__global__ void __launch_bounds__(SSIM_THREADS, 2) ssim_loss_kernel(SsimArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SsimSmem &s = *reinterpret_cast<SsimSmem *>(smem_raw);
     ssim_block(a, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, s);
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_kernel(SsimArgs a) {
 // target and gradient output), pulling global block ids from a counter. Block b of
 // view v writes partial boff[v] + (its index within the view), so each view's
 // partials sit in the order the single-image kernel writes them.
-__global__ void __launch_bounds__(SSIM_THREADS) ssim_loss_batch_kernel(const SsimArgs *views, const int *boff,
+__global__ void __launch_bounds__(SSIM_THREADS, 2) ssim_loss_batch_kernel(const SsimArgs *views, const int *boff,
                                                                        int n_views, int *counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SsimSmem &s = *reinterpret_cast<SsimSmem *>(smem_raw);

@@ -60,3 +60,16 @@ def test_exports(tmp_path):
     assert rgba.shape == (64, 96, 4) and rgba.dtype == np.uint8 and (rgba[..., 3] == 255).all()
     psnr, ssim, l1 = tr.evaluate(0)
     assert np.isfinite(psnr) and 0 < ssim <= 1 and l1 >= 0
+
+
+def test_read_loss_async_matches_the_synchronous_loss():
+    a, b = _trainer(), _trainer()
+    pinned = torch.zeros(1, dtype=torch.float32).pin_memory()
+    for _ in range(3):
+        a.step(sync_loss=True)
+        b.step()
+        ev = b.ctx.read_loss_async(pinned)
+        ev.synchronize()
+        assert float(pinned[0]) == a.last_loss
+    with pytest.raises(ValueError):
+        b.ctx.read_loss_async(torch.zeros(1))  # not pinned
