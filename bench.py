@@ -600,6 +600,74 @@ def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
             "avg_ms": ms, "algorithmic_bytes": algo}
 
 
+PROFILE_CASES = ("sort", "ssim", "adam", "densify")
+
+
+def profile_case(name: str, dev) -> dict:
+    """One stage at a size larger than the 126 MB L2, run twice (the second launch is
+    the one an ncu capture takes with -s 1 -c 1 on the stage's kernel), for the DRAM
+    traffic and achieved bandwidth of that kernel:
+      sort     stable radix sort of 32 M (u64 key, i32 value) pairs, 40 key bits (5 passes)
+      ssim     fused L1 + SSIM forward and backward of a 4096 x 4096 render
+      adam     backward/Adam of a training step over 1 M Gaussians (SH degree 3)
+      densify  clone / split / prune + compaction of 500 k Gaussians (capacity 2 M)"""
+    import torch
+    from msplat_street_b200 import autograd, scenes
+    from msplat_street_b200.backend import AdamState, Context, GaussianParams
+
+    ctx = Context()
+    g = torch.Generator(device=dev).manual_seed(7)
+    out = {"case": name}
+    if name == "sort":
+        n = 32 << 20
+        for _ in range(2):
+            keys = torch.randint(0, 1 << 40, (n,), device=dev, dtype=torch.int64, generator=g)
+            vals = torch.arange(n, device=dev, dtype=torch.int32)
+            ctx.radix_sort(keys, vals, 40)
+        out.update(pairs=n, key_bits=40, bytes_per_pair_pass=24)
+    elif name == "ssim":
+        h = w = 4096
+        img = torch.rand((h, w, 3), device=dev, generator=g)
+        gt = torch.rand((h, w, 3), device=dev, generator=g)
+        for _ in range(2):
+            loss = autograd.ssim_l1_loss(img.requires_grad_(), gt)
+            loss.backward()
+            img.grad = None
+        out.update(pixels=h * w, bytes_per_pixel=36)
+    elif name == "adam":
+        n = 1 << 20
+        p = GaussianParams.from_numpy(scenes.random_gaussians(n, 3, log_scale_mean=-5.0), dev)
+        cam = scenes.small_camera(512, 512, 600.0)
+        gt_img = torch.rand((512, 512, 3), device=dev, generator=g)
+        adam = AdamState.zeros_like(p, [1.6e-4, 5e-3, 1e-3, 2.5e-3, 1.25e-4, 0.05])
+        stats = tuple(torch.zeros(n, device=dev) for _ in range(3))
+        for _ in range(2):
+            ctx.train_step(p, adam, cam, np.zeros(3, np.float32), gt_img, stats)
+        torch.cuda.synchronize()
+        vis = int((ctx.frame("radii") > 0).sum())
+        out.update(gaussians=n, visible=vis, isects=ctx.num_isects(), dense_bytes_per_gaussian=264,
+                   sh_bytes_per_visible=1152, slot_bytes_per_isect=40)
+    elif name == "densify":
+        n, cap = 500_000, 2_000_000  # room for every Gaussian to be split and cloned
+        src = scenes.random_gaussians(n, 4, log_scale_mean=-4.0, log_scale_std=1.5)
+        strides = [3, 3, 4, 3, 45, 1]
+        for _ in range(2):
+            bufs = []
+            for a, st in zip(src.arrays(), strides):
+                b = torch.zeros((cap, st), device=dev)
+                b[:n] = torch.from_numpy(a.reshape(n, st)).to(dev)
+                bufs.append(b)
+            m1 = [torch.rand((cap, st), device=dev, generator=g) for st in strides]
+            m2 = [torch.rand((cap, st), device=dev, generator=g) for st in strides]
+            gn = torch.rand(n, device=dev, generator=g) * 4e-3
+            vc = torch.randint(1, 4, (n,), device=dev, generator=g).float()
+            ms = torch.rand(n, device=dev, generator=g) * 0.3
+            new_n = ctx.densify(n, bufs, m1, m2, gn, vc, ms, 512.0, 1234)
+        out.update(gaussians=n, capacity=cap, new_gaussians=new_n, floats_per_gaussian=59, arrays=3)
+    torch.cuda.synchronize()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -610,7 +678,13 @@ def main(argv=None):
     ap.add_argument("--serving-seconds", type=float, default=1.0,
                     help="length of each Poisson request stream in the serving report (0 = skip)")
     ap.add_argument("--no-batching", action="store_true", help="skip the batched-training report")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES,
+                    help="run one stage at a size larger than L2 (for an ncu capture) and exit")
     args = ap.parse_args(argv)
+    if args.profile_case:
+        import torch
+        print(json.dumps(profile_case(args.profile_case, torch.device("cuda", 0))))
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)
     try:

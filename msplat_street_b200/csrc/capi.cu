@@ -961,7 +961,9 @@ int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float gra
                 return fail(MSPLAT_CUDA_EINVAL, "null buffer for group %d", g);
         }
     }
-    const int64_t rows = 3 * (int64_t)std::max(N, 1);
+    a.cap = buf_capacity;
+    const int64_t rows = 4 * (int64_t)std::max(N, 1);  // a Gaussian may be split and cloned
+    if (rows > (int64_t)INT32_MAX) return fail(MSPLAT_CUDA_EINVAL, "msplat_densify: N (%d) too large", N);
     ENSURE(ctx->d_flags, 6 * rows, int32_t, flags);
     ENSURE(ctx->d_counts, 8 + scan_blocks((int)rows) + 1, int32_t, counts);
     ENSURE(ctx->d_scratch, rows * max_stride, float, scratch);
@@ -977,12 +979,20 @@ int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float gra
     s.n_dup = counts + 1;
     s.n_new = counts + 2;
     s.new_count = counts + 3;
+    s.overflow = counts + 4;
     s.scan_part = counts + 8;
     s.scratch = scratch;
     launch_densify(a, s, st);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(ctx->h_count, s.new_count, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    int32_t overflow = 0;
+    CUDA_TRY(cudaMemcpyAsync(&overflow, s.overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    if (overflow)
+        return fail(MSPLAT_CUDA_ECAPACITY,
+                    "msplat_densify: N + 2 x splits + clones exceeds buf_capacity (%d); a Gaussian can be both "
+                    "split and cloned, so up to 4 N rows are needed; the buffers are unchanged",
+                    buf_capacity);
     *new_count = *ctx->h_count;
     return MSPLAT_CUDA_OK;
 }

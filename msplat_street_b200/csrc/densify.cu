@@ -13,6 +13,11 @@
 //  4. cull (:1432-1448) over the N_new rows and order-preserving compaction of all 18
 //     buffers (6 parameters, 6 first moments, 6 second moments) through a scratch
 //     buffer, one buffer at a time (:1449-1464).
+// A Gaussian can be both split (large on screen) and cloned (small in the world), so
+// the rows after step 3 number up to 4N, not 3N as the reference's capacity check
+// assumes (its CPU port would then write past its buffers). Here every kernel from
+// step 3 on first checks N + 2 splits + clones against the capacity; when it does not
+// fit, nothing is written and the overflow flag is set (the host reports it).
 // Child and clone moments are zeroed. Counts live on the device; the host reads the
 // final count once (the reference's Metal backend also syncs there,
 // core/metal/msplat_metal.mm:1998-2001).
@@ -72,8 +77,21 @@ __device__ __forceinline__ V3 rand_normal3(uint32_t seed, uint32_t stream) {
     return V3{r0 * (float)cos((double)t0), r0 * (float)sin((double)t0), r1 * (float)cos((double)t1)};
 }
 
-__global__ void densify_split_kernel(DensifyArgs a, const int32_t *split, const int32_t *split_ord) {
+// rows after splits and clones, and whether they fit the buffers
+__device__ __forceinline__ bool rows_fit(const DensifyArgs &a, const int32_t *n_split, const int32_t *n_dup,
+                                         int64_t &total) {
+    total = (int64_t)a.n + 2 * (int64_t)(*n_split) + *n_dup;
+    return total <= a.cap;
+}
+
+__global__ void densify_split_kernel(DensifyArgs a, const int32_t *split, const int32_t *split_ord,
+                                     const int32_t *n_split, const int32_t *n_dup, int32_t *overflow) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t total;
+    if (!rows_fit(a, n_split, n_dup, total)) {
+        if (i == 0) *overflow = 1;
+        return;
+    }
     if (i >= a.n || !split[i]) return;
     const int ord = split_ord[i];
     float *means = a.buf[0], *scales = a.buf[1];
@@ -105,8 +123,11 @@ __global__ void densify_split_kernel(DensifyArgs a, const int32_t *split, const 
     for (int j = 0; j < 3; j++) scales[3 * i + j] -= a.log_size_fac;
 }
 
-__global__ void densify_dup_kernel(DensifyArgs a, const int32_t *dup, const int32_t *dup_ord, const int32_t *n_split) {
+__global__ void densify_dup_kernel(DensifyArgs a, const int32_t *dup, const int32_t *dup_ord, const int32_t *n_split,
+                                   const int32_t *n_dup) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t total;
+    if (!rows_fit(a, n_split, n_dup, total)) return;
     if (i >= a.n || !dup[i]) return;
     const int64_t d = (int64_t)a.n + 2 * (int64_t)(*n_split) + dup_ord[i];
     for (int j = 0; j < 3; j++) a.buf[0][3 * d + j] = a.buf[0][3 * i + j];
@@ -118,10 +139,11 @@ __global__ void densify_dup_kernel(DensifyArgs a, const int32_t *dup, const int3
 __global__ void densify_cull_kernel(DensifyArgs a, const int32_t *split, const int32_t *n_split,
                                     const int32_t *n_dup, int32_t *keep, int32_t *n_new) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t total = (int64_t)a.n + 2 * (int64_t)(*n_split) + *n_dup;
-    if (i == 0) *n_new = (int32_t)total;
-    if (i >= 3 * (int64_t)a.n) return;
-    if (i >= total) {
+    int64_t total;
+    const bool fit = rows_fit(a, n_split, n_dup, total);
+    if (i == 0) *n_new = fit ? (int32_t)total : 0;  // no rows to compact when they did not fit
+    if (i >= 4 * (int64_t)a.n) return;
+    if (!fit || i >= total) {
         keep[i] = 0;
         return;
     }
@@ -148,9 +170,10 @@ __global__ void compact_gather_kernel(const float *src, float *scratch, int stri
     scratch[(int64_t)keep_ord[row] * stride + col] = src[t];
 }
 
-__global__ void compact_copy_back_kernel(float *dst, const float *scratch, int stride, const int32_t *new_count) {
+__global__ void compact_copy_back_kernel(float *dst, const float *scratch, int stride, const int32_t *new_count,
+                                         const int32_t *overflow) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)(*new_count) * stride) return;
+    if (*overflow || t >= (int64_t)(*new_count) * stride) return;
     dst[t] = scratch[t];
 }
 
@@ -173,9 +196,10 @@ void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st) {
     densify_classify_kernel<<<gb, bs, 0, st>>>(a, s.split, s.dup);
     scan_exclusive<int32_t>(s.split, s.split_ord, n, s.n_split, s.scan_part, st);
     scan_exclusive<int32_t>(s.dup, s.dup_ord, n, s.n_dup, s.scan_part, st);
-    densify_split_kernel<<<gb, bs, 0, st>>>(a, s.split, s.split_ord);
-    densify_dup_kernel<<<gb, bs, 0, st>>>(a, s.dup, s.dup_ord, s.n_split);
-    const int64_t rows = 3 * (int64_t)n;
+    cudaMemsetAsync(s.overflow, 0, sizeof(int32_t), st);
+    densify_split_kernel<<<gb, bs, 0, st>>>(a, s.split, s.split_ord, s.n_split, s.n_dup, s.overflow);
+    densify_dup_kernel<<<gb, bs, 0, st>>>(a, s.dup, s.dup_ord, s.n_split, s.n_dup);
+    const int64_t rows = 4 * (int64_t)n;  // at most N + 2 N splits + N clones
     densify_cull_kernel<<<(unsigned)((rows + bs - 1) / bs), bs, 0, st>>>(a, s.split, s.n_split, s.n_dup, s.keep,
                                                                        s.n_new);
     scan_exclusive<int32_t>(s.keep, s.keep_ord, (int)rows, s.new_count, s.scan_part, st);
@@ -187,7 +211,7 @@ void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st) {
         const int64_t elems = rows * stride;
         const unsigned grid = (unsigned)((elems + bs - 1) / bs);
         compact_gather_kernel<<<grid, bs, 0, st>>>(buf, s.scratch, stride, s.keep, s.keep_ord, s.n_new);
-        compact_copy_back_kernel<<<grid, bs, 0, st>>>(buf, s.scratch, stride, s.new_count);
+        compact_copy_back_kernel<<<grid, bs, 0, st>>>(buf, s.scratch, stride, s.new_count, s.overflow);
     }
 }
 

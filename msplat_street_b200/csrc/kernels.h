@@ -221,11 +221,13 @@ struct DensifyArgs {
     uint32_t seed;
     float *buf[6], *m1[6], *m2[6];  // capacity-sized: means scales quats dc rest opacity
     int stride[6];
+    int64_t cap;  // rows of every buffer: the rows after splits and clones must fit
 };
 struct DensifyScratch {
-    int32_t *split, *dup, *split_ord, *dup_ord, *keep, *keep_ord;
+    int32_t *split, *dup, *split_ord, *dup_ord, *keep, *keep_ord;  // 4N rows each
     int32_t *n_split, *n_dup, *n_new, *new_count, *scan_part;
-    float *scratch;  // 3N x max(stride) floats
+    int32_t *overflow;  // set when N + 2 splits + clones exceeds cap (nothing is written)
+    float *scratch;     // 4N x max(stride) floats
 };
 void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st);
 void launch_opacity_reset(float *o, float *m1, float *m2, int n, float reset_logit, cudaStream_t st);

@@ -209,7 +209,9 @@ class GaussianTrainer:
         stop_split_at = c.iterations // 2
         do_dens = step < stop_split_at and step % reset_interval > len(self.ds.views) + c.refine_every
         if do_dens and self.stats is not None:
-            self.ensure_capacity(3 * self.num_active)
+            # a Gaussian may be both split and cloned: up to 4 N rows (the reference
+            # reserves 3 N, model.cpp:158-193)
+            self.ensure_capacity(4 * self.num_active)
             gn, vc, ms = self.stats[1], self.stats[0], self.stats[2]
             self.num_active = self.ctx.densify(
                 self.num_active, self.buf, self.m1, self.m2, gn, vc, ms, 0.5 * self.max_dim,

@@ -128,6 +128,43 @@ def test_gpu_densify_matches_oracle(n, check_screen, check_huge):
         assert np.array_equal(t2[g].cpu().numpy()[:new_n], o2[g][:new_n]), g
 
 
+def _split_and_clone_inputs(n, cap, seed):
+    """Small Gaussians (world scale below size_thresh) that are large on screen and
+    have high gradients: each one is both split and cloned, 4 n rows in all."""
+    bufs, m1, m2, stats = _densify_inputs(n, cap, seed)
+    bufs[1][:n] = np.log(0.004)  # every scale small: cloned
+    stats["vis"][:] = 2.0
+    stats["gn"][:] = 1e-3      # (gn / vis) * half_max_dim > 2e-4: high gradient
+    stats["ms"][:] = 0.1       # > screen_thresh 0.05: split on screen size
+    return bufs, m1, m2, stats
+
+
+def test_gpu_densify_split_and_clone_needs_4n_rows():
+    n = 3000
+    cap = 4 * n
+    bufs, m1, m2, stats = _split_and_clone_inputs(n, cap, 9)
+    ob, o1, o2 = [b.copy() for b in bufs], [b.copy() for b in m1], [b.copy() for b in m2]
+    new_o = Oracle("restatement").densify(n, cap, ob, o1, o2, stats, 60.0, 5, check_huge=0)
+    tb = [torch.from_numpy(b).cuda() for b in bufs]
+    t1 = [torch.from_numpy(b).cuda() for b in m1]
+    t2 = [torch.from_numpy(b).cuda() for b in m2]
+    st = [torch.from_numpy(stats[k]).cuda() for k in ("gn", "vis", "ms")]
+    new_n = Context().densify(n, tb, t1, t2, st[0], st[1], st[2], 60.0, 5, check_huge=False)
+    assert new_n == new_o and new_n > 3 * n - n // 2  # the parents are culled, children and clones kept
+    for g in range(6):
+        np.testing.assert_allclose(tb[g].cpu().numpy()[:new_n], ob[g][:new_n], rtol=1e-6, atol=1e-7)
+    # the same Gaussians against 3 n rows: refused, nothing written
+    bufs, m1, m2, stats = _split_and_clone_inputs(n, 3 * n, 9)
+    tb = [torch.from_numpy(b).cuda() for b in bufs]
+    t1 = [torch.from_numpy(b).cuda() for b in m1]
+    t2 = [torch.from_numpy(b).cuda() for b in m2]
+    st = [torch.from_numpy(stats[k]).cuda() for k in ("gn", "vis", "ms")]
+    with pytest.raises(RuntimeError, match="4 N rows"):
+        Context().densify(n, tb, t1, t2, st[0], st[1], st[2], 60.0, 5, check_huge=False)
+    for t, b in zip(tb + t1 + t2, bufs + m1 + m2):
+        assert np.array_equal(t.cpu().numpy(), b)
+
+
 def test_gpu_densify_capacity_error():
     n = 10
     bufs = [torch.zeros((25, s), device="cuda") for s in (3, 3, 4, 3, 45, 1)]
