@@ -126,11 +126,17 @@ __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64
 #pragma unroll
     for (int c = 0; c < 9; c++) s9[c] = 0.f;
     if (sd) *sd = 0.f;
+    long long my_e0 = 0;
+    int my_cnt = 0;
+    if (vis) {  // each lane loads its own Gaussian's range once; the loop shuffles it
+        my_e0 = offsets[g0 + lane];
+        my_cnt = n_tiles[g0 + lane];
+    }
     const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
     for (int gl = 0; gl < 32; gl++) {
         if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
-        const int64_t e0 = offsets[g0 + gl];
-        const int cnt = n_tiles[g0 + gl];
+        const long long e0 = __shfl_sync(0xffffffffu, my_e0, gl);
+        const int cnt = __shfl_sync(0xffffffffu, my_cnt, gl);
         float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, pd = 0.f;
         for (int j = lane; j < cnt; j += 32) {
             const int32_t k = inv[e0 + j];
