@@ -964,7 +964,7 @@ int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float gra
     a.cap = buf_capacity;
     const int64_t rows = 4 * (int64_t)std::max(N, 1);  // a Gaussian may be split and cloned
     if (rows > (int64_t)INT32_MAX) return fail(MSPLAT_CUDA_EINVAL, "msplat_densify: N (%d) too large", N);
-    ENSURE(ctx->d_flags, 6 * rows, int32_t, flags);
+    ENSURE(ctx->d_flags, 7 * rows, int32_t, flags);
     ENSURE(ctx->d_counts, 8 + scan_blocks((int)rows) + 1, int32_t, counts);
     ENSURE(ctx->d_scratch, rows * max_stride, float, scratch);
     if (!ctx->h_count) CUDA_TRY(cudaMallocHost(&ctx->h_count, sizeof(int32_t)));
@@ -975,6 +975,7 @@ int msplat_cuda_densify(msplat_cuda_ctx *ctx, int N, int buf_capacity, float gra
     s.dup_ord = flags + 3 * rows;
     s.keep = flags + 4 * rows;
     s.keep_ord = flags + 5 * rows;
+    s.row_parent = flags + 6 * rows;
     s.n_split = counts;
     s.n_dup = counts + 1;
     s.n_new = counts + 2;

@@ -227,6 +227,7 @@ struct DensifyScratch {
     int32_t *split, *dup, *split_ord, *dup_ord, *keep, *keep_ord;  // 4N rows each
     int32_t *n_split, *n_dup, *n_new, *new_count, *scan_part;
     int32_t *overflow;  // set when N + 2 splits + clones exceeds cap (nothing is written)
+    int32_t *row_parent;  // 3N: the parent of each new row (split children, then clones)
     float *scratch;     // 4N x max(stride) floats
 };
 void launch_densify(const DensifyArgs &a, DensifyScratch &s, cudaStream_t st);
