@@ -176,6 +176,7 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     uint32_t *vv[2] = {v0, v1};
     const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);
     ctx->sorted = cur;
+    ctx->gid_in_vals = false;
     launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
     launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, inv, st);
 
@@ -341,18 +342,19 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     ENSURE(ctx->keys[1], n_isect, uint32_t, k1);
     ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
     ENSURE(ctx->vals[1], n_isect, uint32_t, v1);
-    ENSURE(ctx->emit_gid, n_isect, int32_t, emit_gid);
-    ENSURE(ctx->isect_gid, n_isect, int32_t, isect_gid);
     ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
 
     ctx->timer.mark(1, st);
-    launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, d, k0, v0, emit_gid, st);
+    // render only: the sort carries Gaussian ids, so its sorted values are the
+    // per-intersection ids (no emission-index map, no inverse map)
+    launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, d, k0, v0, nullptr, st);
     uint32_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
     const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);
     ctx->sorted = cur;
+    ctx->gid_in_vals = true;
+    const int32_t *isect_gid = reinterpret_cast<const int32_t *>(vv[cur]);
     launch_tile_ranges(kk[cur], (int)n_isect, T, tile_start, tile_end, st);
-    launch_isect_map(vv[cur], (int)n_isect, emit_gid, isect_gid, nullptr, st);  // render only: no inverse map
 
     for (int v = 0; v < nv; v++) {
         const msplat_cuda_view &w = views[v];
@@ -1228,6 +1230,12 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         {"out_adj", &ctx->pri[PB_ADJ], npix * 3},
         {"v_adj", &ctx->pri[PB_VADJ], npix * 3},
     };
+    if (ctx->gid_in_vals && !std::strcmp(name, "isect_gid")) {  // a batched render's ids: the sorted values
+        if (!ctx->vals[ctx->sorted].ptr) return fail(MSPLAT_CUDA_EINVAL, "frame buffer 'isect_gid' has not been produced");
+        *dev_ptr = ctx->vals[ctx->sorted].ptr;
+        *count = ctx->n_isect;
+        return MSPLAT_CUDA_OK;
+    }
     for (const Entry &e : table)
         if (!std::strcmp(e.name, name)) {
             if (!e.buf->ptr) return fail(MSPLAT_CUDA_EINVAL, "frame buffer '%s' has not been produced", name);

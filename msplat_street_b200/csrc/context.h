@@ -178,6 +178,7 @@ struct msplat_cuda_ctx {
     int n = 0, W = 0, H = 0, tiles_x = 0, tiles_y = 0;
     int64_t n_isect = 0;
     int sorted = 0;  // which key/value buffer pair holds the sorted result
+    bool gid_in_vals = false;  // the sorted values are Gaussian ids (batched render) rather than emission indices
     // per Gaussian
     Buf splats, radii, aabb, n_tiles, offsets, scan_part, total;
     Buf v_xy, v_conic, v_rgb, v_opacity, v_mean3d, v_scale, v_quat;

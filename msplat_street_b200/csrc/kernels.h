@@ -50,7 +50,8 @@ struct DepthScratch {
 };
 void launch_depth_offsets(int n, const Splat *splats, const int32_t *n_tiles, DepthScratch &s, int64_t *offsets,
                           int64_t *d_total, int64_t *scan_part, cudaStream_t st);
-// Emission: key = tile id (global tile id in a batch), value = emission index.
+// Emission: key = tile id (global tile id in a batch), value = emission index, or
+// the Gaussian id when emit_gid is null (render only: no backward needs the map).
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
                       int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
 size_t radix_scratch_bytes(int n);

@@ -207,7 +207,9 @@ __device__ __forceinline__ void rect_of(const Splat &s, float ax, float ay, int 
 
 // Emits the intersections of each thread's Gaussian: the tiles of its rectangle
 // [x0, x1) x [y0, y1) in row-major order at emission indices e0, e0 + 1, ..., key =
-// base + tile id, value = emission index. Rectangles of up to SMALL_RECT tiles are
+// base + tile id, value = emission index (or, with emit_gid null -- render-only
+// frames with no backward -- the Gaussian id itself, so the sorted values are the
+// per-intersection ids with no gather). Rectangles of up to SMALL_RECT tiles are
 // written by their own thread; larger ones by the whole warp, lane l writing entries
 // l, l + 32, ..., so the stores of the big (near-camera) Gaussians coalesce. Every
 // lane of the warp must call it. cap: buffer capacity (entries at or past it dropped).
@@ -222,8 +224,12 @@ __device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y
         for (int y = y0; y < y1; y++)
             for (int x = x0; x < x1 && e < cap; x++, e++) {
                 keys[e] = base + (uint32_t)(y * tiles_x + x);
-                vals[e] = (uint32_t)e;
-                emit_gid[e] = gid;
+                if (emit_gid) {
+                    vals[e] = (uint32_t)e;
+                    emit_gid[e] = gid;
+                } else {
+                    vals[e] = (uint32_t)gid;
+                }
             }
     }
     unsigned big = __ballot_sync(0xffffffffu, cnt > SMALL_RECT);
@@ -241,8 +247,12 @@ __device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y
             if (e >= cap) break;
             const int yy = sy0 + j / sw, xx = sx0 + j % sw;
             keys[e] = sb + (uint32_t)(yy * stx + xx);
-            vals[e] = (uint32_t)e;
-            emit_gid[e] = sg;
+            if (emit_gid) {
+                vals[e] = (uint32_t)e;
+                emit_gid[e] = sg;
+            } else {
+                vals[e] = (uint32_t)sg;
+            }
         }
     }
 }
