@@ -60,7 +60,17 @@ int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
  * "store_transmittance" (K > 0: the forward stores each pixel's transmittance before
  * its first K contributions and the backward reads them instead of recovering T by
  * division, which the reference does (msplat_cpu.cpp:996-997); pixels with more
- * contributions fall back to division; 0 = off, the default). */
+ * contributions fall back to division; 0 = off, the default);
+ * "chunked_raster" (depth-chunked compositing of single-view render / train_step /
+ * render_backward, the Metal backend's path for small frames,
+ * core/metal/msplat_metal.metal:2641-3030 with its rule at msplat_metal.mm:1101-1117:
+ * each tile's list in "chunk_len"-long pieces composited in parallel from T = 1, each
+ * with its own early stop, merged per pixel front to back until T <= 1e-4. 0 = off,
+ * one pass per tile as core/cpu (the default); 1 = frames of fewer than 400 tiles
+ * without a prior, as the Metal backend; 2 = every frame without a prior. Images
+ * differ from one pass by what the per-piece stops let through, about 1e-4; the
+ * batched entry points always composite in one pass);
+ * "chunk_len" (the piece length, 512 by default as in the Metal backend). */
 int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
 /* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
  * backward round, and the backward reduction's sub-batch. Returns the variant count. */

@@ -32,6 +32,7 @@ from .camera import CameraSetup
 _POOL: List[Context] = []
 _POOL_LOCK = threading.Lock()
 _STORE_T = 0
+_CHUNKED = ("off", 512)
 
 
 def set_transmittance_mode(mode: str = "recompute", capacity: int = 256) -> None:
@@ -46,6 +47,16 @@ def set_transmittance_mode(mode: str = "recompute", capacity: int = 256) -> None
     _STORE_T = int(capacity) if mode == "store" else 0
 
 
+def set_chunked_mode(mode: str = "off", chunk_len: int = 512) -> None:
+    """Depth-chunked compositing of the renders and their backward (the Metal backend's
+    path for small frames): "off" (default, one pass per tile as core/cpu), "auto"
+    (frames of fewer than 400 tiles) or "on"; see Context.set_chunked."""
+    global _CHUNKED
+    if mode not in Context._CHUNK_MODES:
+        raise ValueError(f"mode must be one of {sorted(Context._CHUNK_MODES)}")
+    _CHUNKED = (mode, int(chunk_len))
+
+
 def _acquire() -> Context:
     with _POOL_LOCK:
         c = _POOL.pop() if _POOL else None
@@ -53,6 +64,8 @@ def _acquire() -> Context:
         c = Context()
     if c.store_transmittance != _STORE_T:
         c.set_store_transmittance(_STORE_T)
+    if (c.chunked, c.chunk_len) != _CHUNKED:
+        c.set_chunked(*_CHUNKED)
     return c
 
 

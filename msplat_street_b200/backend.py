@@ -18,7 +18,7 @@ from .camera import CameraSetup
 from ._lib import check, lib
 
 PARAM_NAMES = ("means", "scales", "quats", "features_dc", "features_rest", "opacities")
-_FRAME_INT = {"radii", "tile_start", "tile_end", "isect_gid", "final_idx"}
+_FRAME_INT = {"radii", "tile_start", "tile_end", "isect_gid", "final_idx", "chunk_first"}
 
 
 def ptr(t: Optional[torch.Tensor]):
@@ -196,7 +196,8 @@ class PriorStep:
 class Context:
     """One msplat_cuda context: a frame cache plus the stream it works on."""
 
-    def __init__(self, keep_grads: bool = False, store_transmittance: int = 0):
+    def __init__(self, keep_grads: bool = False, store_transmittance: int = 0, chunked: str = "off",
+                 chunk_len: int = 512):
         if not torch.cuda.is_available():
             raise _lib.MsplatCudaError("msplat_street_b200 needs a CUDA device (no CPU fallback)")
         self._lib = lib()
@@ -207,6 +208,21 @@ class Context:
         if keep_grads:
             check(self._lib.msplat_cuda_ctx_set_option(h, b"keep_grads", 1))
         self.set_store_transmittance(store_transmittance)
+        self.set_chunked(chunked, chunk_len)
+
+    _CHUNK_MODES = {"off": 0, "auto": 1, "on": 2}
+
+    def set_chunked(self, mode: str = "auto", chunk_len: int = 512) -> None:
+        """Depth-chunked compositing of single-view frames (the Metal backend's path for
+        small frames, core/metal/msplat_metal.metal:2641-3030): "off" composites each
+        tile in one pass (core/cpu, the default); "auto" chunks frames of fewer than 400
+        tiles, as the Metal backend does (msplat_metal.mm:1101-1117); "on" chunks every
+        frame. Frames with a prior always composite in one pass."""
+        if mode not in self._CHUNK_MODES:
+            raise ValueError(f"chunked must be one of {sorted(self._CHUNK_MODES)}, not {mode!r}")
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"chunk_len", int(chunk_len)))
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"chunked_raster", self._CHUNK_MODES[mode]))
+        self.chunked, self.chunk_len = mode, int(chunk_len)
 
     def set_store_transmittance(self, capacity: int) -> None:
         """0: the backward recovers transmittance by division (the reference's way);

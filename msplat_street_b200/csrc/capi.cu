@@ -95,6 +95,36 @@ SkyArgs sky_args(const msplat_cuda_prior &p, const CamParams &cam) {
 // intersection count, which sizes the sort. With a prior whose aux flag is set, the
 // aux rasterizer also writes the expected-depth numerator and the per-pixel
 // background, sampled from the learned sky when one is set.
+// The depth-chunked planes of the current frame (ctx->n_isect intersections over T
+// tiles): at most n_isect / chunk_len + T items (each tile adds at most one partial
+// piece). backward: also the prefix / suffix planes. Fills ck from the buffers.
+int chunk_buffers(msplat_cuda_ctx *ctx, int T, bool backward, ChunkArgs &ck) {
+    if (!backward) ctx->chunk_cap = ctx->n_isect / ctx->chunk_len + T + 1;
+    const size_t cap = (size_t)ctx->chunk_cap;
+    ENSURE(ctx->ch[CH_COUNTS], T, int32_t, counts);
+    ENSURE(ctx->ch[CH_FIRST], (size_t)T + 1, int32_t, first);
+    ENSURE(ctx->ch[CH_PART], scan_blocks(T) + 1, int32_t, part);
+    ENSURE(ctx->ch[CH_T], cap * TILE_PIX, float, cT);
+    ENSURE(ctx->ch[CH_C], cap * 3 * TILE_PIX, float, cC);
+    ENSURE(ctx->ch[CH_LAST], cap * TILE_PIX, int32_t, clast);
+    (void)counts;
+    (void)part;
+    ck.chunk_len = ctx->chunk_len;
+    ck.first = first;
+    ck.cT = cT;
+    ck.cC = cC;
+    ck.clast = clast;
+    ck.pre = nullptr;
+    ck.aft = nullptr;
+    if (backward) {
+        ENSURE(ctx->ch[CH_PRE], cap * TILE_PIX, float, pre);
+        ENSURE(ctx->ch[CH_AFT], cap * 3 * TILE_PIX, float, aft);
+        ck.pre = pre;
+        ck.aft = aft;
+    }
+    return MSPLAT_CUDA_OK;
+}
+
 int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales, float glob_scale,
             const float *quats, const CamParams &cam, const float *dc, const float *rest, const float *opac,
             const float *bg) {
@@ -206,10 +236,26 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ra.out_depth = out_depth;
     ra.bg_img = bg_img;
     ra.sky_bg = sky ? 1 : 0;
+    // depth-chunked compositing for frames of few tiles (never with a prior: the aux
+    // rasterizer is one-pass only, as in core/metal/msplat_metal.mm:1103-1106)
+    const bool chunked =
+        !aux && T > 0 && (ctx->chunk_mode == 2 || (ctx->chunk_mode == 1 && T < CHUNK_AUTO_TILES));
+    ctx->chunk_frame = chunked;
+    ChunkArgs ck{};
+    if (chunked) {
+        if (int r = chunk_buffers(ctx, T, false, ck)) return r;
+        ra.tstore = nullptr;
+        ra.tcount = nullptr;
+        ra.tcap = 0;
+    }
     ctx->timer.mark(2, st);
     if (aux) {
         if (sky) launch_sky_background(sky_args(*pr, cam), (int)cam.width, (int)cam.height, bg_img, st);
         launch_raster_fwd_aux(ra, st);
+    } else if (chunked) {
+        launch_chunk_items(tile_start, tile_end, T, ck.chunk_len, reinterpret_cast<int32_t *>(ctx->ch[CH_COUNTS].ptr),
+                           ck.first, reinterpret_cast<int32_t *>(ctx->ch[CH_PART].ptr), st);
+        launch_raster_fwd_chunked(ra, ck, ctx->chunk_cap, st, ctx->raster_variant);
     } else {
         launch_raster_fwd(ra, st, ctx->raster_variant);
     }
@@ -445,6 +491,16 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
     }
     if (!std::strcmp(name, "graph")) {
         ctx->tb.graph = value != 0;
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "chunked_raster")) {
+        if (value < 0 || value > 2) return fail(MSPLAT_CUDA_EINVAL, "chunked_raster must be 0 (off), 1 (auto) or 2 (on)");
+        ctx->chunk_mode = (int)value;
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "chunk_len")) {
+        if (value < 1 || value > (1 << 20)) return fail(MSPLAT_CUDA_EINVAL, "chunk_len must be 1..2^20");
+        ctx->chunk_len = (int)value;
         return MSPLAT_CUDA_OK;
     }
     return fail(MSPLAT_CUDA_EINVAL, "unknown option '%s'", name);
@@ -742,6 +798,10 @@ int msplat_cuda_train_step(msplat_cuda_ctx *ctx, int num_points, float *means3d,
         rb.v_aux = v_aux;
         rb.slots_depth = slots_depth;
         launch_raster_bwd_aux(rb, st);
+    } else if (ctx->chunk_frame) {
+        ChunkArgs ck{};
+        if (int r = chunk_buffers(ctx, tiles_x * tiles_y, true, ck)) return r;
+        launch_raster_bwd_chunked(rb, ck, ctx->chunk_cap, st, ctx->raster_variant);
     } else {
         launch_raster_bwd(rb, st, ctx->raster_variant);
     }
@@ -864,7 +924,13 @@ int msplat_cuda_render_backward(msplat_cuda_ctx *ctx, int num_points, const floa
     rb.slots = slots;
     rb.tstore = ctx->tstore_cap > 0 ? reinterpret_cast<const float *>(ctx->tstore.ptr) : nullptr;
     rb.tcount = ctx->tstore_cap > 0 ? reinterpret_cast<const int32_t *>(ctx->tcount.ptr) : nullptr;
-    launch_raster_bwd(rb, st, ctx->raster_variant);
+    if (ctx->chunk_frame) {
+        ChunkArgs ck{};
+        if (int r = chunk_buffers(ctx, tiles_x * tiles_y, true, ck)) return r;
+        launch_raster_bwd_chunked(rb, ck, ctx->chunk_cap, st, ctx->raster_variant);
+    } else {
+        launch_raster_bwd(rb, st, ctx->raster_variant);
+    }
     BackwardArgs ba;
     std::memset(&ba, 0, sizeof ba);
     ba.n = n;
@@ -1177,6 +1243,7 @@ int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {
     int64_t total = 0;
     for (const Buf *b : all) total += (int64_t)b->bytes;
     for (const Buf &b : ctx->pri) total += (int64_t)b.bytes;
+    for (const Buf &b : ctx->ch) total += (int64_t)b.bytes;
     return total;
 }
 
@@ -1229,6 +1296,7 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         {"v_depth", &ctx->pri[PB_VDEPTH], n},
         {"out_adj", &ctx->pri[PB_ADJ], npix * 3},
         {"v_adj", &ctx->pri[PB_VADJ], npix * 3},
+        {"chunk_first", &ctx->ch[CH_FIRST], ctx->chunk_frame ? T + 1 : 0},
     };
     if (ctx->gid_in_vals && !std::strcmp(name, "isect_gid")) {  // a batched render's ids: the sorted values
         if (!ctx->vals[ctx->sorted].ptr) return fail(MSPLAT_CUDA_EINVAL, "frame buffer 'isect_gid' has not been produced");

@@ -168,6 +168,11 @@ enum PriBuf {
     PB_COUNT
 };
 
+// ChunkArgs buffers: per-tile item counts, first items, scan partials, then the
+// per-(item, pixel) planes
+enum ChunkBuf { CH_COUNTS, CH_FIRST, CH_PART, CH_T, CH_C, CH_LAST, CH_PRE, CH_AFT, CH_COUNT };
+constexpr int CHUNK_AUTO_TILES = 400;  // core/metal/msplat_metal.mm:1103
+
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
     int raster_variant = 0;  // option "raster_variant": index into RASTER_VARIANTS
@@ -191,6 +196,13 @@ struct msplat_cuda_ctx {
     // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
     int tstore_cap = 0;
     Buf tstore, tcount;
+    // depth-chunked compositing: option "chunked_raster" (0 off, 1 frames of fewer
+    // than CHUNK_AUTO_TILES tiles, 2 every frame) and "chunk_len"; whether the last
+    // single-view frame ran chunked, its item bound, and the ChunkArgs planes
+    int chunk_mode = 0, chunk_len = 512;
+    bool chunk_frame = false;
+    int64_t chunk_cap = 0;
+    Buf ch[CH_COUNT];
     // depth order of the Gaussians (or batch instances) before key emission
     Buf dkeys[2], dvals[2], dcounts, doff;
     // image pipeline scratch: metrics (moments, terms, row sums) and RGBA8 packing
@@ -231,7 +243,13 @@ struct msplat_cuda_ctx {
             b.ptr = nullptr;
             b.bytes = 0;
         }
+        for (Buf &b : ch) {
+            if (b.ptr) cudaFree(b.ptr);
+            b.ptr = nullptr;
+            b.bytes = 0;
+        }
         aux_frame = false;
+        chunk_frame = false;
         tb.release();  // its graph refers to the buffers just freed
         if (h_total) cudaFreeHost(h_total);
         h_total = nullptr;

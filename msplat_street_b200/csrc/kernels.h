@@ -99,6 +99,33 @@ inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v :
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st);
 
+struct RasterBwdArgs;
+// Depth-chunked compositing (core/metal/msplat_metal.metal:2641-3030): every tile's
+// list split into chunk_len-long pieces, tile t's pieces being work items first[t] ..
+// first[t + 1] - 1 (first[T] = all items). Per (item, thread of the tile block): the
+// piece's own transmittance and colour composited from T = 1, its last contributor
+// (-1 once the pixel's merged transmittance is spent), and for the backward the
+// transmittance in front of the piece and the colour behind it. Planes are [item][256]
+// (cT, clast, pre) and [item][3][256] (cC, aft).
+struct ChunkArgs {
+    int chunk_len;
+    int32_t *first;  // [tiles + 1]
+    float *cT, *cC, *pre, *aft;
+    int32_t *clast;
+};
+// Items of each tile, their exclusive scan into first (first[T] = all); counts and
+// partials are scratch of T and scan_blocks(T) + 1 entries.
+void launch_chunk_items(const int32_t *tile_start, const int32_t *tile_end, int T, int chunk_len, int32_t *counts,
+                        int32_t *first, int32_t *partials, cudaStream_t st);
+// Pieces of at most item_cap items (a host bound on first[T]), then the per-pixel
+// merge into a.out_img / final_T / final_idx.
+void launch_raster_fwd_chunked(const RasterArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,
+                               int variant = 0);
+// Backward: prefix transmittance and suffix colour per (item, pixel), then the pieces
+// back to front into a.slots.
+void launch_raster_bwd_chunked(const RasterBwdArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,
+                               int variant = 0);
+
 // A batch of views rendered by one projection, one sort and one persistent raster
 // launch. Instances (view, Gaussian) and tiles (view, tile) are numbered globally,
 // view after view; every array lives in device memory.

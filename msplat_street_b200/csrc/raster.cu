@@ -93,14 +93,21 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4
 // FB: Gaussians staged in shared memory per round (at most one per thread).
 // AUX: also the expected-depth numerator and a per-pixel background
 // (rasterize_forward_aux, core/cpu/msplat_cpu.cpp:574-626 with f.aux).
-template <int FB, bool AUX = false>
+// CHUNK: composite only piece `chunk` of the list (ck->chunk_len long) from T = 1 and
+// write the piece's transmittance, colour and last contributor to item `item`.
+template <int FB, bool AUX = false, bool CHUNK = false>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
-                                                float4 *s1, float4 *s2, uint8_t *sm) {
+                                                float4 *s1, float4 *s2, uint8_t *sm, const ChunkArgs *ck = nullptr,
+                                                int item = 0, int chunk = 0) {
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
-    const int start = a.tile_start[tile], end = a.tile_end[tile];
+    int start = a.tile_start[tile], end = a.tile_end[tile];
+    if (CHUNK) {
+        start += chunk * ck->chunk_len;
+        end = min(end, start + ck->chunk_len);
+    }
     const float fpx = (float)px, fpy = (float)py;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f, depth = 0.f;
@@ -156,6 +163,15 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
         }
     }
     if (!inside) return;
+    if (CHUNK) {
+        const size_t o = (size_t)item * TILE_PIX + threadIdx.x, o3 = (size_t)item * 3 * TILE_PIX + threadIdx.x;
+        ck->cT[o] = T;
+        ck->cC[o3] = cr;
+        ck->cC[o3 + TILE_PIX] = cg;
+        ck->cC[o3 + 2 * TILE_PIX] = cb;
+        ck->clast[o] = last;
+        return;
+    }
     if (a.final_T) a.final_T[pid] = T;
     if (a.final_idx) a.final_idx[pid] = last;
     if (a.tcount) a.tcount[pid] = stored <= a.tcap ? stored : -1;
@@ -267,9 +283,13 @@ constexpr size_t raster_bwd_smem() {
 // the block calls it; it ends with the block's shared memory free for reuse. AUX: the
 // per-pixel background is the pixel's own, and the expected-depth / alpha cotangents
 // enter v_alpha and a tenth value per intersection (the aux branch of :959-1031).
-template <int BB, int SB, bool AUX = false>
+// CHUNK: piece `chunk` of the list only (item `item`), each pixel starting from the
+// transmittance behind the piece (prefix * piece T), the colour behind it and the
+// piece's last contributor; the background term still uses the merged final T.
+template <int BB, int SB, bool AUX = false, bool CHUNK = false>
 __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
-                                                int &kmax) {
+                                                int &kmax, const ChunkArgs *ck = nullptr, int item = 0,
+                                                int chunk = 0) {
     constexpr int NG = AUX ? 10 : 9;
     constexpr int BWD_BATCH = BB, SUB = SB, SUB_OUT = SB * NG;
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
@@ -280,17 +300,30 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
-    const int start = a.tile_start[tile], end = a.tile_end[tile];
+    int start = a.tile_start[tile], end = a.tile_end[tile];
+    if (CHUNK) {
+        start += chunk * ck->chunk_len;
+        end = min(end, start + ck->chunk_len);
+    }
     if (end <= start) return;  // block-uniform
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pid = py * a.W + px;
     float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f, vd = 0.f, vaa = 0.f;
     float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
+    float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
     int kf = start - 1;
     if (inside) {
         Tf = a.final_T[pid];
         T = Tf;
         kf = a.final_idx[pid];
+        if (CHUNK) {
+            const size_t o = (size_t)item * TILE_PIX + threadIdx.x, o3 = (size_t)item * 3 * TILE_PIX + threadIdx.x;
+            T = ck->pre[o] * ck->cT[o];
+            kf = ck->clast[o];
+            br = ck->aft[o3];
+            bgc = ck->aft[o3 + TILE_PIX];
+            bb = ck->aft[o3 + 2 * TILE_PIX];
+        }
         const float *v = a.v_out + 3 * (size_t)pid;
         vr = v[0];
         vg = v[1];
@@ -312,12 +345,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
     // T_final * bg, then the -ra * (T_final * bg) term of the reference's v_alpha
     const float tbr = Tf * bgr, tbg = Tf * bgg, tbb = Tf * bgb;
-    float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
     float bd = 0.f, ba = 0.f;             // aux: accumulated depth and alpha behind
     const float fpx = (float)px, fpy = (float)py;
     float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
     // stored-transmittance mode: contributions left to pop, -1 = recover T by division
-    int tj = (a.tstore && inside) ? a.tcount[pid] : -1;
+    int tj = (!CHUNK && a.tstore && inside) ? a.tcount[pid] : -1;
     const size_t npix = (size_t)a.W * a.H;
     for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
         const int b_start = max(start, b_end - BWD_BATCH);
@@ -576,6 +608,171 @@ void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off
     MSPLAT_BWD_VARIANTS(X)
 #undef X
     bwd_batch_launch<64, 4>(d_views, d_tile_off, n_views, d_counter, st);
+}
+
+// ---------------------------------------------------------------------------------
+// Depth-chunked compositing (core/metal/msplat_metal.metal:2641-3030): for frames of
+// few tiles, whose lists are long, one block per (tile, piece) instead of one per
+// tile puts the whole GPU on the frame. A block finds its tile by binary search over
+// the tiles' first items; blocks past the item count (the grid is a host bound)
+// return at once.
+
+__global__ void chunk_count_kernel(const int32_t *tile_start, const int32_t *tile_end, int T, int len,
+                                   int32_t *counts) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < T) counts[t] = (tile_end[t] - tile_start[t] + len - 1) / len;
+}
+
+void launch_chunk_items(const int32_t *tile_start, const int32_t *tile_end, int T, int chunk_len, int32_t *counts,
+                        int32_t *first, int32_t *partials, cudaStream_t st) {
+    if (T <= 0) return;
+    chunk_count_kernel<<<(T + 255) / 256, 256, 0, st>>>(tile_start, tile_end, T, chunk_len, counts);
+    scan_exclusive<int32_t>(counts, first, T, first + T, partials, st);
+}
+
+// The tile of item i: the last t with first[t] <= i (tiles without items share their
+// first with the next tile, so the search lands on one that has items).
+__device__ __forceinline__ int chunk_tile(const int32_t *first, int T, int i) {
+    int lo = 0, hi = T;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= i) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - 1;
+}
+
+template <int FB>
+__global__ void __launch_bounds__(TILE_PIX) raster_fwd_chunk_kernel(RasterArgs a, ChunkArgs c) {
+    __shared__ float4 s0[FB], s1[FB], s2[FB];
+    __shared__ uint8_t sm[FB];
+    const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
+    if (item >= c.first[T]) return;  // block-uniform
+    const int tile = chunk_tile(c.first, T, item);
+    raster_fwd_tile<FB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, &c, item,
+                                     item - c.first[tile]);
+}
+
+// rasterize_forward_merge_kernel (.metal:2741-2808): per pixel, the tile's pieces front
+// to back, C += piece C * T (fused), T *= piece T, the last contributor taken from every
+// piece that has one (a piece without contributors reports its start - 1), stopping
+// once T <= 1e-4; the pieces past the stop lose their contributors for the backward.
+__global__ void __launch_bounds__(TILE_PIX) chunk_merge_kernel(RasterArgs a, ChunkArgs c) {
+    const int tile = blockIdx.x, tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    int lx, ly;
+    tile_pixel(threadIdx.x, lx, ly);
+    const int px = tx * TILE + lx, py = ty * TILE + ly;
+    if (px >= a.W || py >= a.H) return;
+    const int i0 = c.first[tile], n = c.first[tile + 1] - i0;
+    float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f;
+    int last = -1, cut = n;
+    for (int k = 0; k < n; k++) {
+        const size_t o = (size_t)(i0 + k) * TILE_PIX + threadIdx.x, o3 = (size_t)(i0 + k) * 3 * TILE_PIX + threadIdx.x;
+        cr = __fmaf_rn(c.cC[o3], T, cr);
+        cg = __fmaf_rn(c.cC[o3 + TILE_PIX], T, cg);
+        cb = __fmaf_rn(c.cC[o3 + 2 * TILE_PIX], T, cb);
+        T *= c.cT[o];
+        const int cl = c.clast[o];
+        if (cl >= 0) last = cl;
+        if (T <= 1e-4f) {
+            cut = k + 1;
+            break;
+        }
+    }
+    for (int k = cut; k < n; k++) c.clast[(size_t)(i0 + k) * TILE_PIX + threadIdx.x] = -1;
+    const size_t pid = (size_t)py * a.W + px;
+    a.final_T[pid] = T;
+    a.final_idx[pid] = last;
+    float *o = a.out_img + 3 * pid;
+    o[0] = clamp01(__fmaf_rn(a.bg[0], T, cr));
+    o[1] = clamp01(__fmaf_rn(a.bg[1], T, cg));
+    o[2] = clamp01(__fmaf_rn(a.bg[2], T, cb));
+}
+
+template <int FB>
+void fwd_chunk_launch(const RasterArgs &a, const ChunkArgs &c, int64_t items, cudaStream_t st) {
+    raster_fwd_chunk_kernel<FB><<<(unsigned)items, TILE_PIX, 0, st>>>(a, c);
+}
+
+void launch_raster_fwd_chunked(const RasterArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,
+                               int variant) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    if (item_cap > 0) {
+        switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
+            case 64: fwd_chunk_launch<64>(a, c, item_cap, st); break;
+            case 256: fwd_chunk_launch<256>(a, c, item_cap, st); break;
+            default: fwd_chunk_launch<128>(a, c, item_cap, st); break;
+        }
+    }
+    chunk_merge_kernel<<<T, TILE_PIX, 0, st>>>(a, c);
+}
+
+// compute_chunk_prefix_suffix_kernel (.metal:2812-2848): per pixel, the product of the
+// transmittances of the pieces in front of each piece and the sum over the pieces
+// behind it of prefix * colour (every piece of the tile, those past the stop included).
+__global__ void __launch_bounds__(TILE_PIX) chunk_prefix_kernel(int W, int H, int tiles_x, ChunkArgs c) {
+    const int tile = blockIdx.x, tx = tile % tiles_x, ty = tile / tiles_x;
+    int lx, ly;
+    tile_pixel(threadIdx.x, lx, ly);
+    if (tx * TILE + lx >= W || ty * TILE + ly >= H) return;
+    const int i0 = c.first[tile], n = c.first[tile + 1] - i0;
+    float p = 1.f;
+    for (int k = 0; k < n; k++) {
+        const size_t o = (size_t)(i0 + k) * TILE_PIX + threadIdx.x;
+        c.pre[o] = p;
+        p *= c.cT[o];
+    }
+    float ar = 0.f, ag = 0.f, ab = 0.f;
+    for (int k = n - 1; k >= 0; k--) {
+        const size_t o = (size_t)(i0 + k) * TILE_PIX + threadIdx.x, o3 = (size_t)(i0 + k) * 3 * TILE_PIX + threadIdx.x;
+        c.aft[o3] = ar;
+        c.aft[o3 + TILE_PIX] = ag;
+        c.aft[o3 + 2 * TILE_PIX] = ab;
+        const float pk = c.pre[o];
+        ar += pk * c.cC[o3];
+        ag += pk * c.cC[o3 + TILE_PIX];
+        ab += pk * c.cC[o3 + 2 * TILE_PIX];
+    }
+}
+
+template <int BB, int SB>
+__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_chunk_kernel(RasterBwdArgs a, ChunkArgs c) {
+    extern __shared__ __align__(16) float4 smem4[];
+    __shared__ int kmax;
+    const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
+    if (item >= c.first[T]) return;  // block-uniform
+    const int tile = chunk_tile(c.first, T, item);
+    raster_bwd_tile<BB, SB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax, &c, item,
+                                         item - c.first[tile]);
+}
+
+template <int BB, int SB>
+void bwd_chunk_launch(const RasterBwdArgs &a, const ChunkArgs &c, int64_t items, cudaStream_t st) {
+    constexpr size_t smem = raster_bwd_smem<BB, SB>();
+    static const bool attr = [] {
+        cudaFuncSetAttribute(raster_bwd_chunk_kernel<BB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return true;
+    }();
+    (void)attr;
+    raster_bwd_chunk_kernel<BB, SB><<<(unsigned)items, TILE_PIX, smem, st>>>(a, c);
+}
+
+void launch_raster_bwd_chunked(const RasterBwdArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,
+                               int variant) {
+    const int T = a.tiles_x * a.tiles_y;
+    if (T <= 0) return;
+    chunk_prefix_kernel<<<T, TILE_PIX, 0, st>>>(a.W, a.H, a.tiles_x, c);
+    if (item_cap <= 0) return;
+    const RasterVariant &v = RASTER_VARIANTS[variant_index(variant)];
+#define X(bb, sb)                                   \
+    if (v.bwd_batch == bb && v.bwd_sub == sb) {     \
+        bwd_chunk_launch<bb, sb>(a, c, item_cap, st); \
+        return;                                     \
+    }
+    MSPLAT_BWD_VARIANTS(X)
+#undef X
+    bwd_chunk_launch<64, 4>(a, c, item_cap, st);
 }
 
 }  // namespace msplat

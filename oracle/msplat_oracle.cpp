@@ -330,6 +330,12 @@ struct State {
     // gradient
     bool aux = false;
     std::vector<float> out_depth, bg_img, v_aux, v_depth, out_adj, v_adj;
+    // depth-chunked frames: tile t's chunks are items ch_first[t] .. ch_first[t + 1] - 1;
+    // per (item, tile pixel q = row * 16 + column): the chunk's own transmittance,
+    // colour and last contributor (-1 past the pixel's cut-off)
+    bool chunked = false;
+    std::vector<int32_t> ch_first, ch_last;
+    std::vector<float> ch_T, ch_C;
 };
 State g;
 bool g_has_prior = false;
@@ -571,6 +577,99 @@ void raster_fwd(State &f, const float *bg, const float *sky_tex = nullptr, const
     }
 }
 
+// ---- depth-chunked compositing (core/metal/msplat_metal.metal:2641-3030) -------------
+//
+// Test-visible switch (orc_set_option "chunk_size"): 0 composites each tile's list in
+// one pass (the CPU backend); C > 0 splits every tile's list into C-long depth chunks
+// (the Metal backend's path for frames of fewer than 400 tiles, chunk length 512,
+// core/metal/msplat_metal.mm:1101-1117), each composited from T = 1 with its own
+// early stop, then merged per pixel front to back. Within a chunk the arithmetic is
+// the one-pass loop's; the merge, prefix and suffix use the Metal kernels' formulas
+// (fma where they write fma). Every chunk of a tile is kept: the Metal path sizes its
+// chunk count from six times the mean list length and drops entries past it; here a
+// tile has ceil(len / C) chunks.
+int g_chunk = 0;
+
+// Chunk k of a tile whose list is [s, e): [s + k C, min(s + (k + 1) C, e)).
+void raster_fwd_chunked(State &f, const float *bg) {
+    const int W = (int)f.W, H = (int)f.H, T = f.tx * f.ty, C = g_chunk;
+    f.out_img.assign((size_t)W * H * 3, 0.f);
+    f.final_Ts.assign((size_t)W * H, 0.f);
+    f.final_idx.assign((size_t)W * H, 0);
+    f.ch_first.assign((size_t)T + 1, 0);
+    for (int t = 0; t < T; t++) f.ch_first[t + 1] = f.ch_first[t] + (f.tile_end[t] - f.tile_start[t] + C - 1) / C;
+    const size_t items = (size_t)f.ch_first[T];
+    f.ch_T.assign(items * 256, 1.f);
+    f.ch_C.assign(items * 256 * 3, 0.f);
+    f.ch_last.assign(items * 256, -1);
+    const V3 b{bg[0], bg[1], bg[2]};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < T; t++) {
+        const int tx = t % f.tx, ty = t / f.tx;
+        const int s = f.tile_start[t], e = f.tile_end[t], i0 = f.ch_first[t], nch = f.ch_first[t + 1] - i0;
+        for (int i = ty * TILE; i < std::min(H, (ty + 1) * TILE); i++)
+            for (int j = tx * TILE; j < std::min(W, (tx + 1) * TILE); j++) {
+                const float px = (float)j, py = (float)i;
+                const size_t q = (size_t)(i - ty * TILE) * TILE + (j - tx * TILE);
+                // rasterize_forward_chunked_kernel (.metal:2641-2736): each chunk alone
+                for (int k = 0; k < nch; k++) {
+                    const int cs = s + k * C, ce = std::min(cs + C, e);
+                    float Tr = 1.f;
+                    V3 acc{0.f, 0.f, 0.f};
+                    int last = cs - 1;
+                    for (int kk = cs; kk < ce; kk++) {
+                        V3 xyo = ld3(f.pk_xyo.data(), kk);
+                        float sg = sigma_of(ld3(f.pk_conic.data(), kk), {xyo.x - px, xyo.y - py});
+                        if (sg < 0.f || sg >= 5.55f) continue;
+                        float a = std::min(0.999f, xyo.z * std::exp(-sg));
+                        if (a < 1.f / 255.f) continue;
+                        float nT = Tr * (1.f - a);
+                        if (nT <= 1e-4f) {
+                            last = kk - 1;
+                            break;
+                        }
+                        float vis = a * Tr;
+                        V3 rgb = ld3(f.pk_rgb.data(), kk);
+                        V3 c{std::max(rgb.x + 0.5f, 0.f), std::max(rgb.y + 0.5f, 0.f), std::max(rgb.z + 0.5f, 0.f)};
+                        acc = add(scl(c, vis), acc);
+                        Tr = nT;
+                        last = kk;
+                    }
+                    const size_t it = (size_t)(i0 + k) * 256 + q;
+                    f.ch_T[it] = Tr;
+                    f.ch_C[3 * it] = acc.x;
+                    f.ch_C[3 * it + 1] = acc.y;
+                    f.ch_C[3 * it + 2] = acc.z;
+                    f.ch_last[it] = last;
+                }
+                // rasterize_forward_merge_kernel (.metal:2741-2808): front to back, stop
+                // once T <= 1e-4; the chunks past the stop lose their contributors
+                float Tr = 1.f;
+                V3 acc{0.f, 0.f, 0.f};
+                int last = -1, cut = nch;
+                for (int k = 0; k < nch; k++) {
+                    const size_t it = (size_t)(i0 + k) * 256 + q;
+                    acc.x = std::fma(f.ch_C[3 * it], Tr, acc.x);
+                    acc.y = std::fma(f.ch_C[3 * it + 1], Tr, acc.y);
+                    acc.z = std::fma(f.ch_C[3 * it + 2], Tr, acc.z);
+                    Tr *= f.ch_T[it];
+                    if (f.ch_last[it] >= 0) last = f.ch_last[it];
+                    if (Tr <= 1e-4f) {
+                        cut = k + 1;
+                        break;
+                    }
+                }
+                for (int k = cut; k < nch; k++) f.ch_last[(size_t)(i0 + k) * 256 + q] = -1;
+                const size_t pid = (size_t)i * W + j;
+                f.final_Ts[pid] = Tr;
+                f.final_idx[pid] = last;
+                f.out_img[3 * pid] = clamp01(std::fma(b.x, Tr, acc.x));
+                f.out_img[3 * pid + 1] = clamp01(std::fma(b.y, Tr, acc.y));
+                f.out_img[3 * pid + 2] = clamp01(std::fma(b.z, Tr, acc.z));
+            }
+    }
+}
+
 // core/cpu/msplat_cpu.cpp:629-657
 void forward(State &f, int N, const float *means, const float *scales, float gsc, const float *quats,
              const float *vm, const float *P, float fx, float fy, float cx, float cy, unsigned H, unsigned W,
@@ -586,7 +685,11 @@ void forward(State &f, int N, const float *means, const float *scales, float gsc
     project(f, N, means, scales, gsc, quats, vm, P, fx, fy, cx, cy, clip, degree, dtu, cam, dc, rest);
     bin_sort(f, N, opac);
     const Sky sky = make_sky(pr, fx, fy, cx, cy);
-    raster_fwd(f, bg, sky.on ? pr->sky_tex : nullptr, &sky, vm);
+    f.chunked = g_chunk > 0 && !f.aux;  // the aux rasterizer is one-pass only (as in Metal)
+    if (f.chunked)
+        raster_fwd_chunked(f, bg);
+    else
+        raster_fwd(f, bg, sky.on ? pr->sky_tex : nullptr, &sky, vm);
 }
 
 // core/cpu/msplat_cpu.cpp:669-785 -- zero-padded separable SSIM + L1, forward and
@@ -770,6 +873,95 @@ void raster_bwd(State &f, const float *bg, const float *v_img) {
                     }
                 }
             }
+    }
+}
+
+// Backward of a depth-chunked frame: compute_chunk_prefix_suffix_kernel
+// (.metal:2812-2848) gives each chunk the transmittance in front of it and the colour
+// behind it (every later chunk of the tile, those past the cut-off included, as
+// there), and rasterize_backward_chunked_kernel (:2852-3030) walks the chunk back to
+// front from its own last contributor, starting from T = prefix * chunk T and that
+// colour. The per-Gaussian arithmetic is the one-pass backward's.
+void raster_bwd_chunked(State &f, const float *bg, const float *v_img) {
+    const int W = (int)f.W, H = (int)f.H, T = f.tx * f.ty, C = g_chunk;
+    const int64_t total = T ? f.tile_end[T - 1] : 0;
+    f.isect_grad.assign((size_t)std::max<int64_t>(total, 1) * GS, 0.f);
+    const V3 b{bg[0], bg[1], bg[2]};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < T; t++) {
+        const int s = f.tile_start[t], e = f.tile_end[t], i0 = f.ch_first[t], nch = f.ch_first[t + 1] - i0;
+        if (e == s) continue;
+        const int tx = t % f.tx, ty = t / f.tx;
+        const int r0 = ty * TILE, r1 = std::min(H, (ty + 1) * TILE), c0 = tx * TILE, c1 = std::min(W, (tx + 1) * TILE);
+        const int npx = (r1 - r0) * (c1 - c0);
+        std::vector<float> pre(nch), aft(3 * (size_t)nch);
+        for (int k = 0; k < nch; k++) {
+            const int cs = s + k * C, ce = std::min(cs + C, e);
+            float *lv = f.isect_grad.data() + (size_t)cs * GS;
+            for (int pi = 0; pi < npx; pi++) {
+                const int qq = g_reverse_sums ? npx - 1 - pi : pi;
+                const int i = r0 + qq / (c1 - c0), j = c0 + qq % (c1 - c0);
+                const size_t q = (size_t)(i - r0) * TILE + (j - c0);
+                // prefix and suffix of this pixel's chunks
+                float pT = 1.f;
+                for (int m = 0; m < nch; m++) {
+                    pre[m] = pT;
+                    pT *= f.ch_T[(size_t)(i0 + m) * 256 + q];
+                }
+                V3 aC{0.f, 0.f, 0.f};
+                for (int m = nch - 1; m >= 0; m--) {
+                    aft[3 * m] = aC.x;
+                    aft[3 * m + 1] = aC.y;
+                    aft[3 * m + 2] = aC.z;
+                    const size_t it = (size_t)(i0 + m) * 256 + q;
+                    aC.x += pre[m] * f.ch_C[3 * it];
+                    aC.y += pre[m] * f.ch_C[3 * it + 1];
+                    aC.z += pre[m] * f.ch_C[3 * it + 2];
+                }
+                const size_t it = (size_t)(i0 + k) * 256 + q;
+                const int kf = f.ch_last[it];
+                if (kf < cs) continue;  // no contributor in this chunk (or past the cut-off)
+                const size_t pid = (size_t)i * W + j;
+                const float px = (float)j, py = (float)i;
+                const float Tf = f.final_Ts[pid];
+                float Tr = pre[k] * f.ch_T[it];
+                V3 buf{aft[3 * k], aft[3 * k + 1], aft[3 * k + 2]};
+                const V3 vo = ld3(v_img, pid);
+                const V3 Tbg = scl(Tf, b);
+                for (int kk = std::min(kf, ce - 1); kk >= cs; kk--) {
+                    V3 xyo = ld3(f.pk_xyo.data(), kk);
+                    V3 cn = ld3(f.pk_conic.data(), kk);
+                    V2 d{xyo.x - px, xyo.y - py};
+                    float sg = sigma_of(cn, d);
+                    if (sg < 0.f || sg >= 5.55f) continue;
+                    float a = std::min(0.999f, xyo.z * std::exp(-sg));
+                    if (a < 1.f / 255.f) continue;
+                    float ra = 1.f / (1.f - a);
+                    Tr *= ra;
+                    const float fac = a * Tr;
+                    const V3 raw = ld3(f.pk_rgb.data(), kk);
+                    const V3 rgb{std::max(raw.x + 0.5f, 0.f), std::max(raw.y + 0.5f, 0.f), std::max(raw.z + 0.5f, 0.f)};
+                    V3 nb{-buf.x, -buf.y, -buf.z};
+                    V3 inner = add(scl(nb, ra), scl(-ra, Tbg));
+                    V3 outer = add(scl(rgb, Tr), inner);
+                    float va = dot3(outer, vo);
+                    buf = add(scl(rgb, fac), buf);
+                    float *gg = lv + (size_t)(kk - cs) * GS;
+                    if (raw.x + 0.5f >= 0.f) gg[5] += fac * vo.x;
+                    if (raw.y + 0.5f >= 0.f) gg[6] += fac * vo.y;
+                    if (raw.z + 0.5f >= 0.f) gg[7] += fac * vo.z;
+                    if (a < 0.999f) {
+                        const float vs = -a * va;
+                        gg[2] += 0.5f * vs * d.x * d.x;
+                        gg[3] += 0.5f * vs * d.x * d.y;
+                        gg[4] += 0.5f * vs * d.y * d.y;
+                        gg[0] += vs * (cn.x * d.x + cn.y * d.y);
+                        gg[1] += vs * (cn.y * d.x + cn.z * d.y);
+                        gg[8] += -vs * (1.f - xyo.z);
+                    }
+                }
+            }
+        }
     }
 }
 
@@ -1106,6 +1298,11 @@ int orc_set_option(const char *name, int value) {
         g_reverse_sums = value != 0;
         return 0;
     }
+    if (std::string(name) == "chunk_size") {
+        if (value < 0) return -1;
+        g_chunk = value;
+        return 0;
+    }
     return -1;
 }
 
@@ -1157,7 +1354,10 @@ float orc_train_step(int n, float *means, float *scales, float gsc, float *quats
     if (aux) prior_loss(f, *pr, loss_grad);
     if (expo) exposure_backward_adam(f.out_img.data(), *pr, npix, f.v_adj.data(), f.v_rendered.data(), b1, b2, eps);
     if (sky_on) sky_backward_adam(f, *pr, make_sky(pr, fx, fy, cx, cy), vm, f.v_rendered.data(), b1, b2, eps);
-    raster_bwd(f, bg, f.v_rendered.data());
+    if (f.chunked)
+        raster_bwd_chunked(f, bg, f.v_rendered.data());
+    else
+        raster_bwd(f, bg, f.v_rendered.data());
     reduce_slots(f, n);
     proj_bwd_adam(f, n, means, scales, gsc, quats, vm, P, fx, fy, degree, dtu, cam, dc, rest, m1[3], m2[3], m1[4],
                   m2[4], ss[3], bc2[3], ss[4], bc2[4], b1, b2, eps);
@@ -1211,6 +1411,7 @@ int64_t orc_frame(const char *name, void **ptr) {
     ORC_F("v_depth", g.v_depth, (int64_t)g.v_depth.size())
     ORC_F("out_adj", g.out_adj, (int64_t)g.out_adj.size())
     ORC_F("v_adj", g.v_adj, (int64_t)g.v_adj.size())
+    ORC_F("chunk_first", g.ch_first, g.chunked ? (int64_t)g.ch_first.size() : 0)
 #undef ORC_F
     *ptr = nullptr;
     return -1;

@@ -25,7 +25,10 @@ extern "C" {
 
 /* Restatement only (the reference build does not export it): "reverse_sums" = 1 makes
  * the backward visit pixels and intersection slots in reverse order, i.e. the same
- * gradient sums in another float rounding order. Returns 0, or -1 if unknown. */
+ * gradient sums in another float rounding order; "chunk_size" = C > 0 renders and
+ * trains through depth-chunked compositing with C-long chunks (the Metal backend's
+ * path for small frames), 0 through the one-pass compositing. Returns 0, or -1 if
+ * unknown. */
 int orc_set_option(const char *name, int value);
 
 /* Prior-guided extras (core/metal/bindings.h:43-76, PriorStep), host pointers. The

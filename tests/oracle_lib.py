@@ -31,7 +31,7 @@ u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 _FRAME_DTYPES = {"radii": np.int32, "tile_start": np.int32, "tile_end": np.int32, "isect_gid": np.int32,
-                 "final_idx": np.int32}
+                 "final_idx": np.int32, "chunk_first": np.int32}
 
 
 def available(kind: str) -> bool:
