@@ -300,6 +300,12 @@ def run_ours(args, world, rank, local):
             diff = differentiation_report(dev)
         except Exception as e:
             diff = {"error": str(e)}
+    chunk = None
+    if rank == 0:
+        try:
+            chunk = chunked_report(dev)
+        except Exception as e:
+            chunk = {"error": str(e)}
 
     # ---- render serving (rank 0) ----
     serve = None
@@ -346,6 +352,7 @@ def run_ours(args, world, rank, local):
             "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
             "cpu_baseline": cpu,
             "differentiation": diff,
+            "chunked_compositing": chunk,
             "serving": serve,
             "batching": batching,
         }
@@ -519,6 +526,56 @@ def differentiation_report(dev):
                      "peak_hbm_bytes": ag.pool_device_bytes() + int(torch.cuda.max_memory_allocated(dev))}
     ag.set_transmittance_mode("recompute")
     ag._POOL.clear()
+    return out
+
+
+def chunked_report(dev):
+    """One-pass vs depth-chunked compositing (512-long pieces, the Metal backend's
+    small-frame path) on frames of 256 tiles: mean ms per call over 10 calls after 3
+    warm-ups (CUDA events). Renders of a 1 M-Gaussian scene drawn from the serving
+    distributions, opaque as drawn and with every opacity logit at -4.5 (alpha <= 0.011:
+    no pixel saturates, so one pass walks whole lists), and a 300 k-Gaussian training
+    step."""
+    import torch
+    from msplat_street_b200 import scenes, serving
+    from msplat_street_b200.backend import AdamState, Context, GaussianParams
+    from msplat_street_b200.workloads import BACKGROUND
+
+    def mean_ms(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    cam = scenes.small_camera(256, 256, 230.0, 3.0)
+    out = {"frame": "256x256 (256 tiles)", "chunk_len": 512}
+    p = serving.random_scene_tensors(1_000_000, 7, device=dev)
+    faint = GaussianParams(p.means, p.scales, p.quats, p.features_dc, p.features_rest,
+                           torch.full_like(p.opacities, -4.5))
+    for name, scene in (("render_1m", p), ("render_1m_faint", faint)):
+        row = {}
+        for mode in ("off", "on"):
+            ctx = Context(chunked=mode)
+            row["one_pass_ms" if mode == "off" else "chunked_ms"] = mean_ms(lambda: ctx.render(scene, cam, BACKGROUND))
+            row["intersections"] = ctx.num_isects()
+        out[name] = row
+    g = scenes.random_gaussians(300_000, 11, log_scale_mean=-3.0)
+    gt = torch.rand((256, 256, 3), device=dev)
+    row = {}
+    for mode in ("off", "on"):
+        ctx = Context(chunked=mode)
+        q = GaussianParams.from_numpy(g, dev)
+        adam = AdamState.zeros_like(q, [1.6e-4, 5e-3, 1e-3, 2.5e-3, 2.5e-3, 0.05])
+        stats = tuple(torch.zeros(g.n, device=dev) for _ in range(3))
+        row["one_pass_ms" if mode == "off" else "chunked_ms"] = mean_ms(
+            lambda: ctx.train_step(q, adam, cam, BACKGROUND, gt, stats))
+    out["train_step_300k"] = row
     return out
 
 

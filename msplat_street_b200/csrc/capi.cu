@@ -393,7 +393,7 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     ctx->timer.mark(1, st);
     // render only: the sort carries Gaussian ids, so its sorted values are the
     // per-intersection ids (no emission-index map, no inverse map)
-    launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, d, k0, v0, nullptr, st);
+    launch_emit_keys_batch(n, splats, aabb, n_tiles, offsets, &ds, d, k0, v0, nullptr, st);
     uint32_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
     const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);

@@ -151,9 +151,11 @@ __device__ __forceinline__ int find_view(const int *off, int n_views, int g) {
 }
 
 void launch_project_batch(const BatchDesc &d, int total, cudaStream_t st);
+// ds (may be null): threads take Gaussians in ds's depth order (after
+// launch_depth_offsets) instead of by index; the entries are the same.
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                            const int64_t *offsets, const BatchDesc &d, uint32_t *keys, uint32_t *vals,
-                            int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
+                            const int64_t *offsets, const DepthScratch *ds, const BatchDesc &d, uint32_t *keys,
+                            uint32_t *vals, int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
 void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant = 0);
 
 struct RasterBwdArgs {

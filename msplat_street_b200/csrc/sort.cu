@@ -16,6 +16,7 @@
 // scan of the digit-major counts, and a scatter kernel that ranks keys stably inside
 // each 2048-key block with warp match/popc. No block waits on another block.
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -190,6 +191,8 @@ void launch_depth_offsets(int n, const Splat *splats, const int32_t *n_tiles, De
     const int nb = (n + 255) / 256;
     depth_keys_kernel<<<nb, 256, 0, st>>>(n, splats, n_tiles, s.keys[0], s.vals[0]);
     const int cur = radix_sort_pairs32(s.keys, s.vals, n, 32, s.radix_scratch, st);
+    if (cur != 0)  // four 8-bit passes end in buffer 0; emission reads the order there
+        cudaMemcpyAsync(s.vals[0], s.vals[1], (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
     gather_counts_kernel<<<nb, 256, 0, st>>>(n, s.vals[cur], n_tiles, s.counts);
     scan_exclusive<int64_t>(s.counts, s.off_sorted, n, d_total, scan_part, st);
     scatter_offsets_kernel<<<nb, 256, 0, st>>>(n, s.vals[cur], s.off_sorted, offsets);
@@ -205,16 +208,36 @@ __device__ __forceinline__ void rect_of(const Splat &s, float ax, float ay, int 
     y1 = min(max(0, (int)(ccy + rry + 1)), ty);
 }
 
-// Emits the intersections of each thread's Gaussian: the tiles of its rectangle
-// [x0, x1) x [y0, y1) in row-major order at emission indices e0, e0 + 1, ..., key =
-// base + tile id, value = emission index (or, with emit_gid null -- render-only
-// frames with no backward -- the Gaussian id itself, so the sorted values are the
-// per-intersection ids with no gather). Rectangles of up to SMALL_RECT tiles are
-// written by their own thread; larger ones by the whole warp, lane l writing entries
-// l, l + 32, ..., so the stores of the big (near-camera) Gaussians coalesce. Every
-// lane of the warp must call it. cap: buffer capacity (entries at or past it dropped).
+// Emission of each Gaussian's intersections: the tiles of its rectangle [x0, x1) x
+// [y0, y1) in row-major order at emission indices e0, e0 + 1, ..., key = base + tile
+// id, value = emission index (or, with emit_gid null -- render-only frames with no
+// backward -- the Gaussian id itself, so the sorted values are the per-intersection
+// ids with no gather). cap: buffer capacity (entries at or past it are dropped).
+// Rectangles of up to SMALL_RECT tiles are written by their own thread; larger ones by
+// the whole warp, lane l writing entries l, l + 32, ..., so their stores coalesce.
+//
+// Two thread-to-Gaussian maps, the same entries either way. BY_DEPTH: thread j takes
+// the Gaussian at position j of the depth order; the emission offsets follow that
+// order, so neighbouring threads write neighbouring ranges and stores fill whole
+// sectors between them -- the better map when most Gaussians cover a few tiles each
+// (renders of large scenes). By index: thread i takes Gaussian i; near-camera
+// Gaussians with hundreds of tiles, which sit side by side in the depth order, then
+// spread over many warps instead of falling to a few warps one after another -- the
+// better map for training views, where such Gaussians carry much of the work.
 constexpr int SMALL_RECT = 8;
 
+__device__ __forceinline__ void emit_one(int64_t e, uint32_t key, int gid, uint32_t *keys, uint32_t *vals,
+                                         int32_t *emit_gid) {
+    keys[e] = key;
+    if (emit_gid) {
+        vals[e] = (uint32_t)e;
+        emit_gid[e] = gid;
+    } else {
+        vals[e] = (uint32_t)gid;
+    }
+}
+
+// Every lane of the warp must call it.
 __device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y1, int tiles_x, uint32_t base,
                                           int64_t e0, int gid, int64_t cap, uint32_t *keys, uint32_t *vals,
                                           int32_t *emit_gid) {
@@ -222,15 +245,8 @@ __device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y
     if (cnt > 0 && cnt <= SMALL_RECT) {
         int64_t e = e0;
         for (int y = y0; y < y1; y++)
-            for (int x = x0; x < x1 && e < cap; x++, e++) {
-                keys[e] = base + (uint32_t)(y * tiles_x + x);
-                if (emit_gid) {
-                    vals[e] = (uint32_t)e;
-                    emit_gid[e] = gid;
-                } else {
-                    vals[e] = (uint32_t)gid;
-                }
-            }
+            for (int x = x0; x < x1 && e < cap; x++, e++)
+                emit_one(e, base + (uint32_t)(y * tiles_x + x), gid, keys, vals, emit_gid);
     }
     unsigned big = __ballot_sync(0xffffffffu, cnt > SMALL_RECT);
     const int lane = threadIdx.x & 31;
@@ -245,68 +261,77 @@ __device__ __forceinline__ void emit_rect(bool ok, int x0, int y0, int x1, int y
         for (int j = lane; j < sc; j += 32) {
             const int64_t e = se + j;
             if (e >= cap) break;
-            const int yy = sy0 + j / sw, xx = sx0 + j % sw;
-            keys[e] = sb + (uint32_t)(yy * stx + xx);
-            if (emit_gid) {
-                vals[e] = (uint32_t)e;
-                emit_gid[e] = sg;
-            } else {
-                vals[e] = (uint32_t)sg;
-            }
+            emit_one(e, sb + (uint32_t)((sy0 + j / sw) * stx + sx0 + j % sw), sg, keys, vals, emit_gid);
         }
     }
 }
 
-__global__ void emit_keys_kernel(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                                 const int64_t *offsets, int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals,
-                                 int32_t *emit_gid) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool ok = i < n && n_tiles[i] > 0;
-    int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+struct EmitSrc {
+    const int32_t *n_tiles;      // per Gaussian (index map)
+    const int64_t *offsets;      // per Gaussian (index map)
+    const uint32_t *order;       // depth order (BY_DEPTH)
+    const int32_t *cnt_sorted;   // tile counts in depth order (BY_DEPTH)
+    const int64_t *off_sorted;   // emission offsets in depth order (BY_DEPTH)
+};
+
+// BATCH: instance g (a Gaussian of one view) keys its tiles with the view's first
+// global tile added, so one stable sort orders every view's tiles at once and each
+// tile's list is the one the single-view sort gives.
+template <bool BATCH, bool BY_DEPTH>
+__global__ void emit_keys_kernel(int n, const Splat *splats, const float *aabb, const EmitSrc src, int tiles_x,
+                                 int tiles_y, const BatchDesc d, uint32_t *keys, uint32_t *vals, int32_t *emit_gid,
+                                 int64_t cap) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = j < n && (BY_DEPTH ? src.cnt_sorted[j] : src.n_tiles[j]) > 0;
+    int x0 = 0, y0 = 0, x1 = 0, y1 = 0, g = 0, tx = tiles_x;
+    uint32_t base = 0;
     int64_t e0 = 0;
     if (ok) {
-        const Splat s = splats[i];
-        rect_of(s, aabb[2 * i], aabb[2 * i + 1], tiles_x, tiles_y, x0, y0, x1, y1);
-        e0 = offsets[i];
+        g = BY_DEPTH ? (int)src.order[j] : j;
+        int ty = tiles_y;
+        if (BATCH) {
+            const int v = find_view(d.inst_off, d.n_views, g);
+            tx = d.tiles_x[v];
+            ty = d.tiles_y[v];
+            base = (uint32_t)d.tile_off[v];
+        }
+        rect_of(splats[g], aabb[2 * g], aabb[2 * g + 1], tx, ty, x0, y0, x1, y1);
+        e0 = BY_DEPTH ? src.off_sorted[j] : src.offsets[g];
     }
-    emit_rect(ok, x0, y0, x1, y1, tiles_x, 0u, e0, i, INT64_MAX, keys, vals, emit_gid);
+    emit_rect(ok, x0, y0, x1, y1, tx, base, e0, g, cap, keys, vals, emit_gid);
 }
+
+namespace {
+EmitSrc emit_src(const int32_t *n_tiles, const int64_t *offsets, const DepthScratch *ds) {
+    EmitSrc s{n_tiles, offsets, nullptr, nullptr, nullptr};
+    if (ds) {
+        s.order = ds->vals[0];
+        s.cnt_sorted = ds->counts;
+        s.off_sorted = ds->off_sorted;
+    }
+    return s;
+}
+}  // namespace
 
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
                       int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st) {
     if (n <= 0) return;
-    emit_keys_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, n_tiles, offsets, tiles_x, tiles_y, keys, vals,
-                                                      emit_gid);
-}
-
-// Batched emission: instance g (a Gaussian of one view) keys its tiles with the
-// view's first global tile added, so one stable sort orders every view's tiles at
-// once and each tile's list is the one the single-view sort gives.
-__global__ void emit_keys_batch_kernel(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                                       const int64_t *offsets, const BatchDesc d, uint32_t *keys, uint32_t *vals,
-                                       int32_t *emit_gid, int64_t cap) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool ok = g < n && n_tiles[g] > 0;
-    int x0 = 0, y0 = 0, x1 = 0, y1 = 0, tiles_x = 0;
-    uint32_t base = 0;
-    int64_t e0 = 0;
-    if (ok) {
-        const int v = find_view(d.inst_off, d.n_views, g);
-        tiles_x = d.tiles_x[v];
-        base = (uint32_t)d.tile_off[v];
-        const Splat s = splats[g];
-        rect_of(s, aabb[2 * g], aabb[2 * g + 1], tiles_x, d.tiles_y[v], x0, y0, x1, y1);
-        e0 = offsets[g];
-    }
-    emit_rect(ok, x0, y0, x1, y1, tiles_x, base, e0, g, cap, keys, vals, emit_gid);
+    emit_keys_kernel<false, false><<<(n + 127) / 128, 128, 0, st>>>(
+        n, splats, aabb, emit_src(n_tiles, offsets, nullptr), tiles_x, tiles_y, BatchDesc{}, keys, vals, emit_gid,
+        INT64_MAX);
 }
 
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
-                            const int64_t *offsets, const BatchDesc &d, uint32_t *keys, uint32_t *vals,
-                            int32_t *emit_gid, cudaStream_t st, int64_t cap) {
+                            const int64_t *offsets, const DepthScratch *ds, const BatchDesc &d, uint32_t *keys,
+                            uint32_t *vals, int32_t *emit_gid, cudaStream_t st, int64_t cap) {
     if (n <= 0) return;
-    emit_keys_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, n_tiles, offsets, d, keys, vals,
-                                                            emit_gid, cap);
+    const EmitSrc src = emit_src(n_tiles, offsets, ds);
+    if (ds)
+        emit_keys_kernel<true, true><<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, src, 0, 0, d, keys, vals,
+                                                                      emit_gid, cap);
+    else
+        emit_keys_kernel<true, false><<<(n + 127) / 128, 128, 0, st>>>(n, splats, aabb, src, 0, 0, d, keys, vals,
+                                                                       emit_gid, cap);
 }
 
 // ---------------------------------------------------------------------------------
@@ -314,14 +339,25 @@ void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const
 // 32- and 64-bit keys.
 
 constexpr int RADIX = 256;
-constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32, SORT_ITEMS = 8;
-constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // keys per block
-constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per warp
+// Keys per block: SORT_THREADS x ITEMS. Large sorts take 16 items a thread (4096 keys
+// a block): each digit's run in a block then averages 16 entries, so the scatter's
+// stores come in runs of 64 bytes or more, and the per-block digit counts (256 per
+// block, scanned every pass) stay small next to the keys. Below LARGE_SORT keys, 8
+// items (2048 keys a block) keep enough blocks to fill the GPU.
+constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32;
+constexpr int LARGE_SORT = 4 << 20;
 
-int radix_blocks(int n) { return (n + SORT_TILE - 1) / SORT_TILE; }
+int sort_items(int n) { return n >= LARGE_SORT ? 16 : 8; }
+int radix_blocks(int n) {
+    const int tile = SORT_THREADS * sort_items(n);
+    return (n + tile - 1) / tile;
+}
+// The most blocks any sort of up to n keys uses (scratch sizing: a sort just below
+// LARGE_SORT has more blocks than one just above it).
+int radix_max_blocks(int n) { return std::max(radix_blocks(std::min(n, LARGE_SORT - 1)), radix_blocks(n)); }
 
 // d_n (may be null): a device-side count that caps n (capacity-bounded launches)
-template <typename K>
+template <typename K, int SORT_ITEMS>
 __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shift, uint32_t mask, uint32_t *counts,
                                   int nb) {
     __shared__ uint32_t h[RADIX];
@@ -329,6 +365,7 @@ __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shif
     for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
     const int base = blockIdx.x * SORT_TILE;
     int dig[SORT_ITEMS];
 #pragma unroll
@@ -347,7 +384,7 @@ __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shif
 }
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
-template <typename K>
+template <typename K, int SORT_ITEMS>
 __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout, uint32_t *vout, int n,
                                      const int *d_n, int shift, uint32_t mask, const int32_t *offs, int nb) {
     // The block's keys are first ranked and placed in shared memory in digit order
@@ -355,9 +392,12 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     // write consecutive entries of each digit's run: coalesced global stores.
     __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
     __shared__ uint32_t gbase[RADIX], bstart[RADIX + 1];
+    constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // keys per block
+    constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per warp
     __shared__ uint32_t ws[33];
-    __shared__ K skey[SORT_TILE];
-    __shared__ uint32_t sval[SORT_TILE];
+    extern __shared__ __align__(16) unsigned char sort_smem[];  // radix_scatter_smem<K, SORT_ITEMS>()
+    K *skey = reinterpret_cast<K *>(sort_smem);
+    uint32_t *sval = reinterpret_cast<uint32_t *>(skey + SORT_TILE);
     if (d_n) n = min(n, *d_n);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&wcnt[0][0])[i] = 0;
@@ -424,8 +464,13 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     }
 }
 
+template <typename K, int ITEMS>
+constexpr size_t radix_scatter_smem() {
+    return (size_t)SORT_THREADS * ITEMS * (sizeof(K) + sizeof(uint32_t));
+}
+
 size_t radix_scratch_bytes(int n) {
-    const int nb = radix_blocks(n > 1 ? n : 1);
+    const int nb = radix_max_blocks(n > 1 ? n : 1);
     const size_t cnt = (size_t)RADIX * nb;
     return cnt * sizeof(int32_t) * 2 + (size_t)scan_blocks((int)cnt) * sizeof(int32_t) + 64;
 }
@@ -433,36 +478,54 @@ size_t radix_scratch_bytes(int n) {
 // Sorts (k[0], v[0]) using (k[1], v[1]) as the ping-pong buffers; returns the index
 // (0 or 1) of the buffer pair holding the result. With d_n, n is a capacity and the
 // count is read on the device (no host round trip; every pass runs).
-template <typename K>
+template <typename K, int ITEMS>
 int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
-    if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
     const int nb = radix_blocks(n);
     const size_t cnt = (size_t)RADIX * nb;
     int32_t *counts = reinterpret_cast<int32_t *>(scratch);
     int32_t *offs = counts + cnt;
     int32_t *partials = offs + cnt;
+    constexpr size_t smem = radix_scatter_smem<K, ITEMS>();
+    if (smem > 32 * 1024) {  // with the static arrays, above the 48 KB default: opt in once per device
+        static std::atomic<uint64_t> done{0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const uint64_t bit = 1ull << (dev & 63);
+        if (!(done.load() & bit)) {
+            cudaFuncSetAttribute(radix_scatter_kernel<K, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            done.fetch_or(bit);
+        }
+    }
     int cur = 0;
     for (int shift = 0; shift < key_bits; shift += 8) {
         const int bits = key_bits - shift < 8 ? key_bits - shift : 8;  // digits above key_bits are ignored
         const uint32_t mask = (1u << bits) - 1u;
-        radix_hist_kernel<K><<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
-                                                          reinterpret_cast<uint32_t *>(counts), nb);
+        radix_hist_kernel<K, ITEMS><<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
+                                                                 reinterpret_cast<uint32_t *>(counts), nb);
         scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<K><<<nb, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift,
-                                                             mask, offs, nb);
+        radix_scatter_kernel<K, ITEMS><<<nb, SORT_THREADS, smem, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n,
+                                                                       d_n, shift, mask, offs, nb);
         cur ^= 1;
     }
     return cur;
 }
 
+template <typename K>
+int radix_sort_dispatch(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
+    if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
+    return sort_items(n) == 16 ? radix_sort_impl<K, 16>(k, v, n, key_bits, scratch, st, d_n)
+                               : radix_sort_impl<K, 8>(k, v, n, key_bits, scratch, st, d_n);
+}
+
 int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
                      const int *d_n) {
-    return radix_sort_impl<uint64_t>(k, v, n, key_bits, scratch, st, d_n);
+    return radix_sort_dispatch<uint64_t>(k, v, n, key_bits, scratch, st, d_n);
 }
 
 int radix_sort_pairs32(uint32_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
                        const int *d_n) {
-    return radix_sort_impl<uint32_t>(k, v, n, std::min(key_bits, 32), scratch, st, d_n);
+    return radix_sort_dispatch<uint32_t>(k, v, n, std::min(key_bits, 32), scratch, st, d_n);
 }
 
 // ---------------------------------------------------------------------------------

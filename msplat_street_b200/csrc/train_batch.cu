@@ -321,7 +321,7 @@ void enqueue_rest(const StepArgs &a, const StepPtrs &P, int64_t isect_cap, int t
     int *d_n = P.counters + C_NISECT, *d_over = P.counters + C_OVERFLOW;
     cudaMemsetAsync(P.counters, 0, N_COUNTERS * sizeof(int), st);
     launch_clamp_count(P.total, isect_cap, d_n, d_over, st);
-    launch_emit_keys_batch(inst, P.splats, P.aabb, P.n_tiles, P.offsets, d, P.k[0], P.v[0], P.emit_gid, st,
+    launch_emit_keys_batch(inst, P.splats, P.aabb, P.n_tiles, P.offsets, nullptr, d, P.k[0], P.v[0], P.emit_gid, st,
                            isect_cap);
     uint32_t *kk[2] = {P.k[0], P.k[1]};
     uint32_t *vv[2] = {P.v[0], P.v[1]};
