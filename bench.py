@@ -657,7 +657,7 @@ def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
             "avg_ms": ms, "algorithmic_bytes": algo}
 
 
-PROFILE_CASES = ("sort", "ssim", "adam", "densify")
+PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")
 
 
 def profile_case(name: str, dev) -> dict:
@@ -667,7 +667,9 @@ def profile_case(name: str, dev) -> dict:
       sort     stable radix sort of 32 M (u64 key, i32 value) pairs, 40 key bits (5 passes)
       ssim     fused L1 + SSIM forward and backward of a 4096 x 4096 render
       adam     backward/Adam of a training step over 1 M Gaussians (SH degree 3)
-      densify  clone / split / prune + compaction of 500 k Gaussians (capacity 2 M)"""
+      densify  clone / split / prune + compaction of 500 k Gaussians (capacity 2 M)
+      render   a batched render (the serving path) of a 3 M-Gaussian scene drawn from
+               the serving distributions at 1920 x 1080 from 5 m"""
     import torch
     from msplat_street_b200 import autograd, scenes
     from msplat_street_b200.backend import AdamState, Context, GaussianParams
@@ -721,6 +723,16 @@ def profile_case(name: str, dev) -> dict:
             ms = torch.rand(n, device=dev, generator=g) * 0.3
             new_n = ctx.densify(n, bufs, m1, m2, gn, vc, ms, 512.0, 1234)
         out.update(gaussians=n, capacity=cap, new_gaussians=new_n, floats_per_gaussian=59, arrays=3)
+    elif name == "render":
+        from msplat_street_b200 import serving
+        from msplat_street_b200.backend import BatchItem
+        from msplat_street_b200.workloads import BACKGROUND
+        p = serving.random_scene_tensors(3_000_000, 7, device=dev)
+        cam = scenes.sphere_camera(np.random.default_rng(3), 1920, 1080, radius=5.0)
+        for _ in range(2):
+            ctx.render_batch([BatchItem(p, cam, BACKGROUND)])
+        torch.cuda.synchronize()
+        out.update(gaussians=3_000_000, resolution="1920x1080", isects=ctx.num_isects())
     torch.cuda.synchronize()
     return out
 
