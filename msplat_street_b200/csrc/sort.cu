@@ -357,6 +357,21 @@ int radix_blocks(int n) {
 int radix_max_blocks(int n) { return std::max(radix_blocks(std::min(n, LARGE_SORT - 1)), radix_blocks(n)); }
 
 // d_n (may be null): a device-side count that caps n (capacity-bounded launches)
+// The lanes of the warp whose digit equals this lane's (d in 0..RADIX, RADIX marking
+// a lane with no key): nine ballots, one per bit of d, each narrowing the set to the
+// lanes that agree on that bit. Constant cost whatever the number of distinct digits
+// in the warp (a warp of scattered tile ids holds up to 32).
+__device__ __forceinline__ unsigned digit_peers(int d) {
+    unsigned m = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; b++) {
+        const bool on = (d >> b) & 1;
+        const unsigned bal = __ballot_sync(0xffffffffu, on);
+        m &= on ? bal : ~bal;
+    }
+    return m;
+}
+
 template <typename K, int SORT_ITEMS>
 __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shift, uint32_t mask, uint32_t *counts,
                                   int nb) {
@@ -376,7 +391,7 @@ __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shif
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
         const int d = dig[j];
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = digit_peers(d);
         if (d < RADIX && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
     }
     __syncthreads();
@@ -420,7 +435,7 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     for (int r = 0; r < SORT_ITEMS; r++) {
         const int d = dig[r];
         const bool ok = d < RADIX;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = digit_peers(d);
         const uint32_t before = ok ? wcnt[warp][d] : 0u;
         rank[r] = before + (uint32_t)__popc(peers & lt);
         __syncwarp();
