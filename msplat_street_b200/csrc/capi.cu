@@ -1273,7 +1273,7 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         Buf *buf;
         int64_t count;
     } table[] = {
-        {"splats", &ctx->splats, n * 12},
+        {"splats", &ctx->splats, n * SPLAT_FLOATS},
         {"radii", &ctx->radii, n},
         {"aabb", &ctx->aabb, n * 2},
         {"tile_start", &ctx->tile_start, T},

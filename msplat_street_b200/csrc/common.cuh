@@ -13,6 +13,7 @@
 // types follow MSL conventions (core/cpu/cpu_math.hpp:1-4).
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -130,14 +131,30 @@ __device__ __forceinline__ void cov3d_of(V3 s, float g, Q4 q, float *cov) {
     cov[5] = t.c[2].z;
 }
 
+// Two floats as a half2 (low half first), each rounded toward +infinity (values
+// beyond the half range become +inf, or -65504 from below).
+__device__ __forceinline__ uint32_t pack_half2_up(float lo, float hi) {
+    const __half l = __float2half_ru(lo), h = __float2half_ru(hi);
+    return (uint32_t)__half_as_ushort(l) | ((uint32_t)__half_as_ushort(h) << 16);
+}
+__device__ __forceinline__ float2 unpack_half2(uint32_t v) {
+    return make_float2(__half2float(__ushort_as_half((unsigned short)(v & 0xffffu))),
+                       __half2float(__ushort_as_half((unsigned short)(v >> 16))));
+}
+
 // One splat record per Gaussian, read by the rasterizer: centre, conic, sigmoid
-// opacity, raw SH colour and the half-extents of the box outside which it cannot be
-// composited (alpha < 1/255), 48 bytes so it loads as three float4.
+// opacity, raw SH colour, depth, and the extents of the region where it can be
+// composited (alpha >= 1/255): the half-widths of its box and its half-extents along
+// the diagonals x + y and x - y, each a half-precision float rounded up (a region
+// never shrinks; -inf marks a splat that never reaches 1/255, +inf an extent with no
+// bound). 48 bytes, loaded as three float4.
 struct __align__(16) Splat {
     float x, y, cx, cy;   // pixel centre, conic (a, b)
     float cz, op, r, g;   // conic c, sigmoid(opacity), raw colour r g
-    float b, depth, ex, ey;
+    float b, depth;       // raw colour b, view depth
+    uint32_t box, diag;   // half2 (ex, ey) and half2 (hp, hm)
 };
+constexpr int SPLAT_FLOATS = sizeof(Splat) / sizeof(float);
 
 // Pixels of a 16x16 tile owned by one warp: an 8x4 block (warp w covers columns
 // 8 * (w % 2) .. +7 and rows 4 * (w / 2) .. +3), compact so that per-warp culling

@@ -135,7 +135,8 @@ __device__ __forceinline__ void project_one(const ProjectArgs &a, int i, int64_t
     // double with margins, so the rasterizers may skip pixel blocks outside it without
     // changing any result. An empty box marks a Gaussian that never reaches 1/255.
     float ex = -1e30f, ey = -1e30f;
-    const double L = fmin(5.55, log(255.0 * (double)op) + 1e-4);
+    const double lg = log(255.0 * (double)op);
+    const double L = fmin(5.55, lg + 1e-4);
     if (L > 0.0) {
         const double ca = conic.x, cb = conic.y, cc = conic.z;
         const double cdet = ca * cc - cb * cb;
@@ -146,10 +147,25 @@ __device__ __forceinline__ void project_one(const ProjectArgs &a, int i, int64_t
             ex = ey = 1e30f;  // not positive definite: never skip
         }
     }
+    // The same region's half-extents along the diagonals, sqrt(2 L u^T C^-1 u) for
+    // u = (1, 1) and (1, -1), with a wider margin on L: the rasterizers test each
+    // warp's 8x4 pixel block against them (separating axes; rotated, elongated splats
+    // have boxes much larger than themselves). Infinite: the box test alone.
+    float hp = __int_as_float(0x7f800000), hm = hp;
+    {
+        const double ca = conic.x, cb = conic.y, cc = conic.z;
+        const double det2 = ca * cc - cb * cb;
+        const double Ld = fmin(5.55, lg) + 1e-2;
+        if (det2 > 0.0 && ca > 0.0 && cc > 0.0 && Ld > 0.0) {
+            hp = (float)(sqrt(2.0 * Ld * fmax(ca + cc - 2.0 * cb, 0.0) / det2) * 1.001 + 0.5);
+            hm = (float)(sqrt(2.0 * Ld * fmax(ca + cc + 2.0 * cb, 0.0) / det2) * 1.001 + 0.5);
+        }
+    }
+    if (ex < -1e29f) ex = ey = -__int_as_float(0x7f800000);  // never reaches 1/255
     float4 *rec = reinterpret_cast<float4 *>(a.splats + o);
     rec[0] = make_float4(ctx, cty, conic.x, conic.y);
     rec[1] = make_float4(conic.z, op, col[0], col[1]);
-    rec[2] = make_float4(col[2], pv.z, ex, ey);
+    rec[2] = make_float4(col[2], pv.z, __uint_as_float(pack_half2_up(ex, ey)), __uint_as_float(pack_half2_up(hp, hm)));
 }
 
 }  // namespace msplat

@@ -51,14 +51,14 @@ __device__ __forceinline__ float staged_colour(float raw) {
 // Which of a tile's eight 8x4 warp blocks (warp w covers columns 8 (w % 2) .. +7 and
 // rows 4 (w / 2) .. +3) a splat can reach with alpha >= 1/255: bit w set unless the
 // block lies outside the splat's box (x + ex < block x0 || x - ex > x1 || y + ey < y0
-// || y - ey > y1) or outside the ellipse's extent along either diagonal, x + y and
-// x - y (separating axes; rotated, elongated splats have boxes much larger than
-// themselves). The diagonal half-extents sqrt(2 L u^T C^-1 u), L = min(5.55,
-// ln(255 o)), are evaluated in double with margins (as the box is), so a block is
-// dropped only when no pixel in it can take part. Computed once per staged splat.
-__device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4 B, const float4 C, int tx,
-                                                    int ty) {
-    const float xr = A.x + C.z, xl = A.x - C.z, yb = A.y + C.w, yt = A.y - C.w;
+// || y - ey > y1) or outside the region's extent along either diagonal, x + y and
+// x - y (separating axes). Both extents come with the record, computed once per
+// Gaussian by the projection in double with margins and stored rounded up, so a block
+// is dropped only when no pixel in it can take part. C = record[2] (its z and w hold
+// the packed box and diagonal extents).
+__device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4 C, int tx, int ty) {
+    const float2 box = unpack_half2(__float_as_uint(C.z));
+    const float xr = A.x + box.x, xl = A.x - box.x, yb = A.y + box.y, yt = A.y - box.y;
     uint32_t cols = 0u, mask = 0u;
 #pragma unroll
     for (int c = 0; c < 2; c++) {
@@ -71,12 +71,8 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4
         if (!(yb < by0 || yt > by1)) mask |= cols << (2 * r);
     }
     if (!mask) return 0u;
-    const double ca = A.z, cb = A.w, cc = B.x;  // conic
-    const double det = ca * cc - cb * cb;
-    const double L = fmin(5.55, log(255.0 * (double)B.y)) + 1e-2;
-    if (!(det > 0.0 && ca > 0.0 && cc > 0.0 && L > 0.0)) return mask;  // box only
-    const float hp = (float)(sqrt(2.0 * L * fmax(ca + cc - 2.0 * cb, 0.0) / det) * 1.001 + 0.5);
-    const float hm = (float)(sqrt(2.0 * L * fmax(ca + cc + 2.0 * cb, 0.0) / det) * 1.001 + 0.5);
+    const float2 dg = unpack_half2(__float_as_uint(C.w));
+    const float hp = dg.x, hm = dg.y;
     const float sp = A.x + A.y, sd = A.x - A.y;
 #pragma unroll
     for (int w = 0; w < 8; w++) {
@@ -125,7 +121,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
             s0[threadIdx.x] = A;
             s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
             s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
-            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, B, C, tx, ty);
+            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
         }
         __syncthreads();
         const int cnt = min(FB, end - b0);
@@ -212,7 +208,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
 // until none are left. A tile's image equals what the per-view kernel renders: the
 // same list (the batch sort keeps each tile's order) and the same code.
 template <int FB>
-__global__ void __launch_bounds__(TILE_PIX) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
+__global__ void __launch_bounds__(TILE_PIX, 4) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     __shared__ int s_tile, s_lt;
@@ -357,7 +353,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         if (threadIdx.x < cnt) {
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[b_start + threadIdx.x]);
             const float4 A = rec[0], B = rec[1], C = rec[2];
-            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, B, C, tx, ty);
+            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
             s0[threadIdx.x] = A;
             s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
             s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
