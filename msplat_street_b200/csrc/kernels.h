@@ -93,7 +93,7 @@ struct RasterVariant {
 };
 constexpr int N_RASTER_VARIANTS = 8;
 constexpr RasterVariant RASTER_VARIANTS[N_RASTER_VARIANTS] = {
-    {128, 64, 4}, {256, 64, 8}, {256, 64, 4}, {256, 32, 4}, {128, 32, 4}, {64, 32, 4}, {256, 128, 4}, {128, 16, 4}};
+    {128, 128, 3}, {128, 64, 3}, {128, 64, 4}, {256, 128, 3}, {64, 128, 3}, {256, 64, 4}, {128, 32, 4}, {256, 128, 4}};
 inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v : 0; }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);

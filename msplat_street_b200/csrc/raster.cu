@@ -561,8 +561,9 @@ void bwd_batch_launch(const RasterBwdArgs *d_views, const int *d_tile_off, int n
 }
 
 // The backward variants' (staged batch, reduction sub-batch) pairs, dispatched to
-// their template instances.
-#define MSPLAT_BWD_VARIANTS(X) X(64, 4) X(64, 8) X(32, 4) X(128, 4) X(16, 4)
+// their template instances. A sub-batch of 3 gives 27 sums per warp round (9 values
+// x 3 splats), one pass of the warp's lanes; 4 gives 36, two passes with 4 lanes busy.
+#define MSPLAT_BWD_VARIANTS(X) X(128, 3) X(64, 3) X(64, 4) X(32, 4) X(128, 4)
 
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
     const int T = a.tiles_x * a.tiles_y;
@@ -575,7 +576,7 @@ void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
     }
     MSPLAT_BWD_VARIANTS(X)
 #undef X
-    bwd_launch<64, 4>(a, T, st);
+    bwd_launch<128, 3>(a, T, st);
 }
 
 // The aux backward, default staging only (as launch_raster_fwd_aux).
@@ -603,7 +604,7 @@ void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off
     }
     MSPLAT_BWD_VARIANTS(X)
 #undef X
-    bwd_batch_launch<64, 4>(d_views, d_tile_off, n_views, d_counter, st);
+    bwd_batch_launch<128, 3>(d_views, d_tile_off, n_views, d_counter, st);
 }
 
 // ---------------------------------------------------------------------------------
@@ -768,7 +769,7 @@ void launch_raster_bwd_chunked(const RasterBwdArgs &a, const ChunkArgs &c, int64
     }
     MSPLAT_BWD_VARIANTS(X)
 #undef X
-    bwd_chunk_launch<64, 4>(a, c, item_cap, st);
+    bwd_chunk_launch<128, 3>(a, c, item_cap, st);
 }
 
 }  // namespace msplat

@@ -35,7 +35,7 @@ def _step(variant):
 
 def test_variants_give_identical_results():
     vs = autotune.raster_variants()
-    assert len(vs) >= 4 and vs[0] == {"variant": 0, "fwd_batch": 128, "bwd_batch": 64, "bwd_sub": 4}
+    assert len(vs) >= 4 and vs[0] == {"variant": 0, "fwd_batch": 128, "bwd_batch": 128, "bwd_sub": 3}
     ref = _step(0)
     for d in vs[1:]:
         got = _step(d["variant"])
