@@ -583,13 +583,13 @@ void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
 void launch_raster_bwd_aux(const RasterBwdArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    constexpr size_t smem = raster_bwd_smem<64, 4, 10>();
+    constexpr size_t smem = raster_bwd_smem<64, 3, 10>();
     static const bool attr = [] {
-        cudaFuncSetAttribute(raster_bwd_kernel<64, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(raster_bwd_kernel<64, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return true;
     }();
     (void)attr;
-    raster_bwd_kernel<64, 4, true><<<T, TILE_PIX, smem, st>>>(a);
+    raster_bwd_kernel<64, 3, true><<<T, TILE_PIX, smem, st>>>(a);
 }
 
 void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
