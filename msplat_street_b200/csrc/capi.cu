@@ -499,7 +499,9 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
         return MSPLAT_CUDA_OK;
     }
     if (!std::strcmp(name, "chunk_len")) {
-        if (value < 1 || value > (1 << 20)) return fail(MSPLAT_CUDA_EINVAL, "chunk_len must be 1..2^20");
+        // at least 16: the per-piece planes (36 bytes per pixel per piece) stay within
+        // about 2.25 bytes per intersection per pixel of the tile
+        if (value < 16 || value > (1 << 20)) return fail(MSPLAT_CUDA_EINVAL, "chunk_len must be 16..2^20");
         ctx->chunk_len = (int)value;
         return MSPLAT_CUDA_OK;
     }
