@@ -70,7 +70,7 @@ int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
  * without a prior, as the Metal backend; 2 = every frame without a prior. Images
  * differ from one pass by what the per-piece stops let through, about 1e-4; the
  * batched entry points always composite in one pass);
- * "chunk_len" (the piece length, 512 by default as in the Metal backend). */
+ * "chunk_len" (the piece length, 16..2^20, 512 by default as in the Metal backend). */
 int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
 /* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
  * backward round, and the backward reduction's sub-batch. Returns the variant count. */
