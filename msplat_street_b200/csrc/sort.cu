@@ -347,6 +347,11 @@ constexpr int RADIX = 256;
 constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32;
 constexpr int LARGE_SORT = 4 << 20;
 
+// Up to this many blocks (131,072 keys at 2048 a block, the depth order of a training
+// view), each scatter block sums the per-block digit counts itself instead of a
+// separate scan launch over them.
+constexpr int DIRECT_SORT_BLOCKS = 64;
+
 int sort_items(int n) { return n >= LARGE_SORT ? 16 : 8; }
 int radix_blocks(int n) {
     const int tile = SORT_THREADS * sort_items(n);
@@ -400,8 +405,12 @@ __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shif
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
 template <typename K, int SORT_ITEMS>
+// offs: the exclusive digit-major scan of the per-block digit counts; or, with offs
+// null (a sort of at most DIRECT_SORT_BLOCKS blocks), counts: the per-block digit counts
+// themselves, from which each block forms its own digit starts (no scan launch).
 __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout, uint32_t *vout, int n,
-                                     const int *d_n, int shift, uint32_t mask, const int32_t *offs, int nb) {
+                                     const int *d_n, int shift, uint32_t mask, const int32_t *offs,
+                                     const uint32_t *counts, int nb) {
     // The block's keys are first ranked and placed in shared memory in digit order
     // (a block-local stable multisplit), then written out so that consecutive threads
     // write consecutive entries of each digit's run: coalesced global stores.
@@ -416,7 +425,20 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     if (d_n) n = min(n, *d_n);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&wcnt[0][0])[i] = 0;
-    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
+    if (offs) {
+        for (int i = threadIdx.x; i < RADIX; i += blockDim.x) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
+    } else {  // thread d: digit d's count over all blocks and over the blocks before this one
+        static_assert(SORT_THREADS == RADIX, "one thread per digit");
+        const uint32_t *row = counts + (size_t)threadIdx.x * nb;
+        uint32_t tot = 0u, before = 0u;
+        for (int b = 0; b < nb; b++) {
+            const uint32_t c = row[b];
+            tot += c;
+            if (b < (int)blockIdx.x) before += c;
+        }
+        uint32_t all;
+        gbase[threadIdx.x] = block_exclusive_scan<uint32_t>(tot, ws, all) + before;
+    }
     K key[SORT_ITEMS];
     uint32_t val[SORT_ITEMS], rank[SORT_ITEMS];
     int dig[SORT_ITEMS];
@@ -518,9 +540,11 @@ int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch,
         const uint32_t mask = (1u << bits) - 1u;
         radix_hist_kernel<K, ITEMS><<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
                                                                  reinterpret_cast<uint32_t *>(counts), nb);
-        scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<K, ITEMS><<<nb, SORT_THREADS, smem, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n,
-                                                                       d_n, shift, mask, offs, nb);
+        const bool direct = nb <= DIRECT_SORT_BLOCKS;
+        if (!direct) scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
+        radix_scatter_kernel<K, ITEMS><<<nb, SORT_THREADS, smem, st>>>(
+            k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift, mask, direct ? nullptr : offs,
+            reinterpret_cast<const uint32_t *>(counts), nb);
         cur ^= 1;
     }
     return cur;
