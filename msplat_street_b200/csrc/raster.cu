@@ -120,7 +120,11 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
             const float4 A = rec[0], B = rec[1], C = rec[2];
             s0[threadIdx.x] = A;
             s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
-            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
+            // z: the sigma above which alpha = o exp(-sigma) < 1/255 for certain,
+            // ln(255 o) plus a margin far above the roundings of logf, of exp_ref and
+            // of the product, so a pixel past it skips the exponential with the
+            // decision the exact test would take
+            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, logf(255.f * B.y) + 1e-3f, C.w);
             sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
         }
         __syncthreads();
@@ -135,7 +139,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
                 const float4 A = s0[j], B = s1[j], C = s2[j];
                 const float dx = A.x - fpx, dy = A.y - fpy;
                 const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
-                if (sigma < 0.f || sigma >= 5.55f) continue;
+                if (sigma < 0.f || sigma >= 5.55f || sigma > C.z) continue;
                 const float alpha = fminf(0.999f, B.y * exp_ref(-sigma));
                 if (alpha < 1.f / 255.f) continue;
                 const float nT = T * (1.f - alpha);
