@@ -343,7 +343,8 @@ constexpr int RADIX = 256;
 // a block): each digit's run in a block then averages 16 entries, so the scatter's
 // stores come in runs of 64 bytes or more, and the per-block digit counts (256 per
 // block, scanned every pass) stay small next to the keys. Below LARGE_SORT keys, 8
-// items (2048 keys a block) keep enough blocks to fill the GPU.
+// items (2048 keys a block) keep enough blocks to fill the GPU; 64-bit keys always
+// take 8 (16 would need 48 KB of staging per block and halve the resident blocks).
 constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32;
 constexpr int LARGE_SORT = 4 << 20;
 
@@ -352,14 +353,9 @@ constexpr int LARGE_SORT = 4 << 20;
 // separate scan launch over them.
 constexpr int DIRECT_SORT_BLOCKS = 64;
 
-int sort_items(int n) { return n >= LARGE_SORT ? 16 : 8; }
-int radix_blocks(int n) {
-    const int tile = SORT_THREADS * sort_items(n);
-    return (n + tile - 1) / tile;
-}
-// The most blocks any sort of up to n keys uses (scratch sizing: a sort just below
-// LARGE_SORT has more blocks than one just above it).
-int radix_max_blocks(int n) { return std::max(radix_blocks(std::min(n, LARGE_SORT - 1)), radix_blocks(n)); }
+int sort_items(int n, int key_bytes) { return key_bytes == 4 && n >= LARGE_SORT ? 16 : 8; }
+// The most blocks any sort of up to n keys uses (scratch sizing): 2048-key blocks.
+int radix_max_blocks(int n) { return (n + SORT_THREADS * 8 - 1) / (SORT_THREADS * 8); }
 
 // d_n (may be null): a device-side count that caps n (capacity-bounded launches)
 // The lanes of the warp whose digit equals this lane's (d in 0..RADIX, RADIX marking
@@ -517,7 +513,7 @@ size_t radix_scratch_bytes(int n) {
 // count is read on the device (no host round trip; every pass runs).
 template <typename K, int ITEMS>
 int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
-    const int nb = radix_blocks(n);
+    const int nb = (n + SORT_THREADS * ITEMS - 1) / (SORT_THREADS * ITEMS);
     const size_t cnt = (size_t)RADIX * nb;
     int32_t *counts = reinterpret_cast<int32_t *>(scratch);
     int32_t *offs = counts + cnt;
@@ -553,7 +549,7 @@ int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch,
 template <typename K>
 int radix_sort_dispatch(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
     if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
-    return sort_items(n) == 16 ? radix_sort_impl<K, 16>(k, v, n, key_bits, scratch, st, d_n)
+    return sort_items(n, (int)sizeof(K)) == 16 ? radix_sort_impl<K, 16>(k, v, n, key_bits, scratch, st, d_n)
                                : radix_sort_impl<K, 8>(k, v, n, key_bits, scratch, st, d_n);
 }
 
