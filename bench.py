@@ -627,6 +627,12 @@ def launches_per_step(n_isect: float) -> float:
     return 1 + 3 + 1 + passes * 5 + 2 + 1 + 2 + 1 + 1
 
 
+# The rasterizer backward under ncu (--set full, the street step's first timed launch,
+# 1.86 M intersections; profiles/train_step_street_1024x512.md): DRAM bytes read +
+# written per launch and the SM issue activity, the figure that bounds it.
+NCU_RAST_BWD = {"dram_bytes": 16.65e6 + 1.42e6, "isects": 1.86e6, "issue_active": 0.823}
+
+
 def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
     """HBM roofline of the dominant stage by time. Algorithmic bytes per launch:
      proj_sh_bwd_adam: per Gaussian 11 dense params x 3 arrays read + written (264 B)
@@ -652,9 +658,16 @@ def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
     ms = per[dom]
     achieved = algo / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
     peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
-    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-            "avg_ms": ms, "algorithmic_bytes": algo}
+    out = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+           "avg_ms": ms, "algorithmic_bytes": algo}
+    if dom == "rast_bwd":
+        # DRAM traffic per launch scaled from the capture by intersections (the splat
+        # records' re-reads hit L2, so it is well below the algorithmic bytes); the
+        # kernel is bound by instruction issue, not HBM
+        out["traffic"] = NCU_RAST_BWD["dram_bytes"] * isect / NCU_RAST_BWD["isects"]
+        out["issue_active"] = NCU_RAST_BWD["issue_active"]
+    return out
 
 
 PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")
