@@ -128,3 +128,59 @@ def test_one_piece_matches_one_pass():
     assert np.array_equal(a.frame("final_Ts").cpu().numpy(), b.frame("final_Ts").cpu().numpy())
     assert np.array_equal(a.frame("final_idx").cpu().numpy(), b.frame("final_idx").cpu().numpy())
     assert max_abs(img_a, img_b) <= 2.4e-7
+
+
+def _empty_scene():
+    z = np.zeros((0, 3), np.float32)
+    return scenes.Gaussians(z, z, np.zeros((0, 4), np.float32), z, np.zeros((0, 15, 3), np.float32),
+                            np.zeros((0, 1), np.float32))
+
+
+@pytest.mark.parametrize("name", ["empty", "one_pixel", "behind_camera"])
+def test_chunked_edges(oracle, name):
+    """Frames with no work items (an empty scene, every Gaussian behind the camera) and
+    a one-pixel frame, chunked, against the oracle's chunked restatement."""
+    if name == "empty":
+        g, cam = _empty_scene(), scenes.small_camera(64, 48, 80.0)
+    elif name == "one_pixel":
+        g, cam = scenes.random_gaussians(3000, 6, log_scale_mean=-2.0), scenes.small_camera(1, 1, 2.0)
+    else:
+        g = scenes.random_gaussians(500, 5)
+        g.means[:, 2] += 10.0
+        cam = scenes.small_camera(64, 48, 80.0)
+    set_option(oracle, "chunk_size", 64)
+    img_o = oracle.render(g, cam, BACKGROUND)
+    ctx = Context(chunked="on", chunk_len=64)
+    img = ctx.render(GaussianParams.from_numpy(g), cam, BACKGROUND).cpu().numpy()
+    assert max_abs(img, img_o) <= IMAGE_ATOL
+    assert np.array_equal(ctx.frame("chunk_first").cpu().numpy(), oracle.frame("chunk_first"))
+    assert np.array_equal(ctx.frame("final_idx").cpu().numpy(), oracle.frame("final_idx"))
+    if name != "one_pixel":
+        assert ctx.frame("chunk_first").cpu().numpy()[-1] == 0  # no work items
+        assert np.array_equal(img, np.broadcast_to(np.clip(BACKGROUND, 0, 1), img.shape))
+    # and a training step through the chunked backward
+    gt = np.random.default_rng(1).random((cam.height, cam.width, 3)).astype(np.float32)
+    go = g.copy()
+    st = {k: np.zeros(g.n, np.float32) for k in ("vis", "gn", "ms")}
+    loss_o = oracle.train_step(go, cam, BACKGROUND, gt, new_adam_state(go, C1_LRS, 1), st)
+    p = GaussianParams.from_numpy(g)
+    ctx2 = Context(keep_grads=True, chunked="on", chunk_len=64)
+    adam = AdamState.zeros_like(p, C1_LRS)
+    stats = tuple(torch.zeros(g.n, device="cuda") for _ in range(3))
+    loss = ctx2.train_step(p, adam, cam, BACKGROUND, torch.from_numpy(gt).cuda(), stats, sync_loss=True)
+    assert abs(loss - loss_o) <= 1e-6 * max(1.0, abs(loss_o))
+    if g.n:
+        for key in GRADS:
+            got, ref = ctx2.frame(key).cpu().numpy(), oracle.frame(key)
+            if not np.any(ref):
+                assert not np.any(got), key
+            else:
+                assert rel_l2(got, ref) <= GRAD_RTOL_L2, (key, rel_l2(got, ref))
+
+
+def test_chunk_len_bounds():
+    ctx = Context()
+    with pytest.raises(ValueError):
+        ctx.set_chunked("on", chunk_len=8)
+    with pytest.raises(ValueError):
+        ctx.set_chunked("sometimes")
