@@ -346,7 +346,7 @@ def run_ours(args, world, rank, local):
                        "gaussians_end": final_n, "isects_mean": float(np.mean(n_isects)),
                        "l2": "256 MB write between timed steps", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
-            "gpu_launches": int(args.steps * launches_per_step(np.mean(n_isects))),
+            "gpu_launches": int(args.steps * launches_per_step(np.mean(n_isects), final_n)),
             "roofline": roof,
             "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
             "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
@@ -618,13 +618,16 @@ class TargetPrefetch:
         return t
 
 
-def launches_per_step(n_isect: float) -> float:
-    """Kernels one plain training step launches: project + 3 scan + emit +
-    passes x (hist + 3 scan + scatter) + ranges + map + raster fwd + ssim + finalize
-    + raster bwd + backward/Adam."""
+def launches_per_step(n_isect: float, n_gauss: float = 1e5) -> float:
+    """Kernels one plain training step launches: project, depth keys, the depth sort
+    (4 passes of hist + scatter, plus a 3-kernel scan per pass above 131,072
+    Gaussians), tile counts gathered, their 3-kernel scan, offsets scattered, emission,
+    the tile sort (2 passes of hist + 3-kernel scan + scatter for 2048 tiles), ranges,
+    map, raster forward, SSIM, loss finalize, raster backward, backward/Adam."""
     tiles_bits = 11  # 1024x512 -> 2048 tiles
-    passes = (32 + tiles_bits + 7) // 8
-    return 1 + 3 + 1 + passes * 5 + 2 + 1 + 2 + 1 + 1
+    tile_passes = (tiles_bits + 7) // 8
+    depth_sort = 4 * (2 if n_gauss <= 131072 else 5)
+    return 1 + 1 + depth_sort + 1 + 3 + 1 + 1 + tile_passes * 5 + 1 + 1 + 1 + 1 + 1 + 1 + 1
 
 
 # The rasterizer backward under ncu (--set full, the street step's first timed launch,
