@@ -429,7 +429,8 @@ def small_batching_report(views_per_step: int = 8, views: int = 960):
         ctx = Context()
         ds = Dataset.from_setups(setups, [None] * 16, np.zeros((1, 3), np.float32), np.zeros((1, 3), np.uint8),
                                  poses)
-        cfg = TrainingConfig(iterations=100000, warmup_length=10 ** 9)  # no densification in the window
+        # full resolution, no densification in the window
+        cfg = TrainingConfig(iterations=100000, warmup_length=10 ** 9, num_downscales=0)
         tr = GaussianTrainer(ds, cfg, init=GaussianParams.from_numpy(init), context=ctx,
                              views_per_step=views_per_step if batched else 1, batched=batched, graph=graph)
         tr._targets = targets

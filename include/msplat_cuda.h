@@ -70,7 +70,11 @@ int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
  * without a prior, as the Metal backend; 2 = every frame without a prior. Images
  * differ from one pass by what the per-piece stops let through, about 1e-4; the
  * batched entry points always composite in one pass);
- * "chunk_len" (the piece length, 16..2^20, 512 by default as in the Metal backend). */
+ * "chunk_len" (the piece length, 16..2^20, 512 by default as in the Metal backend).
+ * Memory: a chunked frame holds per-piece planes of 36 bytes per tile pixel (9216 B
+ * per piece), for up to intersections / chunk_len + tiles pieces: about 18 B per
+ * intersection at 512, 576 B at 16 -- 10 M intersections at chunk_len 16 take some
+ * 6 GB. */
 int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t value);
 /* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
  * backward round, and the backward reduction's sub-batch. Returns the variant count. */
@@ -258,7 +262,11 @@ int msplat_cuda_radix_sort(msplat_cuda_ctx *ctx, uint64_t *keys, int32_t *vals, 
  * call before any stream capture begins. All calls share the one array, so calls
  * whose work overlaps on the GPU (other streams, other host threads) race and must be
  * serialised by the caller. Work is enqueued on `stream` (a cudaStream_t, NULL = the
- * legacy default stream). */
+ * legacy default stream). The address is kept per device ordinal for the life of the
+ * process: after cudaDeviceReset, or from a driver context other than the device's
+ * primary context, the kept address is stale, so neither is supported. A CUDA error
+ * already pending when the call begins is reported as such (MSPLAT_CUDA_ECUDA, "pending
+ * error") and nothing is enqueued. */
 #define MSPLAT_STATIC_SORT_MAX_KEYS (1u << 20)
 #define MSPLAT_STATIC_SORT_BYTES (13u * 1024u * 1024u + 4096u)
 int msplat_cuda_radix_sort_static(void *stream, uint64_t *keys, int32_t *vals, uint32_t n, int key_bits);

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .camera import CameraSetup
+from .camera import CameraSetup, logf
 from ._lib import check, lib
 
 PARAM_NAMES = ("means", "scales", "quats", "features_dc", "features_rest", "opacities")
@@ -533,11 +533,14 @@ class Context:
         return out
 
     def init_gaussians(self, means: torch.Tensor, rgb: torch.Tensor, seed: int = 42,
-                       opacity_logit: float = float(np.log(0.1 / 0.9)), sh_degree: int = 3) -> GaussianParams:
+                       opacity_logit: Optional[float] = None, sh_degree: int = 3) -> GaussianParams:
         """msplat_init_gaussians + zero SH rest: the Model constructor's start state
-        (core/src/model.cpp:57-71)."""
+        (core/src/model.cpp:57-71). opacity_logit defaults to the constructor's
+        std::log(0.1f / 0.9f) (initial opacity 0.1)."""
         self.bind_stream()
         require_cuda(means, "means")
+        if opacity_logit is None:
+            opacity_logit = float(logf(np.float32(0.1) / np.float32(0.9)))
         n = means.shape[0]
         dev = means.device
         scales = torch.empty((n, 3), dtype=torch.float32, device=dev)

@@ -4,17 +4,69 @@ Restates ``Model::prepareCam`` (core/src/model.cpp:498-546): an OpenGL camera-to
 pose (4x4 row-major, camera looking down -Z with +Y up) becomes the world-to-camera
 ``viewmat`` with the Y/Z axes negated (model.cpp:514-521), the full projection
 ``projmat = P(n=0.001, f=1000) @ viewmat`` (model.cpp:522-525), the camera position,
-and the 16x16 tile grid (model.cpp:538-540). All arithmetic is float32, as in the
-reference.
+and the 16x16 tile grid (model.cpp:538-540), at a resolution-schedule level: the
+level's whole-pixel size (``levelSize``, core/include/image_sizing.hpp:62) and the
+intrinsics scaled by the actual per-axis ratio (model.cpp:500-508). All arithmetic is
+float32 in the reference's order, and the reference's float ``std::atan`` /
+``std::tan`` are the C library's ``atanf`` / ``tanf``, called here through ctypes, so
+the matrices are the reference's bit for bit.
 """
 from __future__ import annotations
 
-import math
+import ctypes
+import ctypes.util
 from dataclasses import dataclass, field
 
 import numpy as np
 
 TILE = 16
+
+
+def _libm():
+    lib = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    for name in ("atanf", "tanf", "logf", "expf"):
+        fn = getattr(lib, name)
+        fn.restype = ctypes.c_float
+        fn.argtypes = [ctypes.c_float]
+    lib.powf.restype = ctypes.c_float
+    lib.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+    return lib
+
+
+LIBM = _libm()
+
+
+def atanf(x) -> np.float32:
+    return np.float32(LIBM.atanf(float(x)))
+
+
+def tanf(x) -> np.float32:
+    return np.float32(LIBM.tanf(float(x)))
+
+
+def logf(x) -> np.float32:
+    return np.float32(LIBM.logf(float(x)))
+
+
+def expf(x) -> np.float32:
+    return np.float32(LIBM.expf(float(x)))
+
+
+def powf(x, y) -> np.float32:
+    return np.float32(LIBM.powf(float(x), float(y)))
+
+
+def level_size(full: int, factor: int) -> int:
+    """levelSize (core/include/image_sizing.hpp:62): a schedule level's pixel size."""
+    return int(full) if factor <= 1 else int(full) // int(factor)
+
+
+def schedule_downscale_factor(step: int, num_downscales: int, resolution_schedule: int) -> int:
+    """scheduleDownscaleFactor (core/src/image_sizing.cpp:129-133): 2^(downscales left)."""
+    if num_downscales <= 0 or resolution_schedule <= 0:
+        return 1
+    remaining = num_downscales - int(step) // int(resolution_schedule)
+    return 1 << min(max(remaining, 0), 30)
 
 
 @dataclass
@@ -58,10 +110,17 @@ def look_at(eye, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
     return c2w.astype(np.float32)
 
 
-def prepare_cam(cam_to_world, width: int, height: int, fx: float, fy: float, cx: float, cy: float) -> CameraSetup:
-    """Model::prepareCam (core/src/model.cpp:498-546) for one full-resolution view."""
+def prepare_cam(cam_to_world, width: int, height: int, fx: float, fy: float, cx: float, cy: float,
+                factor: int = 1) -> CameraSetup:
+    """Model::prepareCam (core/src/model.cpp:498-546) for one view at downscale
+    ``factor`` (1 = full resolution)."""
     d = np.asarray(cam_to_world, np.float32).reshape(4, 4)
     f32 = np.float32
+    w, h = level_size(width, factor), level_size(height, factor)
+    rx = f32(w) / f32(width) if width > 0 else f32(1.0) / f32(factor)
+    ry = f32(h) / f32(height) if height > 0 else f32(1.0) / f32(factor)
+    fx, cx = f32(fx) * rx, f32(cx) * rx
+    fy, cy = f32(fy) * ry, f32(cy) * ry
     R = np.empty((3, 3), np.float32)
     T = np.empty(3, np.float32)
     for i in range(3):
@@ -78,10 +137,10 @@ def prepare_cam(cam_to_world, width: int, height: int, fx: float, fy: float, cx:
          [Rinv[1, 0], Rinv[1, 1], Rinv[1, 2], Tinv[1]],
          [Rinv[2, 0], Rinv[2, 1], Rinv[2, 2], Tinv[2]],
          [0, 0, 0, 1]], np.float32)
-    fov_x = f32(2.0) * f32(math.atan(f32(width) / (f32(2.0) * f32(fx))))
-    fov_y = f32(2.0) * f32(math.atan(f32(height) / (f32(2.0) * f32(fy))))
-    t_p = f32(0.001) * f32(math.tan(f32(0.5) * fov_y))
-    r_p = f32(0.001) * f32(math.tan(f32(0.5) * fov_x))
+    fov_x = f32(2.0) * atanf(f32(w) / (f32(2.0) * fx))
+    fov_y = f32(2.0) * atanf(f32(h) / (f32(2.0) * fy))
+    t_p = f32(0.001) * tanf(f32(0.5) * fov_y)
+    r_p = f32(0.001) * tanf(f32(0.5) * fov_x)
     pm = np.array(
         [[f32(0.001) / r_p, 0, 0, 0],
          [0, f32(0.001) / t_p, 0, 0],
@@ -94,5 +153,5 @@ def prepare_cam(cam_to_world, width: int, height: int, fx: float, fy: float, cx:
             for k in range(4):
                 acc = f32(acc + f32(pm[i, k] * vm[k, j]))
             pvm[i, j] = acc
-    return CameraSetup(int(width), int(height), float(fx), float(fy), float(cx), float(cy), vm, pvm,
+    return CameraSetup(int(w), int(h), float(fx), float(fy), float(cx), float(cy), vm, pvm,
                        T.astype(np.float32).copy())

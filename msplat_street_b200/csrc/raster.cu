@@ -275,7 +275,35 @@ constexpr int PB_STRIDE = 36;  // floats per row: 32 lanes + pad, keeps float4 r
 template <int BB, int SB, int NG = 9>
 constexpr size_t raster_bwd_smem() {
     return sizeof(float4) * 3 * BB + sizeof(float) * BWD_WARPS * BB * NG +
-           sizeof(float) * BWD_WARPS * SB * NG * PB_STRIDE + BB + 16;
+           sizeof(float) * BWD_WARPS * SB * NG * PB_STRIDE + sizeof(uint32_t) * BB + BB + 16;
+}
+
+// One warp's sums of its q (<= SB) pending splats: row o = jj * NG + c of the warp's
+// row buffer holds value c of pending splat jj (the oldest first) for the warp's 32
+// lanes; lane o sums it in lane order with float4 loads and stores the sum to
+// red[warp][j][c], j the splat's staged index (pend: 8 bits per splat, the newest
+// lowest). The lanes that own a splat's value 0 mark the warp in hitw[j].
+template <int NG, int SB>
+__device__ __forceinline__ void bwd_warp_sums(const float *mypb, float *red, uint32_t *hitw, uint32_t pend, int q,
+                                              int warp, int lane, int bb) {
+    __syncwarp();
+    for (int o = lane; o < q * NG; o += 32) {
+        const int jj = o / NG, c = o - jj * NG;
+        const int j = (int)((pend >> (8 * (q - 1 - jj))) & 0xffu);
+        const float4 *row = reinterpret_cast<const float4 *>(mypb + o * PB_STRIDE);
+        float s = 0.f;
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const float4 v = row[r];
+            s += v.x;
+            s += v.y;
+            s += v.z;
+            s += v.w;
+        }
+        red[(warp * bb + j) * NG + c] = s;
+        if (c == 0) atomicOr(&hitw[j], 1u << warp);
+    }
+    __syncwarp();
 }
 
 // One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
@@ -295,7 +323,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
     float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][NG]
     float *pbuf = red + BWD_WARPS * BWD_BATCH * NG;           // [BWD_WARPS][SUB_OUT][PB_STRIDE]
-    uint8_t *sm = reinterpret_cast<uint8_t *>(pbuf + BWD_WARPS * SUB_OUT * PB_STRIDE);  // [BWD_BATCH] warp masks
+    uint32_t *hitw = reinterpret_cast<uint32_t *>(pbuf + BWD_WARPS * SUB_OUT * PB_STRIDE);  // [BWD_BATCH] warps hit
+    uint8_t *sm = reinterpret_cast<uint8_t *>(hitw + BWD_BATCH);  // [BWD_BATCH] warp masks
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -358,16 +387,28 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[b_start + threadIdx.x]);
             const float4 A = rec[0], B = rec[1], C = rec[2];
             sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
+            hitw[threadIdx.x] = 0u;
             s0[threadIdx.x] = A;
             s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
             s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
         }
         __syncthreads();
-        for (int sb = (cnt - 1) / SUB; sb >= 0; sb--) {
-            const int jlo = sb * SUB, jhi = min(cnt - 1, jlo + SUB - 1);
-            unsigned any = 0u;  // bit jj: some lane of this warp touched Gaussian jlo + jj
-            for (int j = jhi; j >= jlo; j--) {
-                if (!((sm[j] >> warp) & 1u)) continue;  // the splat cannot reach this warp's block
+        // This warp's reachable splats, back to front, 32 mask bits per ballot. Splats
+        // that some lane of the warp hits are written to the warp's row buffer (one row
+        // of 32 lane values per gradient value); every SUB of them, the warp's lanes sum
+        // whole rows in lane order (one pass of 27 sums for SUB = 3) into red[warp][j],
+        // and the splat's hitw bit for this warp is set. Warps that miss a splat neither
+        // store nor sum for it, and the block's sum over warps skips them: they would
+        // only add +0.0, which leaves every sum (never -0.0) as it is.
+        int q = 0;          // splats pending in the row buffer (warp-uniform)
+        uint32_t pend = 0;  // their staged indices, 8 bits each, the newest lowest
+        for (int c32 = (cnt - 1) >> 5; c32 >= 0; c32--) {
+            const int jl = (c32 << 5) + lane;
+            uint32_t bits = __ballot_sync(0xffffffffu, jl < cnt && ((sm[jl] >> warp) & 1u));
+            while (bits) {
+                const int hb = 31 - __clz(bits);
+                bits &= ~(1u << hb);
+                const int j = (c32 << 5) + hb;
                 const int k = b_start + j;
                 const float4 A = s0[j], C = s2[j];
                 float g[NG];
@@ -419,9 +460,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                             br = __fmaf_rn(cr, fac, br);
                             bgc = __fmaf_rn(cg, fac, bgc);
                             bb = __fmaf_rn(cb, fac, bb);
-                            if (!signbit(cr)) g[5] = fac * vr;  // raw + 0.5 >= 0
-                            if (!signbit(cg)) g[6] = fac * vg;
-                            if (!signbit(cb)) g[7] = fac * vb;
+                            // colour gradients; a channel whose raw + 0.5 < 0 passes none,
+                            // which the block's sum applies once per splat
+                            g[5] = fac * vr;
+                            g[6] = fac * vg;
+                            g[7] = fac * vb;
                             if (alpha < 0.999f) {
                                 const float vs = -alpha * va;
                                 const float hv = 0.5f * vs;
@@ -436,39 +479,30 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                     }
                 }
                 if (__ballot_sync(0xffffffffu, hit)) {
-                    any |= 1u << (j - jlo);
-                    float *row = mypb + (j - jlo) * NG * PB_STRIDE + lane;
+                    float *row = mypb + q * NG * PB_STRIDE + lane;
 #pragma unroll
                     for (int c = 0; c < NG; c++) row[c * PB_STRIDE] = g[c];
-                }
-            }
-            __syncwarp();
-            // this warp's sums for the sub-batch: output o = jj * 9 + c
-            for (int o = lane; o < SUB_OUT; o += 32) {
-                const int jj = o / NG, c = o - jj * NG;
-                if (jlo + jj > jhi) continue;
-                float s = 0.f;
-                if ((any >> jj) & 1u) {
-                    const float4 *row = reinterpret_cast<const float4 *>(mypb + o * PB_STRIDE);
-#pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        const float4 v = row[q];
-                        s += v.x;
-                        s += v.y;
-                        s += v.z;
-                        s += v.w;
+                    pend = (pend << 8) | (uint32_t)j;
+                    if (++q == SUB) {
+                        bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BWD_BATCH);
+                        q = 0;
                     }
                 }
-                red[(warp * BWD_BATCH + jlo + jj) * NG + c] = s;
             }
-            __syncwarp();
         }
+        if (q) bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BWD_BATCH);
         __syncthreads();
         for (int idx = threadIdx.x; idx < cnt * NG; idx += blockDim.x) {
             const int j = idx / NG, c = idx - j * NG;
+            const uint32_t m = hitw[j];
             float s = 0.f;
 #pragma unroll
-            for (int w = 0; w < BWD_WARPS; w++) s += red[(w * BWD_BATCH + j) * NG + c];
+            for (int w = 0; w < BWD_WARPS; w++)
+                if ((m >> w) & 1u) s += red[(w * BWD_BATCH + j) * NG + c];
+            if (c >= 5 && c <= 7) {  // the staged colour's sign bit: raw + 0.5 < 0 passes no gradient
+                const float col = c == 5 ? s1[j].z : (c == 6 ? s1[j].w : s2[j].x);
+                if (signbit(col)) s = 0.f;
+            }
             if (c < 9) a.slots[(size_t)(b_start + j) * 9 + c] = s;
             else a.slots_depth[b_start + j] = s;
         }

@@ -14,7 +14,8 @@
 // is only a host-side stand-in, not a device address: the entry point looks the real
 // address up with cudaGetSymbolAddress, once per device, on that device's first call
 // (which is why the first call on each device should come before any stream capture
-// begins), and passes that address to the kernels.
+// begins), and passes that address to the kernels. The address is kept per device
+// ordinal, so a device reset or a non-primary driver context is not supported.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -59,8 +60,14 @@ int msplat_cuda_radix_sort_static(void *stream, uint64_t *keys, int32_t *vals, u
     if (radix_scratch_bytes((int)n) > STATIC_RADIX_BYTES)
         return static_fail(MSPLAT_CUDA_ECAPACITY, "msplat_cuda_radix_sort_static: histogram scratch too small");
     if (key_bits > 64) key_bits = 64;
+    // an error left by the caller's own earlier work is not this call's: report it as
+    // pending (without clearing it) and enqueue nothing
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return static_fail(MSPLAT_CUDA_ECUDA, std::string("msplat_cuda_radix_sort_static: pending error before the "
+                                                          "call: ") + cudaGetErrorString(e));
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return static_fail(MSPLAT_CUDA_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= MAX_DEVICES) return static_fail(MSPLAT_CUDA_EINVAL, "device ordinal out of range");
     void *base = nullptr;

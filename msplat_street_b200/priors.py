@@ -23,6 +23,8 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
+from .camera import expf, logf
+
 MAX_PRIOR_DIM = 1024  # core/include/priors.hpp:33
 
 
@@ -199,7 +201,7 @@ def depth_weight_at(opts: PriorOptions, step: int, max_steps: int) -> float:
     t = f(min(max(f(step) / f(max(1, max_steps)), f(0)), f(1)))
     if w1 == 0:
         return float(w0 * (f(1) - t))
-    return float(f(math.exp(float(f(math.log(w0)) * (f(1) - t) + f(math.log(w1)) * t))))
+    return float(expf(logf(w0) * (f(1) - t) + logf(w1) * t))
 
 
 def compute_sky_frame(cam_to_worlds: Sequence[np.ndarray]) -> np.ndarray:

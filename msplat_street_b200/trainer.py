@@ -3,12 +3,19 @@
 Restates core/src/model.cpp's training-side host code over the C-ABI:
  * capacity-backed parameter and Adam buffers with views of the active rows
    (setupOptimizers / refreshViews / ensureCapacity, model.cpp:81-193);
- * per-group learning rates and the log-linear means decay (model.cpp:100, :140-143);
+ * per-group learning rates and the log-linear means decay (model.cpp:100, :140-143),
+   in float32 with the C library's logf / expf as the reference evaluates it;
  * Adam bias correction per step (fullIteration, :638-651);
  * the densification schedule (afterTrain, :199-245): every refine_every steps after
    the warm-up, densify while step < iterations / 2 and the reset-interval rule holds,
-   reset opacities on the reset interval, clear the statistics;
+   reset opacities on the reset interval, clear the statistics (after_train_plan);
+ * the resolution schedule: step s trains at downscale 2^max(num_downscales -
+   s // resolution_schedule, 0) (image_sizing.cpp:129-133) on the target's area-
+   downsampled pyramid level (Camera::getGPUImage, input_data.cpp:56-69);
  * SH degree ramp degrees_to_use = min(step // sh_degree_interval, sh_degree) (:535).
+Steps are numbered from 1 as GaussianTrainer::step numbers them
+(python/bindings.cpp:261-274): step s prepares its camera, trains, decays the means
+learning rate and runs the densification schedule, all with s.
 The camera set-up (prepareCam) is msplat_street_b200.camera.prepare_cam. The public
 surface mirrors the reference's TrainingConfig / TrainingStats / GaussianTrainer
 (python/msplat/_core.pyi:157-267) for in-memory datasets. Prior-guided training
@@ -29,7 +36,7 @@ import torch
 from . import formats
 from . import priors as _priors
 from .backend import AdamState, Context, GaussianParams, PriorStep
-from .camera import CameraSetup, prepare_cam
+from .camera import CameraSetup, expf, logf, powf, prepare_cam, schedule_downscale_factor
 
 LR_INIT = (0.00016, 0.005, 0.001, 0.0025, 0.000125, 0.05)  # model.cpp:100
 MEANS_LR_FINAL = 0.0000016                                   # model.cpp:111
@@ -44,6 +51,8 @@ class TrainingConfig:
     sh_degree: int = 3
     sh_degree_interval: int = 1000
     ssim_weight: float = 0.2
+    num_downscales: int = 2
+    resolution_schedule: int = 3000
     refine_every: int = 100
     warmup_length: int = 500
     reset_alpha_every: int = 30
@@ -68,6 +77,55 @@ class TrainingStats:
     ms_per_step: float
 
 
+def sh_degrees_to_use(step: int, cfg: TrainingConfig) -> int:
+    """Model::prepareCam's degreesToUse = min(step / shDegreeInterval, shDegree)
+    (core/src/model.cpp:535)."""
+    return min(step // max(cfg.sh_degree_interval, 1), cfg.sh_degree)
+
+
+def means_lr(step: int, iterations: int) -> float:
+    """Model::schedulersStep (core/src/model.cpp:140-143): the means learning rate after
+    step ``step``, log-linear from 1.6e-4 to 1.6e-6 over the run, in float32 with the C
+    library's logf / expf (the reference's std::log / std::exp on floats)."""
+    f = np.float32
+    t = min(max(f(step) / f(max(iterations, 1)), f(0.0)), f(1.0))
+    return float(expf(logf(f(LR_INIT[0])) * (f(1.0) - t) + logf(f(MEANS_LR_FINAL)) * t))
+
+
+@dataclass
+class AfterTrainPlan:
+    """What Model::afterTrain (core/src/model.cpp:199-245) does after step ``step``:
+    densify (with these arguments) and / or reset opacities; the statistics are cleared
+    whenever a plan exists."""
+
+    step: int
+    densify: bool
+    reset: bool
+    check_screen: bool
+    check_huge: bool
+    half_max_dim: float
+    seed: int
+
+
+def after_train_plan(step: int, cfg: TrainingConfig, num_cameras: int, last_width: int,
+                     last_height: int) -> Optional[AfterTrainPlan]:
+    """None on steps that are not refinement steps (step % refine_every != 0 or within
+    the warm-up); else the plan. ``last_width`` / ``last_height``: the size the step
+    trained at (its resolution-schedule level), as Model::lastWidth / lastHeight."""
+    if not (step % cfg.refine_every == 0 and step > cfg.warmup_length):
+        return None
+    reset_interval = cfg.reset_alpha_every * cfg.refine_every
+    stop_split_at = cfg.iterations // 2
+    return AfterTrainPlan(
+        step=step,
+        densify=step < stop_split_at and step % reset_interval > num_cameras + cfg.refine_every,
+        reset=step < stop_split_at and step % reset_interval == cfg.refine_every,
+        check_screen=step < cfg.stop_screen_size_at,
+        check_huge=step > cfg.refine_every * cfg.reset_alpha_every,
+        half_max_dim=float(np.float32(0.5) * np.float32(max(last_width, last_height))),
+        seed=(step * 2654435761) & 0xFFFFFFFF)
+
+
 @dataclass
 class View:
     """One training camera: its pose, intrinsics and target image."""
@@ -84,6 +142,16 @@ class View:
 
     def __post_init__(self):
         self.setup = prepare_cam(self.cam_to_world, self.width, self.height, self.fx, self.fy, self.cx, self.cy)
+        self._levels = {1: self.setup}
+
+    def setup_at(self, factor: int) -> CameraSetup:
+        """The camera at a resolution-schedule level (Model::prepareCam at downscale
+        ``factor``)."""
+        s = self._levels.get(factor)
+        if s is None:
+            s = prepare_cam(self.cam_to_world, self.width, self.height, self.fx, self.fy, self.cx, self.cy, factor)
+            self._levels[factor] = s
+        return s
 
 
 class Dataset:
@@ -122,7 +190,8 @@ class GaussianTrainer:
         if init is None:
             pts = torch.from_numpy(dataset.points).to(device)
             init = self.ctx.init_gaussians(pts, torch.from_numpy(dataset.colors), seed=42,
-                                           opacity_logit=math.log(0.1 / 0.9), sh_degree=config.sh_degree)
+                                           opacity_logit=float(logf(np.float32(0.1) / np.float32(0.9))),
+                                           sh_degree=config.sh_degree)
         self.lrs = list(config.lrs) if config.lrs is not None else list(LR_INIT)
         self._setup_buffers(init)
         self.current_step = 0
@@ -135,7 +204,10 @@ class GaussianTrainer:
         self.stats = None
         self.last_loss = None
         self.radii_ready = False
-        self.max_dim = max(max(v.width, v.height) for v in dataset.views) if dataset.views else 1
+        # the size the last step trained at (Model::lastWidth / lastHeight)
+        self.last_width = dataset.views[0].width if dataset.views else 1
+        self.last_height = dataset.views[0].height if dataset.views else 1
+        self.last_views: List[int] = []  # the views the last step trained on
         # prior-guided training (configure_priors)
         self.prior_opts: Optional[_priors.PriorOptions] = None
         self.cam_priors: List[Optional[_priors.CameraPrior]] = [None] * len(dataset.views)
@@ -143,6 +215,34 @@ class GaussianTrainer:
         self.sky: Optional[dict] = None
         self.exposure: Optional[dict] = None
         self.prior_loss_terms: Optional[torch.Tensor] = None
+
+    # -- targets and their resolution-schedule levels ---------------------------------
+    @property
+    def _targets(self) -> List[Optional[torch.Tensor]]:
+        return self._full_targets
+
+    @_targets.setter
+    def _targets(self, targets) -> None:
+        self._full_targets = list(targets)
+        self._pyramid = {}
+
+    def target_at(self, ci: int, factor: int) -> Optional[torch.Tensor]:
+        """View ci's target at downscale ``factor``: the full image area-downsampled to
+        the level's size on the GPU and kept (Camera::getGPUImage, input_data.cpp:56-69)."""
+        full = self._full_targets[ci]
+        if full is None or factor <= 1:
+            return full
+        key = (ci, factor)
+        t = self._pyramid.get(key)
+        if t is None:
+            s = self.ds.views[ci].setup_at(factor)
+            t = self.ctx.resize_area(full, s.width, s.height)
+            self._pyramid[key] = t
+        return t
+
+    def downscale_factor(self, step: int) -> int:
+        """Model::getDownscaleFactor (model.cpp:195-197)."""
+        return schedule_downscale_factor(step, self.cfg.num_downscales, self.cfg.resolution_schedule)
 
     # -- capacity buffers (model.cpp:81-193) ------------------------------------------
     def _setup_buffers(self, p: GaussianParams):
@@ -192,35 +292,30 @@ class GaussianTrainer:
         return int(self._order.pop())
 
     def degrees_to_use(self, step: Optional[int] = None) -> int:
-        s = self.current_step if step is None else step
-        return min(s // max(self.cfg.sh_degree_interval, 1), self.cfg.sh_degree)
+        """SH degrees used at ``step`` (default: the last step taken)."""
+        return sh_degrees_to_use(self.current_step if step is None else step, self.cfg)
 
     def _schedulers_step(self, step: int) -> None:
         """Log-linear means LR decay (model.cpp:140-143)."""
-        t = min(max(step / max(self.cfg.iterations, 1), 0.0), 1.0)
-        self.lrs[0] = float(np.float32(math.exp(math.log(LR_INIT[0]) * (1 - t) + math.log(MEANS_LR_FINAL) * t)))
+        self.lrs[0] = means_lr(step, self.cfg.iterations)
 
     def _after_train(self, step: int) -> None:
         """Model::afterTrain (model.cpp:199-245)."""
         c = self.cfg
-        if not (step % c.refine_every == 0 and step > c.warmup_length):
+        plan = after_train_plan(step, c, len(self.ds.views), self.last_width, self.last_height)
+        if plan is None:
             return
-        reset_interval = c.reset_alpha_every * c.refine_every
-        stop_split_at = c.iterations // 2
-        do_dens = step < stop_split_at and step % reset_interval > len(self.ds.views) + c.refine_every
-        if do_dens and self.stats is not None:
+        if plan.densify and self.stats is not None:
             # a Gaussian may be both split and cloned: up to 4 N rows (the reference
             # reserves 3 N, model.cpp:158-193)
             self.ensure_capacity(4 * self.num_active)
             gn, vc, ms = self.stats[1], self.stats[0], self.stats[2]
             self.num_active = self.ctx.densify(
-                self.num_active, self.buf, self.m1, self.m2, gn, vc, ms, 0.5 * self.max_dim,
-                (step * 2654435761) & 0xFFFFFFFF, grad_thresh=c.densify_grad_thresh,
-                size_thresh=c.densify_size_thresh, screen_thresh=c.split_screen_size,
-                check_screen=step < c.stop_screen_size_at, cull_alpha=c.cull_alpha_thresh,
-                cull_scale=c.cull_scale_thresh, cull_screen=c.cull_screen_size,
-                check_huge=step > c.refine_every * c.reset_alpha_every)
-        if step < stop_split_at and step % reset_interval == c.refine_every:
+                self.num_active, self.buf, self.m1, self.m2, gn, vc, ms, plan.half_max_dim, plan.seed,
+                grad_thresh=c.densify_grad_thresh, size_thresh=c.densify_size_thresh,
+                screen_thresh=c.split_screen_size, check_screen=plan.check_screen, cull_alpha=c.cull_alpha_thresh,
+                cull_scale=c.cull_scale_thresh, cull_screen=c.cull_screen_size, check_huge=plan.check_huge)
+        if plan.reset:
             n = self.num_active
             self.ctx.opacity_reset(self.buf[5][:n], self.m1[5][:n], self.m2[5][:n], n, RESET_LOGIT)
         self.stats = None
@@ -286,8 +381,8 @@ class GaussianTrainer:
         ps.aux = ps.aux or depth_w > 0 or sky_terms or masks
 
         def bias(lr, t):
-            return float(f(lr) / (f(1) - np.power(f(adam.beta1), f(t)))), float(
-                np.sqrt(f(1) - np.power(f(adam.beta2), f(t))))
+            # std::pow(float, float) is the C library's powf (model.cpp:591-592, :618-619)
+            return float(f(lr) / (f(1) - powf(adam.beta1, f(t)))), float(np.sqrt(f(1) - powf(adam.beta2, f(t))))
 
         if ps.sky:
             self.sky["steps"] += 1
@@ -314,7 +409,7 @@ class GaussianTrainer:
             ps.expo_step_size, ps.expo_bc2_sqrt = bias(o.exposure_lr, e["steps"][ci])
             ps.expo_reg = o.exposure_reg
         if o.max_scale_ratio > 1.0:
-            ps.log_max_scale_ratio = float(f(math.log(f(o.max_scale_ratio))))
+            ps.log_max_scale_ratio = float(logf(o.max_scale_ratio))
         return ps
 
     def prior_losses(self) -> dict:
@@ -348,6 +443,9 @@ class GaussianTrainer:
     def step(self, sync_loss: bool = False, target: Optional[torch.Tensor] = None) -> TrainingStats:
         """One training iteration (GaussianTrainer::step, python/bindings.cpp:261-284)."""
         t0 = time.perf_counter()
+        step = self.current_step + 1  # GaussianTrainer::step numbers steps from 1
+        factor = self.downscale_factor(step)
+        dtu = self.degrees_to_use(step)
         n = self.num_active
         if self.stats is None:
             self.stats = tuple(torch.zeros(n, dtype=torch.float32, device=self.device) for _ in range(3))
@@ -358,31 +456,36 @@ class GaussianTrainer:
             if self._priors_active():
                 raise ValueError("prior-guided training runs one view per step")
             self.ctx.set_prior(None)
-            views = []
+            views, picked = [], []
             for _ in range(self.views_per_step):
                 ci = self._next_camera()
-                if self._targets[ci] is None:
+                picked.append(ci)
+                gt = self.target_at(ci, factor)
+                if gt is None:
                     raise ValueError(f"view {ci} has no target image")
-                views.append((self.ds.views[ci].setup, self._targets[ci]))
+                views.append((self.ds.views[ci].setup_at(factor), gt))
             losses = self.ctx.train_batch(self.params, adam, views, self.bg, self.stats,
-                                          ssim_weight=self.cfg.ssim_weight, degrees_to_use=self.degrees_to_use(),
-                                          sync_loss=sync_loss)
+                                          ssim_weight=self.cfg.ssim_weight, degrees_to_use=dtu, sync_loss=sync_loss)
             self.last_loss = float(np.mean(losses)) if losses is not None else None
+            last = views[-1][0]
         else:
             ci = self._next_camera()
-            view = self.ds.views[ci]
-            gt = target if target is not None else self._targets[ci]
+            picked = [ci]
+            last = self.ds.views[ci].setup_at(factor)
+            gt = target if target is not None else self.target_at(ci, factor)
             if gt is None:
                 raise ValueError(f"view {ci} has no target image")
-            self.ctx.set_prior(self._train_prior(ci, self.current_step + 1, adam) if self._priors_active() else None)
-            self.last_loss = self.ctx.train_step(self.params, adam, view.setup, self.bg, gt, self.stats,
-                                                 ssim_weight=self.cfg.ssim_weight,
-                                                 degrees_to_use=self.degrees_to_use(), sync_loss=sync_loss)
+            self.ctx.set_prior(self._train_prior(ci, step, adam) if self._priors_active() else None)
+            self.last_loss = self.ctx.train_step(self.params, adam, last, self.bg, gt, self.stats,
+                                                 ssim_weight=self.cfg.ssim_weight, degrees_to_use=dtu,
+                                                 sync_loss=sync_loss)
+        self.last_width, self.last_height = last.width, last.height
+        self.last_views = picked
         self.adam_step = adam.step
-        self.current_step += 1
-        self._schedulers_step(self.current_step)
-        self._after_train(self.current_step)
-        return TrainingStats(self.current_step, self.num_active, (time.perf_counter() - t0) * 1e3)
+        self.current_step = step
+        self._schedulers_step(step)
+        self._after_train(step)
+        return TrainingStats(step, self.num_active, (time.perf_counter() - t0) * 1e3)
 
     def train(self, callback: Optional[Callable[[TrainingStats], None]] = None, callback_every: int = 100) -> None:
         while self.current_step < self.cfg.iterations:

@@ -7,7 +7,8 @@ scene in a 20 x 4 x 20 m box, 16 target renders at 1024 x 512 from cameras on a
 3-NN mean distance. Densify every 100 steps from step 500 (warm-up 400, so step 500
 is the first refinement), split/clone above a view-space gradient of 2e-4, prune
 below opacity 0.005; iterations 2000 (so refinement stops at step 1000, the
-reference's iterations / 2 rule).
+reference's iterations / 2 rule). Every step trains at the full 1024 x 512 (no
+resolution schedule: num_downscales 0).
 """
 from __future__ import annotations
 
@@ -27,7 +28,8 @@ BACKGROUND = np.array([0.6130, 0.0101, 0.3984], np.float32)
 
 def street_config(iterations: int = 2000) -> TrainingConfig:
     return TrainingConfig(iterations=iterations, sh_degree=3, sh_degree_interval=1000, ssim_weight=0.2,
-                          refine_every=100, warmup_length=400, densify_grad_thresh=2e-4, cull_alpha_thresh=0.005)
+                          num_downscales=0, refine_every=100, warmup_length=400, densify_grad_thresh=2e-4,
+                          cull_alpha_thresh=0.005)
 
 
 def street_views(gt_n: int = STREET_GT_N):

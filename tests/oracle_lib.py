@@ -22,6 +22,7 @@ PATHS = {
     "reference_fast": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_fast.so"),
     "reference_formats": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_formats.so"),
     "reference_priors": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_priors.so"),
+    "reference_model": os.path.join(ORACLE_DIR, "_ref", "libmsplat_ref_model.so"),
 }
 
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")

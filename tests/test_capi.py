@@ -59,7 +59,8 @@ def test_argument_errors_are_status_codes():
     lib.msplat_cuda_ctx_destroy(ctx)
 
 
-REF = os.environ.get("MSPLAT_REFERENCE_ROOT", "/root/reference")
+# the reference checkout: MSPLAT_REFERENCE_ROOT, else a `reference` directory beside the repository
+REF = os.environ.get("MSPLAT_REFERENCE_ROOT", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "core", "metal", "bindings.h")),

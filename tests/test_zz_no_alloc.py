@@ -64,6 +64,26 @@ def test_static_sort_matches_context_sort_on_two_calls(n, bits, hi):
         np.testing.assert_array_equal(got_v, np.argsort(keys & mask, kind="stable"), err_msg=f"call {call}")
 
 
+def test_static_sort_allocates_no_device_memory():
+    """After a first call (which looks up the array's address), a 2^20-key sort leaves
+    the device's free memory where it was; the context sort of the same keys grows
+    about 13 MB of scratch in its context."""
+    n = MAX_KEYS
+    keys = np.random.default_rng(1).integers(0, 2 ** 63, n, dtype=np.uint64)
+    k = torch.from_numpy(keys.view(np.int64)).cuda()
+    v = torch.arange(n, dtype=torch.int32, device="cuda")
+    lib = _lib.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(lib.msplat_cuda_radix_sort_static(st, C.c_void_p(k.data_ptr()), C.c_void_p(v.data_ptr()), n, 64))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        _lib.check(lib.msplat_cuda_radix_sort_static(st, C.c_void_p(k.data_ptr()), C.c_void_p(v.data_ptr()), n, 64))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_static_sort_refuses_more_keys_than_its_array_holds():
     lib = _lib.lib()
     n = MAX_KEYS + 1
