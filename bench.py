@@ -229,16 +229,22 @@ def run_ours(args, world, rank, local):
     ctx.enable_stage_timing(True)
     ctx.drain_stage_times()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    n_isects = []
+    n_isects, pairs, n_gauss = [], [], []
+    window = {"first": trainer.iteration + 1, "sh_first": trainer.degrees_to_use(trainer.iteration + 1),
+              "gaussians_first": trainer.splat_count, "densify": []}
     barrier(world, dev)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         for i in range(args.steps):
             flush.zero_()
+            n_gauss.append(trainer.splat_count)
             evs[i][0].record()
-            trainer.step()
+            st = trainer.step()
             evs[i][1].record()
             n_isects.append(ctx.num_isects())
+            pairs.append(ctx.pair_counts())  # outside the events: a counting kernel and a readback
+            if st.splat_count != n_gauss[-1]:
+                window["densify"].append(st.iteration)
         torch.cuda.synchronize()
     barrier(world, dev)
     step_ms = [a.elapsed_time(b) for a, b in evs]
@@ -247,14 +253,26 @@ def run_ours(args, world, rank, local):
     ctx.enable_stage_timing(False)
     final_n = trainer.splat_count
     value = world * args.steps / (total_ms / 1e3)
+    window.update(last=trainer.iteration, sh_last=trainer.degrees_to_use(), gaussians_last=final_n)
+    timed_window = (f"iterations {window['first']}..{window['last']} of the 2000-iteration schedule: SH degree "
+                    f"{window['sh_first']}..{window['sh_last']}, {window['gaussians_first']}..{window['gaussians_last']}"
+                    f" Gaussians, densify steps {window['densify'] or 'none'}")
 
     if args.quick:  # device pass only (profiling runs)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "quick": True,
+                              "timed_window": timed_window,
                               "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
-                              "isects_mean": float(np.mean(n_isects))}))
+                              "isects_mean": float(np.mean(n_isects)),
+                              "pairs_mean": [float(np.mean([p[0] for p in pairs])),
+                                             float(np.mean([p[1] for p in pairs]))]}))
         return
+
+    # ---- the rest of the schedule: 20-step windows spread over it (rank 0 times them
+    # on the same trainer, densification steps included) ----
+    sched = schedule_sample(trainer, ctx, flush, dev) if rank == 0 else None
+    knn = knn_rate(trainer, ctx) if rank == 0 else None
 
     # ---- end-to-end pass through the public API: host targets, loss read back ----
     ctx2 = Context()
@@ -291,7 +309,11 @@ def run_ours(args, world, rank, local):
 
     # ---- roofline of the dominant stage (live CUDA-event durations) ----
     peaks, peak_kind = measured_peaks()
-    roof = roofline(stages, n_isects, final_n, peaks, peak_kind)
+    ck = clocks.summary()
+    roof = roofline(stages, n_isects, float(np.mean(n_gauss)), peaks, peak_kind, pairs, ck.get("sm_mhz"))
+    thr = throughput(stages, n_isects, float(np.mean(n_gauss)), pairs, peaks, peak_kind, ck.get("sm_mhz"))
+    if knn:
+        thr["knn"] = knn
 
     # ---- differentiable path: recomputed vs stored transmittance (rank 0) ----
     diff = None
@@ -337,17 +359,18 @@ def run_ours(args, world, rank, local):
                    "sample": f"unavailable: {e}"}
 
     if rank == 0:
-        ck = clocks.summary()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "timed_window": f"iterations {args.warmup + 1}..{total_steps}",
+            "config": {"workload": WORKLOAD, "timed_window": timed_window,
                        "gaussians_end": final_n, "isects_mean": float(np.mean(n_isects)),
                        "l2": "256 MB write between timed steps", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
             "gpu_launches": int(args.steps * launches_per_step(np.mean(n_isects), final_n)),
             "roofline": roof,
+            "throughput": thr,
+            "schedule_sample": sched,
             "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
             "clocks": {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")},
             "cpu_baseline": cpu,
@@ -631,34 +654,60 @@ def launches_per_step(n_isect: float, n_gauss: float = 1e5) -> float:
     return 1 + 1 + depth_sort + 1 + 3 + 1 + 1 + tile_passes * 5 + 1 + 1 + 1 + 1 + 1 + 1 + 1
 
 
-# The rasterizer backward under ncu (--set full, the street step's first timed launch,
-# 1.86 M intersections; profiles/train_step_street_1024x512.md): DRAM bytes read +
-# written per launch and the SM issue activity, the figure that bounds it.
-NCU_RAST_BWD = {"dram_bytes": 16.65e6 + 1.42e6, "isects": 1.86e6, "issue_active": 0.823}
+# DRAM bytes read + written by one launch of the rasterizer backward, from an ncu
+# capture of the street step's first timed launch (1.86 M intersections), and the
+# intersections it processed; the run scales it by its own intersections.
+NCU_RAST_BWD = {"dram_bytes": 16.65e6 + 1.42e6, "isects": 1.86e6}
+
+SM_COUNT, FP32_LANES = 148, 128
+NPIX = 1024 * 512
+# FP32 operations per evaluated (pixel, Gaussian) pair: forward sigma, alpha and the
+# colour / transmittance update; backward recovery, v_alpha, the sigma, conic, xy,
+# colour and opacity gradients
+FWD_OPS_PER_PAIR, BWD_OPS_PER_PAIR = 20.0, 50.0
 
 
-def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
-    """HBM roofline of the dominant stage by time. Algorithmic bytes per launch:
-     proj_sh_bwd_adam: per Gaussian 11 dense params x 3 arrays read + written (264 B)
-       + visible SH 48 x 3 x 2 (1152 B) + slots 36 B per intersection read;
-     rast_fwd: splat records 48 B + id 4 B per intersection + 20 B per pixel written;
-     rast_bwd: 48 + 4 B per intersection read + 36 B slot written + 32 B per pixel;
+def stage_bytes(n_isects: float, n_gauss: float) -> dict:
+    """Algorithmic bytes per step of each stage (each input read once, each output
+    written once):
+     proj_sh_fwd: 236 B of parameters read + 48 B splat record, radius, box, tile
+       count (76 B) written per Gaussian;
+     bin_sort: key emission 12 B per intersection, the tile sort's passes 24 B per
+       intersection per pass (2 passes for 2048 tiles), ranges and map 8 + 8 B;
+     rast_fwd: splat record 48 B + id 4 B per intersection, 20 B per pixel written;
      loss_fwd_bwd: 36 B per pixel (render + target read, gradient written);
-     bin_sort: 8 passes-worth of key/value traffic, 32 B per intersection per pass."""
+     rast_bwd: 48 + 4 B per intersection read + 36 B slot written, 32 B per pixel read;
+     proj_sh_bwd_adam: per Gaussian 11 dense parameters x 3 arrays read + written
+       (264 B) + SH 48 x 3 x 2 (1152 B), 36 B slot per intersection read."""
+    return {
+        "proj_sh_fwd": n_gauss * (236 + 76),
+        "bin_sort": n_isects * (12 + 2 * 24 + 16),
+        "rast_fwd": n_isects * 52 + NPIX * 20,
+        "loss_fwd_bwd": NPIX * 36,
+        "rast_bwd": n_isects * 88 + NPIX * 32,
+        "proj_sh_bwd_adam": n_gauss * (264 + 1152) + n_isects * 36,
+    }
+
+
+def fp32_peak_gflops(sm_mhz) -> float:
+    """148 SMs x 128 FP32 lanes x 2 (a fused multiply-add) x the sampled SM clock."""
+    mhz = float(sm_mhz) if sm_mhz else 1965.0
+    return SM_COUNT * FP32_LANES * 2 * mhz * 1e6 / 1e9
+
+
+def roofline(stages, n_isects, n_gauss, peaks, peak_kind, pairs=None, sm_mhz=None):
+    """The dominant stage by time against the measured HBM copy bandwidth, with its
+    algorithmic bytes (stage_bytes) over its live CUDA-event duration. For the
+    rasterizers, which are bound by instruction issue rather than HBM, `compute` adds
+    the FP32 fraction: the reference loops' (pixel, Gaussian) pairs (counted on the
+    device each step) x the operations per pair over the FP32 peak at the sampled
+    clock."""
     if not stages:
         return None
     per = {k: v[0] / max(v[1], 1) for k, v in stages.items()}
     dom = max(per, key=per.get)
     isect = float(np.mean(n_isects)) if n_isects else 0.0
-    npix = 1024 * 512
-    algo = {
-        "proj_sh_bwd_adam": n_gauss * (264 + 1152) + isect * 40,
-        "rast_fwd": isect * 52 + npix * 20,
-        "rast_bwd": isect * 88 + npix * 32,
-        "loss_fwd_bwd": npix * 36,
-        "bin_sort": isect * 32 * 6 + isect * 24,
-        "proj_sh_fwd": n_gauss * (236 + 76),
-    }.get(dom, 0.0)
+    algo = stage_bytes(isect, n_gauss).get(dom, 0.0)
     ms = per[dom]
     achieved = algo / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
     peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
@@ -666,12 +715,107 @@ def roofline(stages, n_isects, n_gauss, peaks, peak_kind):
            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
            "avg_ms": ms, "algorithmic_bytes": algo}
     if dom == "rast_bwd":
-        # DRAM traffic per launch scaled from the capture by intersections (the splat
-        # records' re-reads hit L2, so it is well below the algorithmic bytes); the
-        # kernel is bound by instruction issue, not HBM
+        # the splat records' re-reads hit L2, so DRAM traffic is well below the
+        # algorithmic bytes
         out["traffic"] = NCU_RAST_BWD["dram_bytes"] * isect / NCU_RAST_BWD["isects"]
-        out["issue_active"] = NCU_RAST_BWD["issue_active"]
+        out["traffic_source"] = "ncu capture of one launch (street step, 1.86 M intersections), scaled by intersections"
+    if dom in ("rast_fwd", "rast_bwd") and pairs:
+        k = 0 if dom == "rast_fwd" else 1
+        ops = FWD_OPS_PER_PAIR if dom == "rast_fwd" else BWD_OPS_PER_PAIR
+        gflops = float(np.mean([p[k] for p in pairs])) * ops / (ms * 1e-3) / 1e9
+        pk = fp32_peak_gflops(sm_mhz)
+        out["compute"] = {"bound": "fp32 issue", "achieved": gflops, "peak": pk, "unit": "GFLOP/s",
+                          "frac": gflops / pk, "ops_per_pair": ops,
+                          "peak_source": "computed: 148 SMs x 128 lanes x 2 x sampled SM clock"}
     return out
+
+
+def throughput(stages, n_isects, n_gauss, pairs, peaks, peak_kind, sm_mhz) -> dict:
+    """Per-stage rates of the timed window in the units of the path: Gaussians/s
+    projected, Mpix/s composited, (pixel, Gaussian) pairs/s and the FP32 fraction of the
+    rasterizers, and every stage's algorithmic HBM GB/s against the measured peak."""
+    per = {k: v[0] / max(v[1], 1) for k, v in stages.items()}
+    isect = float(np.mean(n_isects)) if n_isects else 0.0
+    peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
+    fwd_pairs = float(np.mean([p[0] for p in pairs])) if pairs else 0.0
+    bwd_pairs = float(np.mean([p[1] for p in pairs])) if pairs else 0.0
+    pk = fp32_peak_gflops(sm_mhz)
+    out = {"gaussians": n_gauss, "isects": isect, "pairs_fwd": fwd_pairs, "pairs_bwd": bwd_pairs,
+           "fp32_peak_gflops": pk, "hbm_peak_gbs": peak, "peak_source": peak_kind}
+    if per.get("proj_sh_fwd"):
+        out["gaussians_per_s_projected"] = n_gauss / (per["proj_sh_fwd"] * 1e-3)
+    if per.get("rast_fwd"):
+        t = per["rast_fwd"] * 1e-3
+        out["mpix_per_s_composited"] = NPIX / t / 1e6
+        out["pairs_per_s_fwd"] = fwd_pairs / t
+        out["fp32_frac_fwd"] = fwd_pairs * FWD_OPS_PER_PAIR / t / 1e9 / pk
+    if per.get("rast_bwd"):
+        t = per["rast_bwd"] * 1e-3
+        out["pairs_per_s_bwd"] = bwd_pairs / t
+        out["fp32_frac_bwd"] = bwd_pairs * BWD_OPS_PER_PAIR / t / 1e9 / pk
+    hbm = {}
+    for k, b in stage_bytes(isect, n_gauss).items():
+        if per.get(k):
+            gbs = b / (per[k] * 1e-3) / 1e9
+            hbm[k] = {"ms": per[k], "bytes": b, "gbs": gbs, "frac": gbs / peak}
+    out["hbm"] = hbm
+    return out
+
+
+SCHEDULE_WINDOWS = ((500, 519), (1000, 1019), (1500, 1519), (1980, 1999))
+
+
+def schedule_sample(trainer, ctx, flush, dev, windows=SCHEDULE_WINDOWS) -> list:
+    """Continues the timed trainer through the schedule and times 20-step windows at
+    its landmarks -- the first densification (step 500), the last (1000, where
+    refinement stops and SH degree 1 begins), mid-run and the end -- each step
+    device-timed with CUDA events like the headline window, L2 flushed between
+    steps."""
+    import torch
+    out = []
+    for a, b in windows:
+        if trainer.iteration >= a or b > trainer.cfg.iterations:
+            continue
+        while trainer.iteration < a - 1:
+            trainer.step()
+        torch.cuda.synchronize()
+        n0, dens, ms, isects = trainer.splat_count, [], [], []
+        for _ in range(b - a + 1):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            before = trainer.splat_count
+            e0.record()
+            st = trainer.step()
+            e1.record()
+            isects.append(ctx.num_isects())
+            if st.splat_count != before:
+                dens.append(st.iteration)
+            ms.append((e0, e1))
+        torch.cuda.synchronize()
+        t = sum(x.elapsed_time(y) for x, y in ms)
+        out.append({"iterations": [a, b], "ms_per_step": t / len(ms), "iters_per_s": len(ms) / (t / 1e3),
+                    "gaussians": [n0, trainer.splat_count], "sh_degree": trainer.degrees_to_use(),
+                    "densify_steps": dens, "isects_mean": float(np.mean(isects))})
+    return out
+
+
+def knn_rate(trainer, ctx, reps: int = 5) -> dict:
+    """Exact 3-NN mean distance (the scale init) over the workload's initial point
+    cloud: points/s, CUDA events around each call."""
+    import torch
+    pts = torch.from_numpy(trainer.ds.points).cuda()
+    ctx.knn3_mean_dist(pts)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.knn3_mean_dist(pts)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = statistics.median(ts)
+    return {"points": int(pts.shape[0]), "ms": ms, "points_per_s": pts.shape[0] / (ms * 1e-3)}
 
 
 PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")

@@ -79,6 +79,12 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
 /* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
  * backward round, and the backward reduction's sub-batch. Returns the variant count. */
 int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, int32_t *bwd_sub);
+/* No counterpart in the reference (measurement). The (pixel, Gaussian) pairs the
+ * reference's loops evaluate over the context's last single-view frame: out[0] for the
+ * forward (core/cpu/msplat_cpu.cpp:574-626: each pixel walks its tile's list up to the
+ * entry that ends it, or to the end), out[1] for the backward (:959-1031: from the
+ * pixel's last contributor down). Synchronises the context's stream. */
+int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out);
 /* Bytes of device memory the context's caches hold. */
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx);
 

@@ -590,6 +590,13 @@ class Context:
     def num_isects(self) -> int:
         return int(self._lib.msplat_cuda_num_isects(self.handle))
 
+    def pair_counts(self):
+        """(forward, backward) (pixel, Gaussian) pairs the reference's loops evaluate
+        over the last single-view frame (msplat_cuda_frame_pair_counts). Synchronises."""
+        out = np.zeros(2, np.int64)
+        check(self._lib.msplat_cuda_frame_pair_counts(self.handle, C.c_void_p(out.ctypes.data)))
+        return int(out[0]), int(out[1])
+
     def enable_stage_timing(self, on: bool = True) -> None:
         check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"stage_timing", int(on)))
 

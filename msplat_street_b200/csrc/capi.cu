@@ -1219,6 +1219,31 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
 
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
 
+int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out) {
+    if (!ctx || !out) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    out[0] = out[1] = 0;
+    if (ctx->tiles_x <= 0 || ctx->tiles_y <= 0 || !ctx->tile_start.ptr || !ctx->final_idx.ptr) return MSPLAT_CUDA_OK;
+    if (ctx->gid_in_vals) return fail(MSPLAT_CUDA_EINVAL, "the last frame was a batched render");
+    ENSURE(ctx->pairs, 2, unsigned long long, d);
+    RasterArgs a{};
+    a.W = ctx->W;
+    a.H = ctx->H;
+    a.tiles_x = ctx->tiles_x;
+    a.tiles_y = ctx->tiles_y;
+    a.tile_start = reinterpret_cast<const int32_t *>(ctx->tile_start.ptr);
+    a.tile_end = reinterpret_cast<const int32_t *>(ctx->tile_end.ptr);
+    a.isect_gid = reinterpret_cast<const int32_t *>(ctx->isect_gid.ptr);
+    a.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
+    a.final_idx = reinterpret_cast<int32_t *>(ctx->final_idx.ptr);
+    launch_pair_counts(a, d, ctx->stream);
+    unsigned long long h[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    out[0] = (int64_t)h[0];
+    out[1] = (int64_t)h[1];
+    return MSPLAT_CUDA_OK;
+}
+
 int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, int32_t *bwd_sub) {
     if (v >= 0 && v < N_RASTER_VARIANTS) {
         if (fwd_batch) *fwd_batch = RASTER_VARIANTS[v].fwd_batch;

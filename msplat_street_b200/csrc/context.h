@@ -196,6 +196,7 @@ struct msplat_cuda_ctx {
     // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
     int tstore_cap = 0;
     Buf tstore, tcount;
+    Buf pairs;  // the frame's pair counts (msplat_cuda_frame_pair_counts)
     // depth-chunked compositing: option "chunked_raster" (0 off, 1 frames of fewer
     // than CHUNK_AUTO_TILES tiles, 2 every frame) and "chunk_len"; whether the last
     // single-view frame ran chunked, its item bound, and the ChunkArgs planes
@@ -231,7 +232,7 @@ struct msplat_cuda_ctx {
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
+                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &pairs, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
                       &dvals[0], &dvals[1], &dcounts, &doff, &img[0], &img[1], &img[2], &img[3], &img[4], &img[5]};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);

@@ -97,6 +97,9 @@ constexpr RasterVariant RASTER_VARIANTS[N_RASTER_VARIANTS] = {
 inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v : 0; }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
+// (pixel, Gaussian) pairs the reference's forward / backward loops evaluate over the
+// frame (out[0], out[1]; device counters)
+void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st);
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st);
 
 struct RasterBwdArgs;

@@ -314,7 +314,18 @@ __device__ __forceinline__ void bwd_warp_sums(const float *mypb, float *red, uin
 // CHUNK: piece `chunk` of the list only (item `item`), each pixel starting from the
 // transmittance behind the piece (prefix * piece T), the colour behind it and the
 // piece's last contributor; the background term still uses the merged final T.
-template <int BB, int SB, bool AUX = false, bool CHUNK = false>
+// TS: stored-transmittance mode (a.tstore set): T before each of a pixel's first
+// a.tcap contributions is read back instead of recovered by division.
+//
+// Per hit the lanes keep nine sums for the slot: the colour gradients fac * v (3), and
+// for the sigma gradient vs = -alpha v_alpha its moments vs dx, vs dy, vs dx^2,
+// vs dx dy, vs dy^2 and vs itself; the block's sum turns the moments into the
+// reference's slot values once per splat (xy = conic * (vs dx, vs dy), conic = vs d d^T
+// / 2, opacity logit = (o - 1) vs), which is the reference's per-pixel arithmetic
+// with the splat's constants factored out of the sums. The colour part of v_alpha
+// needs the colour behind the pixel only through its dot product with the pixel's
+// colour cotangent, so one running scalar replaces the three-channel buffer.
+template <int BB, int SB, bool AUX = false, bool CHUNK = false, bool TS = false>
 __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
                                                 int &kmax, const ChunkArgs *ck = nullptr, int item = 0,
                                                 int chunk = 0) {
@@ -339,7 +350,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     const int pid = py * a.W + px;
     float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f, vd = 0.f, vaa = 0.f;
     float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
-    float br = 0.f, bgc = 0.f, bb = 0.f;  // accumulated colour behind (the "buffer")
+    float br = 0.f, bgc = 0.f, bb = 0.f;  // chunked: the colour behind the piece
     int kf = start - 1;
     if (inside) {
         Tf = a.final_T[pid];
@@ -372,13 +383,16 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     if (inside) atomicMax(&kmax, min(kf, end - 1));
     __syncthreads();
     const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
-    // T_final * bg, then the -ra * (T_final * bg) term of the reference's v_alpha
-    const float tbr = Tf * bgr, tbg = Tf * bgg, tbb = Tf * bgb;
+    // (T_final bg) . v, the background's share of every v_alpha, and the colour behind
+    // the current Gaussian dotted with v (the chunked backward starts from the colour
+    // behind its piece)
+    const float tbv = __fmaf_rn(Tf * bgr, vr, __fmaf_rn(Tf * bgg, vg, Tf * bgb * vb));
+    float bv = CHUNK ? __fmaf_rn(br, vr, __fmaf_rn(bgc, vg, bb * vb)) : 0.f;
     float bd = 0.f, ba = 0.f;             // aux: accumulated depth and alpha behind
     const float fpx = (float)px, fpy = (float)py;
     float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
     // stored-transmittance mode: contributions left to pop, -1 = recover T by division
-    int tj = (!CHUNK && a.tstore && inside) ? a.tcount[pid] : -1;
+    int tj = (TS && inside) ? a.tcount[pid] : -1;
     const size_t npix = (size_t)a.W * a.H;
     for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
         const int b_start = max(start, b_end - BWD_BATCH);
@@ -433,23 +447,18 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                             // no decision depends on T here: the hardware reciprocal (within
                             // an ulp or two) recovers it within the gradient tolerance
                             const float ra = __fdividef(1.f, 1.f - alpha);
-                            if (tj > 0) {
+                            if (TS && tj > 0) {
                                 tj--;
                                 T = a.tstore[(size_t)tj * npix + pid];  // T before this Gaussian, as stored
                             } else {
                                 T *= ra;  // recovered by division (core/cpu/msplat_cpu.cpp:996-997)
                             }
                             const float fac = alpha * T;
-                            const float cr = B.z, cg = B.w, cb = C.x;  // staged colours
                             // gradient arithmetic (no decision depends on it) uses fused
                             // multiply-adds; the reference's values are met within the
                             // gradient tolerance, not bit for bit
-                            const float nra = -ra;
-                            const float ir = __fmaf_rn(-br, ra, nra * tbr), ig = __fmaf_rn(-bgc, ra, nra * tbg),
-                                        ib = __fmaf_rn(-bb, ra, nra * tbb);
-                            const float orr = __fmaf_rn(cr, T, ir), og = __fmaf_rn(cg, T, ig),
-                                        ob = __fmaf_rn(cb, T, ib);
-                            float va = __fmaf_rn(orr, vr, __fmaf_rn(og, vg, ob * vb));
+                            const float cv = __fmaf_rn(B.z, vr, __fmaf_rn(B.w, vg, C.x * vb));  // staged colour . v
+                            float va = __fmaf_rn(T, cv, -ra * (bv + tbv));
                             if (AUX) {
                                 const float z = C.y;
                                 va += __fmaf_rn(__fmaf_rn(-bd, ra, z * T), vd, __fmaf_rn(-ba, ra, T) * vaa);
@@ -457,23 +466,20 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                                 ba += fac;
                                 g[9] = fac * vd;
                             }
-                            br = __fmaf_rn(cr, fac, br);
-                            bgc = __fmaf_rn(cg, fac, bgc);
-                            bb = __fmaf_rn(cb, fac, bb);
+                            bv = __fmaf_rn(fac, cv, bv);
                             // colour gradients; a channel whose raw + 0.5 < 0 passes none,
                             // which the block's sum applies once per splat
                             g[5] = fac * vr;
                             g[6] = fac * vg;
                             g[7] = fac * vb;
-                            if (alpha < 0.999f) {
+                            if (alpha < 0.999f) {  // moments of vs = -alpha v_alpha
                                 const float vs = -alpha * va;
-                                const float hv = 0.5f * vs;
-                                g[2] = hv * dx * dx;
-                                g[3] = hv * dx * dy;
-                                g[4] = hv * dy * dy;
-                                g[0] = vs * __fmaf_rn(A.z, dx, A.w * dy);
-                                g[1] = vs * __fmaf_rn(A.w, dx, B.x * dy);
-                                g[8] = __fmaf_rn(vs, op, -vs);  // -vs * (1 - op)
+                                g[0] = vs * dx;
+                                g[1] = vs * dy;
+                                g[2] = g[0] * dx;
+                                g[3] = g[0] * dy;
+                                g[4] = g[1] * dy;
+                                g[8] = vs;
                             }
                         }
                     }
@@ -495,16 +501,31 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         for (int idx = threadIdx.x; idx < cnt * NG; idx += blockDim.x) {
             const int j = idx / NG, c = idx - j * NG;
             const uint32_t m = hitw[j];
-            float s = 0.f;
+            float s = 0.f, s2nd = 0.f;  // xy: the sums of vs dx and vs dy
+            const int c0 = c < 2 ? 0 : c;
 #pragma unroll
             for (int w = 0; w < BWD_WARPS; w++)
-                if ((m >> w) & 1u) s += red[(w * BWD_BATCH + j) * NG + c];
-            if (c >= 5 && c <= 7) {  // the staged colour's sign bit: raw + 0.5 < 0 passes no gradient
+                if ((m >> w) & 1u) {
+                    const float *r = red + (w * BWD_BATCH + j) * NG;
+                    s += r[c0];
+                    if (c < 2) s2nd += r[1];
+                }
+            float out;
+            if (c < 2) {  // v_xy = conic * (sum vs dx, sum vs dy)
+                const float ca = s0[j].z, cb = s0[j].w, cc = s1[j].x;
+                out = c == 0 ? __fmaf_rn(ca, s, cb * s2nd) : __fmaf_rn(cb, s, cc * s2nd);
+            } else if (c < 5) {
+                out = 0.5f * s;  // v_conic = (vs dx dx, vs dx dy, vs dy dy) / 2
+            } else if (c < 8) {  // the staged colour's sign bit: raw + 0.5 < 0 passes no gradient
                 const float col = c == 5 ? s1[j].z : (c == 6 ? s1[j].w : s2[j].x);
-                if (signbit(col)) s = 0.f;
+                out = signbit(col) ? 0.f : s;
+            } else if (c == 8) {
+                out = __fmaf_rn(s, s1[j].y, -s);  // opacity logit: -vs (1 - o)
+            } else {
+                out = s;  // aux: depth
             }
-            if (c < 9) a.slots[(size_t)(b_start + j) * 9 + c] = s;
-            else a.slots_depth[b_start + j] = s;
+            if (c < 9) a.slots[(size_t)(b_start + j) * 9 + c] = out;
+            else a.slots_depth[b_start + j] = out;
         }
         __syncthreads();
     }
@@ -516,12 +537,12 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
     }
 }
 
-template <int BB, int SB, bool AUX = false>
+template <int BB, int SB, bool AUX = false, bool TS = false>
 __global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_kernel(RasterBwdArgs a) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
     const int tile = blockIdx.x;
-    raster_bwd_tile<BB, SB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
+    raster_bwd_tile<BB, SB, AUX, false, TS>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
 }
 
 // Persistent backward over the tiles of a batch of views, pulling global tile ids
@@ -575,15 +596,16 @@ void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
     }
 }
 
-template <int BB, int SB>
+template <int BB, int SB, bool AUX = false, bool TS = false>
 void bwd_launch(const RasterBwdArgs &a, int T, cudaStream_t st) {
-    constexpr size_t smem = raster_bwd_smem<BB, SB>();
-    static const bool attr = [] {  // once per variant, thread-safe
-        cudaFuncSetAttribute(raster_bwd_kernel<BB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    constexpr size_t smem = raster_bwd_smem<BB, SB, AUX ? 10 : 9>();
+    static const bool attr = [] {  // once per instance, thread-safe
+        cudaFuncSetAttribute(raster_bwd_kernel<BB, SB, AUX, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         return true;
     }();
     (void)attr;
-    raster_bwd_kernel<BB, SB><<<T, TILE_PIX, smem, st>>>(a);
+    raster_bwd_kernel<BB, SB, AUX, TS><<<T, TILE_PIX, smem, st>>>(a);
 }
 
 template <int BB, int SB>
@@ -606,6 +628,10 @@ void bwd_batch_launch(const RasterBwdArgs *d_views, const int *d_tile_off, int n
 void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
+    if (a.tstore) {  // stored-transmittance mode: the default staging only
+        bwd_launch<128, 3, false, true>(a, T, st);
+        return;
+    }
     const RasterVariant &v = RASTER_VARIANTS[variant_index(variant)];
 #define X(bb, sb)                                    \
     if (v.bwd_batch == bb && v.bwd_sub == sb) {      \
@@ -621,13 +647,8 @@ void launch_raster_bwd(const RasterBwdArgs &a, cudaStream_t st, int variant) {
 void launch_raster_bwd_aux(const RasterBwdArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    constexpr size_t smem = raster_bwd_smem<64, 3, 10>();
-    static const bool attr = [] {
-        cudaFuncSetAttribute(raster_bwd_kernel<64, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        return true;
-    }();
-    (void)attr;
-    raster_bwd_kernel<64, 3, true><<<T, TILE_PIX, smem, st>>>(a);
+    if (a.tstore) bwd_launch<64, 3, true, true>(a, T, st);
+    else bwd_launch<64, 3, true, false>(a, T, st);
 }
 
 void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off, int n_views, int *d_counter,
@@ -643,6 +664,54 @@ void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off
     MSPLAT_BWD_VARIANTS(X)
 #undef X
     bwd_batch_launch<128, 3>(d_views, d_tile_off, n_views, d_counter, st);
+}
+
+// ---------------------------------------------------------------------------------
+// Work counts of a frame (measurement): per pixel, the (pixel, Gaussian) pairs the
+// reference's loops evaluate. rasterize_forward (core/cpu/msplat_cpu.cpp:574-626)
+// walks the tile's list from its start until the entry that ends the pixel -- the
+// first contributing entry after the pixel's last contributor, if any -- or to the
+// list's end; rasterize_backward (:959-1031) walks from min(final_idx, end - 1) down
+// to the start. out[0] += forward pairs, out[1] += backward pairs.
+__global__ void __launch_bounds__(TILE_PIX) pair_count_kernel(RasterArgs a, unsigned long long *out) {
+    const int tile = blockIdx.x, tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    int lx, ly;
+    tile_pixel(threadIdx.x, lx, ly);
+    const int px = tx * TILE + lx, py = ty * TILE + ly;
+    unsigned long long fwd = 0, bwd = 0;
+    if (px < a.W && py < a.H) {
+        const int start = a.tile_start[tile], end = a.tile_end[tile];
+        const size_t pid = (size_t)py * a.W + px;
+        const int last = a.final_idx[pid];
+        bwd = (unsigned long long)max(0, min(last, end - 1) - start + 1);
+        int stop = end;  // the entry that ends the pixel, or the list's end
+        for (int k = max(last + 1, start); k < end; k++) {
+            const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
+            const float4 A = rec[0], B = rec[1];
+            const float dx = A.x - (float)px, dy = A.y - (float)py;
+            const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
+            if (sigma < 0.f || sigma >= 5.55f) continue;
+            if (fminf(0.999f, B.y * exp_ref(-sigma)) < 1.f / 255.f) continue;
+            stop = k + 1;
+            break;
+        }
+        fwd = (unsigned long long)max(0, stop - start);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        fwd += __shfl_xor_sync(0xffffffffu, fwd, o);
+        bwd += __shfl_xor_sync(0xffffffffu, bwd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, fwd);
+        atomicAdd(out + 1, bwd);
+    }
+}
+
+void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st) {
+    const int T = a.tiles_x * a.tiles_y;
+    cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), st);
+    if (T > 0) pair_count_kernel<<<T, TILE_PIX, 0, st>>>(a, d_out);
 }
 
 // ---------------------------------------------------------------------------------

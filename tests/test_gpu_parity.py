@@ -230,3 +230,45 @@ def test_hundred_steps_c1_trajectory(oracle):
     psnr = 10 * np.log10(1.0 / max(np.mean((a - b) ** 2), 1e-20))
     print("trajectory PSNR after 100 steps:", psnr)
     assert psnr > 30.0
+
+
+def test_pair_counts_follow_the_reference_loops(oracle):
+    """msplat_cuda_frame_pair_counts: per pixel, the forward pairs are the entries the
+    reference's rasterize_forward visits (core/cpu/msplat_cpu.cpp:574-626: up to and
+    including the one that ends the pixel, else the whole list) and the backward pairs
+    those rasterize_backward visits (:959-1031: from min(final_idx, end - 1) down to
+    the start), recounted here from the frame with the kernels' float32 arithmetic."""
+    g = scenes.random_gaussians(600, 12, log_scale_mean=-2.5)
+    cam = prepare_cam(look_at((0.3, 0.2, 2.4), (0, 0, 0)), 70, 45, 80.0, 78.0, 35.0, 22.0)
+    oracle.render(g, cam, BACKGROUND)
+    ctx = Context()
+    ctx.render(GaussianParams.from_numpy(g), cam, BACKGROUND)
+    got = ctx.pair_counts()
+    # the frame's lists and last contributors equal the oracle's bit for bit (test_forward);
+    # the splat records are the kernel's own
+    ts, te = ctx.frame("tile_start").cpu().numpy(), ctx.frame("tile_end").cpu().numpy()
+    gid, fidx = ctx.frame("isect_gid").cpu().numpy(), ctx.frame("final_idx").cpu().numpy()
+    assert np.array_equal(fidx, oracle.frame("final_idx"))
+    sp = splat_fields(ctx.frame("splats").cpu().numpy())
+    xy, con, op = sp["xys"], sp["conics"], sp["opacity"]
+    f = np.float32
+    fwd = bwd = 0
+    for py in range(cam.height):
+        for px in range(cam.width):
+            t = (py // 16) * cam.tiles_x + px // 16
+            s, e, last = int(ts[t]), int(te[t]), int(fidx[py * cam.width + px])
+            bwd += max(0, min(last, e - 1) - s + 1)
+            stop = e
+            for k in range(max(last + 1, s), e):
+                i = gid[k]
+                dx, dy = f(xy[i, 0]) - f(px), f(xy[i, 1]) - f(py)
+                sig = f(0.5) * (con[i, 0] * dx * dx + con[i, 2] * dy * dy) + con[i, 1] * dx * dy
+                if sig < 0 or sig >= f(5.55):
+                    continue
+                if min(f(0.999), f(op[i]) * f(np.exp(-np.float64(sig)))) < f(1.0) / f(255.0):
+                    continue
+                stop = k + 1
+                break
+            fwd += max(0, stop - s)
+    assert got == (fwd, bwd), (got, fwd, bwd)
+    assert fwd >= bwd > 0
