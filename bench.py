@@ -53,7 +53,10 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms around the timed
+    region. A timed region can be shorter than nvidia-smi's start-up, so entering waits
+    (at most 5 s) for the first sample and leaving waits (at most 2 s) for one taken
+    after the region ended: the record always brackets the region."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -69,14 +72,29 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self._wait_rows(1, 5.0)
         except Exception:
             self.proc = None
         return self
 
+    def _rows(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.count(",") >= 8)
+        except Exception:
+            return 0
+
+    def _wait_rows(self, n: int, limit_s: float) -> None:
+        t0 = time.perf_counter()
+        while self.proc is not None and self.proc.poll() is None and self._rows() < n \
+                and time.perf_counter() - t0 < limit_s:
+            time.sleep(0.01)
+
     def __exit__(self, *exc):
         if self.proc is not None:
+            self._wait_rows(self._rows() + 1, 2.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -345,6 +363,14 @@ def run_ours(args, world, rank, local):
         except Exception as e:
             batching = {"error": f"{type(e).__name__}: {e}"}
 
+    # ---- the reference's C++ callers' path: bindings.h with host tensors (rank 0) ----
+    bindings = None
+    if rank == 0:
+        try:
+            bindings = bindings_report(dev)
+        except Exception as e:
+            bindings = {"error": f"{type(e).__name__}: {e}"}
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if world == 1:
@@ -378,6 +404,7 @@ def run_ours(args, world, rank, local):
             "chunked_compositing": chunk,
             "serving": serve,
             "batching": batching,
+            "bindings_h": bindings,
         }
         if serve and "rates" in serve:
             hi = serve["rates"].get("1000") or next(iter(serve["rates"].values()))
@@ -386,6 +413,46 @@ def run_ours(args, world, rank, local):
                               "plain_p50_ms": hi["plain"]["p50_ms"], "plain_p99_ms": hi["plain"]["p99_ms"],
                               "at_rate_req_s": 1000}
         print(json.dumps(line))
+
+
+def bindings_report(dev, steps: int = 300, warmup: int = 10) -> dict:
+    """Training-step throughput on the small plain config (10k Gaussians, 256x256)
+    through bindings.h with host tensors -- the path core/src/model.cpp and the CLI take
+    (msplat_street_b200/_build/train_bindings, wall clock, every call staging its
+    tensors to the device and back) -- next to the same step through the Python API
+    with device-resident tensors (CUDA events)."""
+    import torch
+    from msplat_street_b200 import build, scenes
+    from msplat_street_b200.backend import AdamState, Context, GaussianParams
+    from msplat_street_b200.trainer import LR_INIT
+    out = {"config": "10k Gaussians, 256x256, SH degree 3, L1 + 0.2 SSIM, Adam"}
+    if os.path.exists(build.TRAIN_BINDINGS):
+        r = subprocess.run([build.TRAIN_BINDINGS, str(steps), str(warmup)], capture_output=True, text=True,
+                           timeout=300)
+        line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        out["bindings_h"] = json.loads(line[-1]) if r.returncode == 0 and line else {"error": r.stderr[-300:]}
+    else:
+        out["bindings_h"] = {"error": "train_bindings not built (needs the reference headers at build time)"}
+    ctx = Context()
+    cam = scenes.small_camera()
+    bg = np.array([0.6130, 0.0101, 0.3984], np.float32)
+    gt = ctx.render(GaussianParams.from_numpy(scenes.small_scene(1)), cam, bg).clone()
+    p = GaussianParams.from_numpy(scenes.small_scene(0))
+    adam = AdamState.zeros_like(p, LR_INIT)
+    stats = tuple(torch.zeros(p.n, device=dev) for _ in range(3))
+    for _ in range(warmup):
+        ctx.train_step(p, adam, cam, bg, gt, stats)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        ctx.train_step(p, adam, cam, bg, gt, stats)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out["python_api"] = {"iters_per_s": 1e3 / ms, "ms_per_step": ms, "steps": steps}
+    ctx.close()
+    return out
 
 
 def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_step: int = 8):

@@ -97,6 +97,10 @@ int msplat_cuda_sync(msplat_cuda_ctx *ctx);
 /* bindings.h:18-19 gpu_zeros / gpu_empty -- managed (host- and device-visible) memory. */
 int msplat_cuda_alloc(size_t bytes, int zero, void **out);
 int msplat_cuda_free(void *ptr);
+/* No counterpart in the reference. Plain device memory (cudaMalloc; release with
+ * msplat_cuda_free), for callers that stage host data themselves with
+ * msplat_cuda_copy_buffer -- the bindings.h layer keeps its per-tensor staging in it. */
+int msplat_cuda_device_alloc(size_t bytes, void **out);
 
 /* bindings.h:143 msplat_copy_buffer -- copy `bytes` from src to dst, ordered on the
  * context's stream (any mix of device, managed and host memory). */
@@ -338,7 +342,8 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
 /* Per-frame intermediates of the last render / train step (test and debug hook, like
  * the reference's _gpu_* hooks, python/bindings.cpp:655-738). Names: splats (N x 12
  * floats: x y conic_a conic_b | conic_c sigmoid(opacity) r g | b depth - -), radii,
- * aabb, tile_start, tile_end, isect_gid, out_img, final_Ts, final_idx, v_rendered and,
+ * aabb, tile_start, tile_end, isect_gid, slots (per sorted intersection the 9 gradient
+ * sums of its tile: xy conic rgb opacity-logit), out_img, final_Ts, final_idx, v_rendered and,
  * with option keep_grads, v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat; with a
  * prior (msplat_cuda_set_prior): out_depth bg_img v_aux (dL/d depth numerator, dL/d
  * alpha per pixel) out_adj v_adj (exposure-adjusted render and its gradient) and,

@@ -103,6 +103,28 @@ def build_reference_gradcheck(ref_root: str, force: bool = False) -> str:
     return GRADCHECK
 
 
+TRAIN_BINDINGS = os.path.join(BUILD, "train_bindings")
+
+
+def build_bindings_bench(ref_root: str, force: bool = False) -> str:
+    """Builds integration/train_bindings.cpp (training-step throughput through
+    bindings.h with host tensors, as the reference's own callers hold them) against the
+    reference's headers and integration/bindings_cuda.cpp. Needs g++ and the reference
+    tree; the result runs without either."""
+    src = os.path.join(PKG, "integration", "train_bindings.cpp")
+    shim = os.path.join(PKG, "integration", "bindings_cuda.cpp")
+    lib = build(force)
+    deps = [src, shim, lib, os.path.join(ROOT, "include", "msplat_cuda.h")]
+    if force or _stale(TRAIN_BINDINGS, deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ref_root, "core", "metal"), "-I",
+               os.path.join(ref_root, "core", "include"), "-I", os.path.join(ROOT, "include"), "-o", TRAIN_BINDINGS,
+               src, shim, "-L", PKG, "-lmsplat_cuda", "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"train_bindings build failed:\n{r.stdout}\n{r.stderr}")
+    return TRAIN_BINDINGS
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")

@@ -535,6 +535,13 @@ int msplat_cuda_alloc(size_t bytes, int zero, void **out) {
     return MSPLAT_CUDA_OK;
 }
 
+int msplat_cuda_device_alloc(size_t bytes, void **out) {
+    if (!out) return fail(MSPLAT_CUDA_EINVAL, "null output pointer");
+    if (bytes == 0) bytes = 4;
+    CUDA_TRY(cudaMalloc(out, bytes));
+    return MSPLAT_CUDA_OK;
+}
+
 int msplat_cuda_free(void *ptr) {
     if (ptr) CUDA_TRY(cudaFree(ptr));
     return MSPLAT_CUDA_OK;
@@ -1306,6 +1313,7 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         {"tile_start", &ctx->tile_start, T},
         {"tile_end", &ctx->tile_end, T},
         {"isect_gid", &ctx->isect_gid, ctx->n_isect},
+        {"slots", &ctx->slots, ctx->n_isect * 9},
         {"out_img", &ctx->out_img, npix * 3},
         {"final_Ts", &ctx->final_T, npix},
         {"final_idx", &ctx->final_idx, npix},

@@ -41,6 +41,42 @@ __host__ __device__ inline uint32_t num_sh_bases(uint32_t degree) {
 // exp in double, rounded once to float
 __device__ __forceinline__ float exp_ref(float x) { return (float)exp((double)x); }
 
+// Two float32 values in one 64-bit register pair, for sm_100's packed FP32
+// instructions (PTX add / mul / fma .rn.f32x2): one instruction issues two IEEE
+// single-precision operations, each rounded exactly as its scalar form, so packing
+// changes no result -- only the instruction count of an issue-bound kernel.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(f32x2 v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 struct V2 { float x, y; };
 struct V3 { float x, y, z; };
 struct Q4 { float x, y, z, w; };  // quaternion stored (w, x, y, z) lands in x, y, z, w
@@ -163,6 +199,10 @@ __device__ __forceinline__ void tile_pixel(int t, int &lx, int &ly) {
     const int w = t >> 5, l = t & 31;
     lx = ((w & 1) << 3) + (l & 7);
     ly = ((w >> 1) << 2) + (l >> 3);
+}
+// The thread index tile_pixel maps to pixel (lx, ly) of the tile (its inverse).
+__device__ __forceinline__ int tile_index(int lx, int ly) {
+    return ((((ly >> 2) << 1) + (lx >> 3)) << 5) + ((ly & 3) << 3) + (lx & 7);
 }
 
 // Counter-based RNG: PCG hash + Box-Muller (core/cpu/msplat_cpu.cpp:304-323)

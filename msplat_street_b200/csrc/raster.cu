@@ -1,11 +1,15 @@
 // 16x16-tile front-to-back alpha compositing, forward and backward.
 //
-// One 256-thread CTA per tile, one pixel per thread. The tile's depth-sorted list is
-// walked in batches whose splat records are staged in shared memory; every thread
-// reads each record as a broadcast. Staging also clamps the colours once and marks
-// which of the tile's eight warp blocks (8x4 pixels each) the splat can reach at all
-// (its box and its ellipse's diagonal extents), so a warp passes over the splats that
-// miss its pixels with one bit test; the forward walks its splats by ballot.
+// One CTA per tile. The tile's depth-sorted list is walked in batches whose splat
+// records are staged in shared memory; every thread reads each record as a broadcast.
+// Staging also clamps the colours once and marks which of the tile's warp blocks the
+// splat can reach at all (its box and its ellipse's diagonal extents, tested on 8 x 4
+// pixel blocks), so a warp passes over the splats that miss its pixels with one bit
+// test and walks the rest by ballot. The forward runs one pixel per thread (256
+// threads, 8 x 4 pixels per warp). The backward runs two pixels per thread (128
+// threads, one column and rows y, y + 4 of the warp's 8 x 8 block): its decisions and
+// sigma stay scalar, and its gradient arithmetic uses sm_100's packed FP32
+// instructions (add / mul / fma .f32x2), two operations per instruction.
 //
 // Forward: rasterize_forward (core/cpu/msplat_cpu.cpp:574-626): sigma < 0 or >= 5.55
 // skips, alpha = min(0.999, o * exp(-sigma)) with alpha < 1/255 skipped, and the pixel
@@ -37,7 +41,10 @@
 
 namespace msplat {
 
-constexpr int BWD_WARPS = TILE_PIX / 32;
+// the forward's block: one thread per pixel (8 x 4 pixels per warp); the backward's:
+// 128 threads, two pixels each (8 x 8 pixels per warp)
+constexpr int FWD_THREADS = TILE_PIX;
+constexpr int BWD_THREADS = TILE_PIX / 2, BWD_WARPS = BWD_THREADS / 32;
 
 // A splat's colour channel as the rasterizers use it, max(raw + 0.5, 0), computed once
 // at staging. A channel clamped to zero is stored as -0.0, so its sign bit carries the
@@ -200,7 +207,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
 }
 
 template <int FB, bool AUX = false>
-__global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(FWD_THREADS) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     const int tile = blockIdx.x;
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(TILE_PIX) raster_fwd_kernel(RasterArgs a) {
 // until none are left. A tile's image equals what the per-view kernel renders: the
 // same list (the batch sort keeps each tile's order) and the same code.
 template <int FB>
-__global__ void __launch_bounds__(TILE_PIX, 4) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
+__global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     __shared__ int s_tile, s_lt;
@@ -238,19 +245,20 @@ __global__ void __launch_bounds__(TILE_PIX, 4) raster_fwd_batch_kernel(const Bat
 
 // Resident blocks of a kernel on the whole GPU.
 template <typename K>
-int resident_grid(K kernel, size_t smem) {
+int resident_grid(K kernel, size_t smem, int threads = TILE_PIX) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE_PIX, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     return std::max(1, sms * std::max(per_sm, 1));
 }
 
 template <int FB>
 void fwd_batch_launch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st) {
-    static const int grid = resident_grid(raster_fwd_batch_kernel<FB>, 0);  // once per variant, thread-safe
+    // once per variant, thread-safe
+    static const int grid = resident_grid(raster_fwd_batch_kernel<FB>, 0, FWD_THREADS);
     const int g = tiles_hint > 0 ? std::min(grid, tiles_hint) : grid;
-    raster_fwd_batch_kernel<FB><<<g, TILE_PIX, 0, st>>>(d, d_counter);
+    raster_fwd_batch_kernel<FB><<<g, FWD_THREADS, 0, st>>>(d, d_counter);
 }
 
 // tiles_hint: the batch's tile count when the host knows it (caps the grid), else 0
@@ -264,10 +272,10 @@ void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter,
 }
 
 // Per-warp reduction of the 9 gradient values over the warp's 32 pixels, done in
-// sub-batches of SB Gaussians: each lane stores its contributions to a transposed
-// buffer (one row of 32 lane values per output), then each lane sums whole rows with
-// float4 loads. 9 SB outputs x 31 adds per sub-batch, in a fixed lane order. BB
-// Gaussians are staged in shared memory per round.
+// sub-batches of SB hit Gaussians: each lane stores its contributions to a transposed
+// buffer (one row of 32 lane values per output), then each lane sums a whole row with
+// float4 loads as a fixed pairwise tree (15 packed adds and one add). BB Gaussians
+// are staged in shared memory per round.
 constexpr int PB_STRIDE = 36;  // floats per row: 32 lanes + pad, keeps float4 rows conflict-free
 
 // NG: gradient values per intersection, 9 (xy conic rgb opacity) or 10 with the
@@ -280,7 +288,7 @@ constexpr size_t raster_bwd_smem() {
 
 // One warp's sums of its q (<= SB) pending splats: row o = jj * NG + c of the warp's
 // row buffer holds value c of pending splat jj (the oldest first) for the warp's 32
-// lanes; lane o sums it in lane order with float4 loads and stores the sum to
+// lanes; lane o sums it (a fixed pairwise tree) and stores the sum to
 // red[warp][j][c], j the splat's staged index (pend: 8 bits per splat, the newest
 // lowest). The lanes that own a splat's value 0 mark the warp in hitw[j].
 template <int NG, int SB>
@@ -290,17 +298,20 @@ __device__ __forceinline__ void bwd_warp_sums(const float *mypb, float *red, uin
     for (int o = lane; o < q * NG; o += 32) {
         const int jj = o / NG, c = o - jj * NG;
         const int j = (int)((pend >> (8 * (q - 1 - jj))) & 0xffu);
+        // the row's 32 lane values summed as a fixed pairwise tree, two sums per packed add
         const float4 *row = reinterpret_cast<const float4 *>(mypb + o * PB_STRIDE);
-        float s = 0.f;
+        f32x2 p[8];
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const float4 v = row[r];
-            s += v.x;
-            s += v.y;
-            s += v.z;
-            s += v.w;
+            p[r] = add2(pack2(v.x, v.y), pack2(v.z, v.w));
         }
-        red[(warp * bb + j) * NG + c] = s;
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1)
+#pragma unroll
+            for (int r = 0; r < w; r++) p[r] = add2(p[r], p[r + w]);
+        const float2 t = unpack2(p[0]);
+        red[(warp * bb + j) * NG + c] = t.x + t.y;
         if (c == 0) atomicOr(&hitw[j], 1u << warp);
     }
     __syncwarp();
@@ -308,21 +319,29 @@ __device__ __forceinline__ void bwd_warp_sums(const float *mypb, float *red, uin
 
 // One tile of the backward; `tile` indexes tile_start / tile_end and the slots (a
 // global tile id in a batch), (tx, ty) is its position in its view. Every thread of
-// the block calls it; it ends with the block's shared memory free for reuse. AUX: the
-// per-pixel background is the pixel's own, and the expected-depth / alpha cotangents
-// enter v_alpha and a tenth value per intersection (the aux branch of :959-1031).
+// the block (BWD_THREADS) calls it; it ends with the block's shared memory free for
+// reuse. Each thread owns two pixels of one column, rows y and y + 4 of its warp's
+// 8 x 8 block (warp w covers columns 8 (w % 2) .. +7 and rows 8 (w / 2) .. +7), and
+// evaluates both with sm_100's packed FP32 instructions: one instruction, two IEEE
+// operations, each rounded as its scalar form. Per-pixel decisions (sigma range,
+// alpha cut-offs, last contributor) stay per pixel; a pixel that does not take part
+// in a pair carries alpha = 0 through the packed update (T * 1, fac = 0), which leaves
+// its state exactly as it was.
+// AUX: the per-pixel background is the pixel's own, and the expected-depth / alpha
+// cotangents enter v_alpha and a tenth value per intersection (the aux branch of
+// :959-1031).
 // CHUNK: piece `chunk` of the list only (item `item`), each pixel starting from the
 // transmittance behind the piece (prefix * piece T), the colour behind it and the
 // piece's last contributor; the background term still uses the merged final T.
 // TS: stored-transmittance mode (a.tstore set): T before each of a pixel's first
 // a.tcap contributions is read back instead of recovered by division.
 //
-// Per hit the lanes keep nine sums for the slot: the colour gradients fac * v (3), and
-// for the sigma gradient vs = -alpha v_alpha its moments vs dx, vs dy, vs dx^2,
+// Per hit the lanes keep nine sums for the slot: the colour gradients fac * v (3), the
+// xy gradient vs (conic d) (2), and for vs = -alpha v_alpha its moments vs dx^2,
 // vs dx dy, vs dy^2 and vs itself; the block's sum turns the moments into the
-// reference's slot values once per splat (xy = conic * (vs dx, vs dy), conic = vs d d^T
-// / 2, opacity logit = (o - 1) vs), which is the reference's per-pixel arithmetic
-// with the splat's constants factored out of the sums. The colour part of v_alpha
+// reference's slot values once per splat (conic = vs d d^T / 2, opacity logit =
+// (o - 1) vs), the reference's per-pixel arithmetic with the splat's constants
+// factored out of the sums (the xy gradient stays per pixel: its two terms can cancel). The colour part of v_alpha
 // needs the colour behind the pixel only through its dot product with the pixel's
 // colour cotangent, so one running scalar replaces the three-channel buffer.
 template <int BB, int SB, bool AUX = false, bool CHUNK = false, bool TS = false>
@@ -330,90 +349,98 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                                                 int &kmax, const ChunkArgs *ck = nullptr, int item = 0,
                                                 int chunk = 0) {
     constexpr int NG = AUX ? 10 : 9;
-    constexpr int BWD_BATCH = BB, SUB = SB, SUB_OUT = SB * NG;
-    float4 *s0 = smem4, *s1 = s0 + BWD_BATCH, *s2 = s1 + BWD_BATCH;
-    float *red = reinterpret_cast<float *>(s2 + BWD_BATCH);  // [BWD_WARPS][BWD_BATCH][NG]
-    float *pbuf = red + BWD_WARPS * BWD_BATCH * NG;           // [BWD_WARPS][SUB_OUT][PB_STRIDE]
-    uint32_t *hitw = reinterpret_cast<uint32_t *>(pbuf + BWD_WARPS * SUB_OUT * PB_STRIDE);  // [BWD_BATCH] warps hit
-    uint8_t *sm = reinterpret_cast<uint8_t *>(hitw + BWD_BATCH);  // [BWD_BATCH] warp masks
-    int lx, ly;
-    tile_pixel(threadIdx.x, lx, ly);
-    const int px = tx * TILE + lx, py = ty * TILE + ly;
-    const bool inside = px < a.W && py < a.H;
+    constexpr int SUB = SB, SUB_OUT = SB * NG;
+    static_assert(BB <= BWD_THREADS, "one staging thread per splat");
+    float4 *s0 = smem4, *s1 = s0 + BB, *s2 = s1 + BB;
+    float *red = reinterpret_cast<float *>(s2 + BB);    // [BWD_WARPS][BB][NG]
+    float *pbuf = red + BWD_WARPS * BB * NG;             // [BWD_WARPS][SUB_OUT][PB_STRIDE]
+    uint32_t *hitw = reinterpret_cast<uint32_t *>(pbuf + BWD_WARPS * SUB_OUT * PB_STRIDE);  // [BB] warps hit
+    uint8_t *sm = reinterpret_cast<uint8_t *>(hitw + BB);  // [BB] warp masks
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lx = ((warp & 1) << 3) + (lane & 7), ly = ((warp >> 1) << 3) + (lane >> 3);
+    const int px = tx * TILE + lx, py[2] = {ty * TILE + ly, ty * TILE + ly + 4};
+    const bool inside[2] = {px < a.W && py[0] < a.H, px < a.W && py[1] < a.H};
     int start = a.tile_start[tile], end = a.tile_end[tile];
     if (CHUNK) {
         start += chunk * ck->chunk_len;
         end = min(end, start + ck->chunk_len);
     }
     if (end <= start) return;  // block-uniform
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pid = py * a.W + px;
-    float T = 0.f, Tf = 0.f, vr = 0.f, vg = 0.f, vb = 0.f, vd = 0.f, vaa = 0.f;
-    float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
-    float br = 0.f, bgc = 0.f, bb = 0.f;  // chunked: the colour behind the piece
-    int kf = start - 1;
-    if (inside) {
-        Tf = a.final_T[pid];
-        T = Tf;
-        kf = a.final_idx[pid];
-        if (CHUNK) {
-            const size_t o = (size_t)item * TILE_PIX + threadIdx.x, o3 = (size_t)item * 3 * TILE_PIX + threadIdx.x;
-            T = ck->pre[o] * ck->cT[o];
-            kf = ck->clast[o];
-            br = ck->aft[o3];
-            bgc = ck->aft[o3 + TILE_PIX];
-            bb = ck->aft[o3 + 2 * TILE_PIX];
-        }
-        const float *v = a.v_out + 3 * (size_t)pid;
-        vr = v[0];
-        vg = v[1];
-        vb = v[2];
+    int pid[2], kf[2] = {start - 1, start - 1}, tj[2] = {-1, -1};
+    float T[2] = {0.f, 0.f}, tbv[2] = {0.f, 0.f}, bv[2] = {0.f, 0.f}, vr[2] = {0.f, 0.f}, vg[2] = {0.f, 0.f},
+          vb[2] = {0.f, 0.f}, vd[2] = {0.f, 0.f}, vaa[2] = {0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        pid[i] = py[i] * a.W + px;
+        if (!inside[i]) continue;
+        const float Tf = a.final_T[pid[i]];
+        T[i] = Tf;
+        kf[i] = a.final_idx[pid[i]];
+        const float *v = a.v_out + 3 * (size_t)pid[i];
+        vr[i] = v[0];
+        vg[i] = v[1];
+        vb[i] = v[2];
+        float bgr = a.bg[0], bgg = a.bg[1], bgb = a.bg[2];
         if (AUX) {
-            const float2 va2 = reinterpret_cast<const float2 *>(a.v_aux)[pid];
-            vd = va2.x;
-            vaa = va2.y;
-            const float *bp = a.bg_img + 3 * (size_t)pid;
+            const float2 va2 = reinterpret_cast<const float2 *>(a.v_aux)[pid[i]];
+            vd[i] = va2.x;
+            vaa[i] = va2.y;
+            const float *bp = a.bg_img + 3 * (size_t)pid[i];
             bgr = bp[0];
             bgg = bp[1];
             bgb = bp[2];
         }
+        // (T_final bg) . v: the background's share of every v_alpha
+        tbv[i] = __fmaf_rn(Tf * bgr, vr[i], __fmaf_rn(Tf * bgg, vg[i], Tf * bgb * vb[i]));
+        if (CHUNK) {  // the piece's transmittance, last contributor, and the colour behind it
+            const int ti = tile_index(lx, ly + 4 * i);
+            const size_t o = (size_t)item * TILE_PIX + ti, o3 = (size_t)item * 3 * TILE_PIX + ti;
+            T[i] = ck->pre[o] * ck->cT[o];
+            kf[i] = ck->clast[o];
+            bv[i] = __fmaf_rn(ck->aft[o3], vr[i], __fmaf_rn(ck->aft[o3 + TILE_PIX], vg[i], ck->aft[o3 + 2 * TILE_PIX] * vb[i]));
+        }
+        if (TS) tj[i] = a.tcount[pid[i]];  // contributions left to pop, -1 = recover T by division
     }
     if (threadIdx.x == 0) kmax = start - 1;
     __syncthreads();
-    if (inside) atomicMax(&kmax, min(kf, end - 1));
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+        if (inside[i]) atomicMax(&kmax, min(kf[i], end - 1));
     __syncthreads();
     const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
-    // (T_final bg) . v, the background's share of every v_alpha, and the colour behind
-    // the current Gaussian dotted with v (the chunked backward starts from the colour
-    // behind its piece)
-    const float tbv = __fmaf_rn(Tf * bgr, vr, __fmaf_rn(Tf * bgg, vg, Tf * bgb * vb));
-    float bv = CHUNK ? __fmaf_rn(br, vr, __fmaf_rn(bgc, vg, bb * vb)) : 0.f;
-    float bd = 0.f, ba = 0.f;             // aux: accumulated depth and alpha behind
-    const float fpx = (float)px, fpy = (float)py;
+    // packed per-pixel state: (row y, row y + 4)
+    f32x2 T2 = pack2(T[0], T[1]), bv2 = pack2(bv[0], bv[1]);
+    const f32x2 tbv2 = pack2(tbv[0], tbv[1]), vr2 = pack2(vr[0], vr[1]), vg2 = pack2(vg[0], vg[1]),
+                vb2 = pack2(vb[0], vb[1]);
+    const float fpy[2] = {(float)py[0], (float)py[1]};
+    f32x2 bd2 = pack2(0.f, 0.f), ba2 = pack2(0.f, 0.f);  // aux: accumulated depth and alpha behind
+    const f32x2 vd2 = pack2(vd[0], vd[1]), vaa2 = pack2(vaa[0], vaa[1]);
+    const float fpx = (float)px;
     float *mypb = pbuf + warp * SUB_OUT * PB_STRIDE;
-    // stored-transmittance mode: contributions left to pop, -1 = recover T by division
-    int tj = (TS && inside) ? a.tcount[pid] : -1;
     const size_t npix = (size_t)a.W * a.H;
-    for (int b_end = kend; b_end > start; b_end -= BWD_BATCH) {
-        const int b_start = max(start, b_end - BWD_BATCH);
+    for (int b_end = kend; b_end > start; b_end -= BB) {
+        const int b_start = max(start, b_end - BB);
         const int cnt = b_end - b_start;
         if (threadIdx.x < cnt) {
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[b_start + threadIdx.x]);
             const float4 A = rec[0], B = rec[1], C = rec[2];
-            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
+            // the 8 x 4 blocks' reach bits, merged pairwise into the 8 x 8 warp blocks
+            const uint32_t m8 = warp_block_mask(A, C, tx, ty);
+            sm[threadIdx.x] = (uint8_t)(((m8 | (m8 >> 2)) & 3u) | ((((m8 >> 4) | (m8 >> 6)) & 3u) << 2));
             hitw[threadIdx.x] = 0u;
-            s0[threadIdx.x] = A;
-            s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
+            // staged: (x, y, conic a, conic c), (conic b, opacity, colour r, g), (colour b, depth)
+            s0[threadIdx.x] = make_float4(A.x, A.y, A.z, B.x);
+            s1[threadIdx.x] = make_float4(A.w, B.y, staged_colour(B.z), staged_colour(B.w));
             s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
         }
         __syncthreads();
         // This warp's reachable splats, back to front, 32 mask bits per ballot. Splats
-        // that some lane of the warp hits are written to the warp's row buffer (one row
-        // of 32 lane values per gradient value); every SUB of them, the warp's lanes sum
-        // whole rows in lane order (one pass of 27 sums for SUB = 3) into red[warp][j],
-        // and the splat's hitw bit for this warp is set. Warps that miss a splat neither
-        // store nor sum for it, and the block's sum over warps skips them: they would
-        // only add +0.0, which leaves every sum (never -0.0) as it is.
+        // that some pixel of the warp hits are written to the warp's row buffer (one row
+        // of 32 lane values, each the sum of the lane's two pixels, per gradient value);
+        // every SUB of them, the warp's lanes sum whole rows (one pass of 27 sums for
+        // SUB = 3) into red[warp][j], and the splat's hitw bit for this warp is set.
+        // Warps that miss a splat neither store nor sum for it, and the block's sum over
+        // warps (in warp order) skips them.
         int q = 0;          // splats pending in the row buffer (warp-uniform)
         uint32_t pend = 0;  // their staged indices, 8 bits each, the newest lowest
         for (int c32 = (cnt - 1) >> 5; c32 >= 0; c32--) {
@@ -424,96 +451,132 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                 bits &= ~(1u << hb);
                 const int j = (c32 << 5) + hb;
                 const int k = b_start + j;
-                const float4 A = s0[j], C = s2[j];
-                float g[NG];
+                const float4 A = s0[j], B = s1[j];
+                // sigma = 0.5 (a dx^2 + c dy^2) + b dx dy per pixel, scalar and in the
+                // reference's order of roundings: the decisions below must equal the
+                // forward pass's, and the compiler may fuse a packed multiply into a
+                // following packed add (dx is the pixels' shared column)
+                const float dx = A.x - fpx;
+                const float dy[2] = {A.y - fpy[0], A.y - fpy[1]};
+                const float adx = A.z * dx, bdx = B.x * dx;
+                float al[2];
+                bool hit[2];
 #pragma unroll
-                for (int c = 0; c < NG; c++) g[c] = 0.f;
-                bool hit = false;
-                if (inside && k <= kf) {
-                    const float4 B = s1[j];
-                    const float dx = A.x - fpx, dy = A.y - fpy;
-                    const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
-                    if (sigma >= 0.f && sigma < 5.55f) {
-                        const float op = B.y;
+                for (int i = 0; i < 2; i++) {
+                    const float sigma = 0.5f * (A.z * dx * dx + A.w * dy[i] * dy[i]) + B.x * dx * dy[i];
+                    hit[i] = false;
+                    al[i] = 0.f;
+                    if (inside[i] && k <= kf[i] && sigma >= 0.f && sigma < 5.55f) {
                         // The fast exponential is within 8 ulps here; near the 1/255 and
                         // 0.999 cut-offs alpha is recomputed exactly, so every decision
                         // equals the forward pass's.
-                        const float va_fast = op * __expf(-sigma);
+                        const float va_fast = B.y * __expf(-sigma);
                         float alpha = fminf(0.999f, va_fast);
                         if (fabsf(va_fast - 1.f / 255.f) <= 1e-5f * (1.f / 255.f) || fabsf(va_fast - 0.999f) <= 1e-5f)
-                            alpha = fminf(0.999f, op * exp_ref(-sigma));
+                            alpha = fminf(0.999f, B.y * exp_ref(-sigma));
                         if (alpha >= 1.f / 255.f) {
-                            hit = true;
-                            // no decision depends on T here: the hardware reciprocal (within
-                            // an ulp or two) recovers it within the gradient tolerance
-                            const float ra = __fdividef(1.f, 1.f - alpha);
-                            if (TS && tj > 0) {
-                                tj--;
-                                T = a.tstore[(size_t)tj * npix + pid];  // T before this Gaussian, as stored
-                            } else {
-                                T *= ra;  // recovered by division (core/cpu/msplat_cpu.cpp:996-997)
-                            }
-                            const float fac = alpha * T;
-                            // gradient arithmetic (no decision depends on it) uses fused
-                            // multiply-adds; the reference's values are met within the
-                            // gradient tolerance, not bit for bit
-                            const float cv = __fmaf_rn(B.z, vr, __fmaf_rn(B.w, vg, C.x * vb));  // staged colour . v
-                            float va = __fmaf_rn(T, cv, -ra * (bv + tbv));
-                            if (AUX) {
-                                const float z = C.y;
-                                va += __fmaf_rn(__fmaf_rn(-bd, ra, z * T), vd, __fmaf_rn(-ba, ra, T) * vaa);
-                                bd = __fmaf_rn(z, fac, bd);
-                                ba += fac;
-                                g[9] = fac * vd;
-                            }
-                            bv = __fmaf_rn(fac, cv, bv);
-                            // colour gradients; a channel whose raw + 0.5 < 0 passes none,
-                            // which the block's sum applies once per splat
-                            g[5] = fac * vr;
-                            g[6] = fac * vg;
-                            g[7] = fac * vb;
-                            if (alpha < 0.999f) {  // moments of vs = -alpha v_alpha
-                                const float vs = -alpha * va;
-                                g[0] = vs * dx;
-                                g[1] = vs * dy;
-                                g[2] = g[0] * dx;
-                                g[3] = g[0] * dy;
-                                g[4] = g[1] * dy;
-                                g[8] = vs;
-                            }
+                            hit[i] = true;
+                            al[i] = alpha;
                         }
                     }
                 }
-                if (__ballot_sync(0xffffffffu, hit)) {
-                    float *row = mypb + q * NG * PB_STRIDE + lane;
+                const bool any = hit[0] || hit[1];
+                if (!__ballot_sync(0xffffffffu, any)) continue;
+                float g[NG];
+                if (any) {
+                    const float4 C = s2[j];
+                    // no decision depends on T here: the hardware reciprocal (within an
+                    // ulp or two) recovers it within the gradient tolerance; a pixel that
+                    // takes no part keeps T (times 1) and gets fac = 0
+                    float ra[2];
 #pragma unroll
-                    for (int c = 0; c < NG; c++) row[c * PB_STRIDE] = g[c];
-                    pend = (pend << 8) | (uint32_t)j;
-                    if (++q == SUB) {
-                        bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BWD_BATCH);
-                        q = 0;
+                    for (int i = 0; i < 2; i++) ra[i] = hit[i] ? __fdividef(1.f, 1.f - al[i]) : 1.f;
+                    const f32x2 ra2 = pack2(ra[0], ra[1]);
+                    if (TS && (tj[0] > 0 || tj[1] > 0)) {
+                        float2 t = unpack2(T2);
+#pragma unroll
+                        for (int i = 0; i < 2; i++) {
+                            float &Ti = i ? t.y : t.x;
+                            if (!hit[i]) continue;
+                            if (tj[i] > 0) {
+                                tj[i]--;
+                                Ti = a.tstore[(size_t)tj[i] * npix + pid[i]];  // T before this Gaussian, as stored
+                            } else {
+                                Ti *= ra[i];
+                            }
+                        }
+                        T2 = pack2(t.x, t.y);
+                    } else {
+                        T2 = mul2(T2, ra2);  // recovered by division (core/cpu/msplat_cpu.cpp:996-997)
                     }
+                    const f32x2 al2 = pack2(al[0], al[1]);
+                    const f32x2 fac2 = mul2(al2, T2);
+                    // gradient arithmetic (no decision depends on it) uses fused
+                    // multiply-adds; the reference's values are met within the gradient
+                    // tolerance, not bit for bit
+                    const f32x2 cv2 = fma2(pack2(B.z, B.z), vr2, fma2(pack2(B.w, B.w), vg2, mul2(pack2(C.x, C.x), vb2)));
+                    const f32x2 nra2 = pack2(-ra[0], -ra[1]);
+                    f32x2 va2 = fma2(T2, cv2, mul2(nra2, add2(bv2, tbv2)));
+                    if (AUX) {
+                        const f32x2 z2 = pack2(C.y, C.y);
+                        // (z T - bd ra) vd + (T - ba ra) vaa
+                        va2 = add2(va2, fma2(fma2(bd2, nra2, mul2(z2, T2)), vd2, mul2(fma2(ba2, nra2, T2), vaa2)));
+                        bd2 = fma2(z2, fac2, bd2);
+                        ba2 = add2(ba2, fac2);
+                        const float2 gd = unpack2(mul2(fac2, vd2));
+                        g[9] = gd.x + gd.y;
+                    }
+                    bv2 = fma2(fac2, cv2, bv2);
+                    // colour gradients; a channel whose raw + 0.5 < 0 passes none, which the
+                    // block's sum applies once per splat
+                    const float2 gr = unpack2(mul2(fac2, vr2)), gg = unpack2(mul2(fac2, vg2)),
+                                 gb = unpack2(mul2(fac2, vb2));
+                    g[5] = gr.x + gr.y;
+                    g[6] = gg.x + gg.y;
+                    g[7] = gb.x + gb.y;
+                    // vs = -alpha v_alpha for the pixels with alpha < 0.999: the xy gradient
+                    // vs (conic d) per pixel (its two terms can cancel, so the sum is not
+                    // factored), and the moments vs dx^2, vs dx dy, vs dy^2 and vs
+                    const f32x2 nal2 = pack2(hit[0] && al[0] < 0.999f ? -al[0] : 0.f,
+                                             hit[1] && al[1] < 0.999f ? -al[1] : 0.f);
+                    const f32x2 vs2 = mul2(nal2, va2), dx2 = pack2(dx, dx), dy2 = pack2(dy[0], dy[1]);
+                    const f32x2 cdy2 = mul2(pack2(A.w, A.w), dy2);
+                    const f32x2 m0 = mul2(vs2, dx2), m1 = mul2(vs2, dy2);
+                    const float2 e0 = unpack2(mul2(vs2, fma2(pack2(B.x, B.x), dy2, pack2(adx, adx)))),
+                                 e1 = unpack2(mul2(vs2, add2(pack2(bdx, bdx), cdy2))), e2 = unpack2(mul2(m0, dx2)),
+                                 e3 = unpack2(mul2(m0, dy2)), e4 = unpack2(mul2(m1, dy2)), e8 = unpack2(vs2);
+                    g[0] = e0.x + e0.y;
+                    g[1] = e1.x + e1.y;
+                    g[2] = e2.x + e2.y;
+                    g[3] = e3.x + e3.y;
+                    g[4] = e4.x + e4.y;
+                    g[8] = e8.x + e8.y;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NG; c++) g[c] = 0.f;
+                }
+                float *row = mypb + q * NG * PB_STRIDE + lane;
+#pragma unroll
+                for (int c = 0; c < NG; c++) row[c * PB_STRIDE] = g[c];
+                pend = (pend << 8) | (uint32_t)j;
+                if (++q == SUB) {
+                    bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BB);
+                    q = 0;
                 }
             }
         }
-        if (q) bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BWD_BATCH);
+        if (q) bwd_warp_sums<NG, SUB>(mypb, red, hitw, pend, q, warp, lane, BB);
         __syncthreads();
-        for (int idx = threadIdx.x; idx < cnt * NG; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < cnt * NG; idx += BWD_THREADS) {
             const int j = idx / NG, c = idx - j * NG;
             const uint32_t m = hitw[j];
-            float s = 0.f, s2nd = 0.f;  // xy: the sums of vs dx and vs dy
-            const int c0 = c < 2 ? 0 : c;
+            float s = 0.f;
 #pragma unroll
             for (int w = 0; w < BWD_WARPS; w++)
-                if ((m >> w) & 1u) {
-                    const float *r = red + (w * BWD_BATCH + j) * NG;
-                    s += r[c0];
-                    if (c < 2) s2nd += r[1];
-                }
+                if ((m >> w) & 1u) s += red[(w * BB + j) * NG + c];
             float out;
-            if (c < 2) {  // v_xy = conic * (sum vs dx, sum vs dy)
-                const float ca = s0[j].z, cb = s0[j].w, cc = s1[j].x;
-                out = c == 0 ? __fmaf_rn(ca, s, cb * s2nd) : __fmaf_rn(cb, s, cc * s2nd);
+            if (c < 2) {
+                out = s;  // v_xy
             } else if (c < 5) {
                 out = 0.5f * s;  // v_conic = (vs dx dx, vs dx dy, vs dy dy) / 2
             } else if (c < 8) {  // the staged colour's sign bit: raw + 0.5 < 0 passes no gradient
@@ -530,7 +593,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         __syncthreads();
     }
     // intersections above every pixel's last contributor get zero slots
-    for (int k = kend + threadIdx.x; k < end; k += blockDim.x) {
+    for (int k = kend + threadIdx.x; k < end; k += BWD_THREADS) {
 #pragma unroll
         for (int c = 0; c < 9; c++) a.slots[(size_t)k * 9 + c] = 0.f;
         if (AUX) a.slots_depth[k] = 0.f;
@@ -538,7 +601,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
 }
 
 template <int BB, int SB, bool AUX = false, bool TS = false>
-__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_kernel(RasterBwdArgs a) {
+__global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_kernel(RasterBwdArgs a) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
     const int tile = blockIdx.x;
@@ -548,7 +611,7 @@ __global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_kernel(RasterBwdArgs a
 // Persistent backward over the tiles of a batch of views, pulling global tile ids
 // from a counter (the forward's counterpart, raster_fwd_batch_kernel).
 template <int BB, int SB>
-__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_batch_kernel(const RasterBwdArgs *views,
+__global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_batch_kernel(const RasterBwdArgs *views,
                                                                         const int *tile_off, int n_views,
                                                                         int *counter) {
     extern __shared__ __align__(16) float4 smem4[];
@@ -575,7 +638,7 @@ __global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_batch_kernel(const Ras
 
 template <int FB>
 void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
-    raster_fwd_kernel<FB><<<T, TILE_PIX, 0, st>>>(a);
+    raster_fwd_kernel<FB><<<T, FWD_THREADS, 0, st>>>(a);
 }
 
 // The aux forward runs the default staging only (the reference too forces one
@@ -583,7 +646,7 @@ void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    raster_fwd_kernel<128, true><<<T, TILE_PIX, 0, st>>>(a);
+    raster_fwd_kernel<128, true><<<T, FWD_THREADS, 0, st>>>(a);
 }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
@@ -605,7 +668,7 @@ void bwd_launch(const RasterBwdArgs &a, int T, cudaStream_t st) {
         return true;
     }();
     (void)attr;
-    raster_bwd_kernel<BB, SB, AUX, TS><<<T, TILE_PIX, smem, st>>>(a);
+    raster_bwd_kernel<BB, SB, AUX, TS><<<T, BWD_THREADS, smem, st>>>(a);
 }
 
 template <int BB, int SB>
@@ -615,9 +678,9 @@ void bwd_batch_launch(const RasterBwdArgs *d_views, const int *d_tile_off, int n
     static const int grid = [] {
         cudaFuncSetAttribute(raster_bwd_batch_kernel<BB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
-        return resident_grid(raster_bwd_batch_kernel<BB, SB>, smem);
+        return resident_grid(raster_bwd_batch_kernel<BB, SB>, smem, BWD_THREADS);
     }();
-    raster_bwd_batch_kernel<BB, SB><<<grid, TILE_PIX, smem, st>>>(d_views, d_tile_off, n_views, d_counter);
+    raster_bwd_batch_kernel<BB, SB><<<grid, BWD_THREADS, smem, st>>>(d_views, d_tile_off, n_views, d_counter);
 }
 
 // The backward variants' (staged batch, reduction sub-batch) pairs, dispatched to
@@ -747,7 +810,7 @@ __device__ __forceinline__ int chunk_tile(const int32_t *first, int T, int i) {
 }
 
 template <int FB>
-__global__ void __launch_bounds__(TILE_PIX) raster_fwd_chunk_kernel(RasterArgs a, ChunkArgs c) {
+__global__ void __launch_bounds__(FWD_THREADS) raster_fwd_chunk_kernel(RasterArgs a, ChunkArgs c) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
@@ -795,7 +858,7 @@ __global__ void __launch_bounds__(TILE_PIX) chunk_merge_kernel(RasterArgs a, Chu
 
 template <int FB>
 void fwd_chunk_launch(const RasterArgs &a, const ChunkArgs &c, int64_t items, cudaStream_t st) {
-    raster_fwd_chunk_kernel<FB><<<(unsigned)items, TILE_PIX, 0, st>>>(a, c);
+    raster_fwd_chunk_kernel<FB><<<(unsigned)items, FWD_THREADS, 0, st>>>(a, c);
 }
 
 void launch_raster_fwd_chunked(const RasterArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,
@@ -841,7 +904,7 @@ __global__ void __launch_bounds__(TILE_PIX) chunk_prefix_kernel(int W, int H, in
 }
 
 template <int BB, int SB>
-__global__ void __launch_bounds__(TILE_PIX, 3) raster_bwd_chunk_kernel(RasterBwdArgs a, ChunkArgs c) {
+__global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_chunk_kernel(RasterBwdArgs a, ChunkArgs c) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
@@ -859,7 +922,7 @@ void bwd_chunk_launch(const RasterBwdArgs &a, const ChunkArgs &c, int64_t items,
         return true;
     }();
     (void)attr;
-    raster_bwd_chunk_kernel<BB, SB><<<(unsigned)items, TILE_PIX, smem, st>>>(a, c);
+    raster_bwd_chunk_kernel<BB, SB><<<(unsigned)items, BWD_THREADS, smem, st>>>(a, c);
 }
 
 void launch_raster_bwd_chunked(const RasterBwdArgs &a, const ChunkArgs &c, int64_t item_cap, cudaStream_t st,

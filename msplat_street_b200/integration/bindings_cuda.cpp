@@ -6,18 +6,23 @@
 // Compiled against the reference's own headers (core/metal/bindings.h and
 // core/include/metal_tensor.hpp, found on the include path; nothing of them is copied
 // here). On non-Apple hosts those MTensors are host blocks, so every call stages its
-// tensors through managed device memory (msplat_cuda_alloc): inputs are copied in,
-// the arrays the call updates are copied back after a synchronisation. That keeps the
-// reference's host-side semantics (callers read data_ptr() after msplat_gpu_sync) at
-// the cost of the copies; a deployment that keeps its tensors on the device calls the
-// C-ABI directly. One context (msplat_cuda_default_ctx) stands in for the reference's
-// process-global frame cache. Errors throw std::runtime_error with the library's
-// message, as the reference throws.
+// tensors through device memory: inputs are copied in on the context's stream, and
+// the arrays the call updates are copied back after the call's work, with one
+// synchronisation at the end. That keeps the reference's host-side semantics (callers
+// read data_ptr() after msplat_gpu_sync) at the cost of the copies; a deployment that
+// keeps its tensors on the device calls the C-ABI directly. The staging buffers
+// persist across calls, one per host tensor (keyed by its host address, grown when the
+// tensor grows), so a training loop allocates device memory only in its first steps
+// and after Model::ensureCapacity; buffers no call has used for STAGE_IDLE_CALLS calls
+// are released. One context (msplat_cuda_default_ctx) stands in for the reference's
+// process-global frame cache; like the reference, this layer is single-threaded.
+// Errors throw std::runtime_error with the library's message, as the reference throws.
 #include "bindings.h"
 
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "msplat_cuda.h"
@@ -31,66 +36,97 @@ void check(int status, const char *what) {
         throw std::runtime_error(std::string("msplat (") + what + "): " + msplat_cuda_last_error());
 }
 
-// A managed-memory copy of a host tensor for the duration of one call; written back
-// to the host tensor when `back` is set.
-class Stage {
-  public:
-    Stage() = default;
-    Stage(MTensor *t, bool back) : host_(t ? t->data_ptr() : nullptr), back_(back) {
-        if (!t || !t->defined()) {
-            host_ = nullptr;
-            return;
-        }
-        bytes_ = t->nbytes();
-        check(msplat_cuda_alloc(bytes_ ? bytes_ : 4, 0, &dev_), "stage");
-        if (bytes_) std::memcpy(dev_, host_, bytes_);
-    }
-    Stage(const Stage &) = delete;
-    Stage &operator=(const Stage &) = delete;
-    Stage(Stage &&o) noexcept : host_(o.host_), dev_(o.dev_), bytes_(o.bytes_), back_(o.back_) { o.dev_ = nullptr; }
-    ~Stage() {
-        if (dev_) msplat_cuda_free(dev_);
-    }
-    // after msplat_cuda_sync
-    void copy_back() {
-        if (dev_ && back_ && bytes_) std::memcpy(host_, dev_, bytes_);
-    }
-    template <typename T>
-    T *ptr() const {
-        return static_cast<T *>(dev_);
-    }
+// Device staging buffers, one per host tensor address, kept across calls.
+constexpr uint64_t STAGE_IDLE_CALLS = 256;
 
-  private:
-    void *host_ = nullptr;
-    void *dev_ = nullptr;
-    size_t bytes_ = 0;
-    bool back_ = false;
+struct StageCache {
+    struct Entry {
+        void *dev = nullptr;
+        size_t bytes = 0;
+        uint64_t last_call = 0;
+    };
+    std::unordered_map<const void *, Entry> map;
+    uint64_t calls = 0;
+
+    void *get(const void *host, size_t bytes) {
+        Entry &e = map[host];
+        if (e.bytes < bytes) {
+            if (e.dev) check(msplat_cuda_free(e.dev), "stage free");
+            e.dev = nullptr;
+            e.bytes = 0;
+            check(msplat_cuda_device_alloc(bytes, &e.dev), "stage alloc");
+            e.bytes = bytes;
+        }
+        e.last_call = calls;
+        return e.dev;
+    }
+    // after a call's synchronisation: release what recent calls have not used
+    void end_call() {
+        calls++;
+        if (calls % STAGE_IDLE_CALLS) return;
+        for (auto it = map.begin(); it != map.end();) {
+            if (calls - it->second.last_call > STAGE_IDLE_CALLS) {
+                msplat_cuda_free(it->second.dev);
+                it = map.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    void clear() {
+        for (auto &kv : map) msplat_cuda_free(kv.second.dev);
+        map.clear();
+    }
 };
 
-// Stages of one call, copied back together after one synchronisation.
+StageCache &cache() {
+    static StageCache c;
+    return c;
+}
+
+// The tensors of one call: each staged once (a tensor passed twice shares its buffer),
+// inputs copied to the device when staged, updated ones copied back in finish().
 struct Staging {
-    std::vector<Stage> st;
+    struct Item {
+        void *host;
+        void *dev;
+        size_t bytes;
+        bool back;
+    };
+    std::vector<Item> items;
+
+    void *stage(MTensor *t, bool back) {
+        if (!t || !t->defined()) return nullptr;
+        void *host = t->data_ptr();
+        const size_t bytes = t->nbytes();
+        for (Item &it : items)
+            if (it.host == host) {
+                it.back = it.back || back;
+                return it.dev;
+            }
+        void *dev = cache().get(host, bytes ? bytes : 4);
+        if (bytes) check(msplat_cuda_copy_buffer(ctx(), dev, host, bytes), "stage in");
+        items.push_back({host, dev, bytes, back});
+        return dev;
+    }
     template <typename T = float>
     T *in(MTensor &t) {
-        st.emplace_back(&t, false);
-        return st.back().ptr<T>();
+        return static_cast<T *>(stage(&t, false));
     }
     template <typename T = float>
     T *inout(MTensor &t) {
-        st.emplace_back(&t, true);
-        return st.back().ptr<T>();
+        return static_cast<T *>(stage(&t, true));
     }
     template <typename T = float>
     T *opt(MTensor *t, bool back) {
-        if (!t || !t->defined()) return nullptr;
-        st.emplace_back(t, back);
-        return st.back().ptr<T>();
+        return static_cast<T *>(stage(t, back));
     }
     void finish() {
+        for (Item &it : items)
+            if (it.back && it.bytes) check(msplat_cuda_copy_buffer(ctx(), it.host, it.dev, it.bytes), "stage out");
         check(msplat_cuda_sync(ctx()), "sync");
-        for (Stage &s : st) s.copy_back();
+        cache().end_call();
     }
-    Staging() { st.reserve(64); }  // stable element addresses while staging
 };
 
 // msplat_cuda_prior over staged copies of a PriorStep's tensors
@@ -145,7 +181,10 @@ unsigned g_last_w = 0, g_last_h = 0;
 
 }  // namespace
 
-void cleanup_msplat_metal() { check(msplat_cuda_cleanup(ctx()), "cleanup"); }
+void cleanup_msplat_metal() {
+    check(msplat_cuda_cleanup(ctx()), "cleanup");
+    cache().clear();
+}
 void *msplat_device() { return nullptr; }
 MTensor gpu_zeros(std::vector<int64_t> shape, DType dtype) { return host_tensor(std::move(shape), dtype); }
 MTensor gpu_empty(std::vector<int64_t> shape, DType dtype) { return host_tensor(std::move(shape), dtype); }
