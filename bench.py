@@ -60,7 +60,7 @@ class ClockSampler:
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
@@ -128,8 +128,10 @@ class ClockSampler:
         mx = [num(r[2]) for r in rows if num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        util = [num(r[9]) for r in rows if len(r) > 9 and num(r[9]) is not None]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows),
+                "gpu_util_pct": statistics.mean(util) if util else None}
 
 
 def dist_setup(args):
@@ -476,13 +478,23 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
             tr.step()
         torch.cuda.synchronize()
         steps = views // per
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            tr.step()
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        if not graph:  # the eager arms report per-view device time by stage (CUDA events)
+            ctx.enable_stage_timing(True)
+            ctx.drain_stage_times()
+        with ClockSampler(torch.cuda.current_device()) as smi:
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                tr.step()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
         out[name] = {"views_per_s": steps * per / dt, "steps_per_s": steps / dt, "ms_per_step": dt / steps * 1e3,
-                     "gaussians": tr.splat_count}
+                     "gaussians": tr.splat_count, "gpu_util_pct": smi.summary().get("gpu_util_pct")}
+        if not graph:
+            st = ctx.drain_stage_times()
+            ctx.enable_stage_timing(False)
+            out[name]["stage_ms_per_view"] = {k: a / max(c, 1) / per for k, (a, c) in st.items()}
+            out[name]["device_ms_per_view"] = sum(out[name]["stage_ms_per_view"].values())
+            out[name]["wall_ms_per_view"] = dt / (steps * per) * 1e3
         if graph:
             out[name]["graph"] = ctx.graph_stats()
         del tr

@@ -85,6 +85,10 @@ int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, in
  * entry that ends it, or to the end), out[1] for the backward (:959-1031: from the
  * pixel's last contributor down). Synchronises the context's stream. */
 int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out);
+/* No counterpart in the reference (test hook). The rasterizers' exponential -- exp(x)
+ * for x in [-700, 0], Tang's table-driven method in double precision, rounded once to
+ * float -- of n device inputs into out, on the context's stream. */
+int msplat_cuda_rasterizer_exp(msplat_cuda_ctx *ctx, const float *x, int64_t n, float *out);
 /* Bytes of device memory the context's caches hold. */
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx);
 

@@ -63,6 +63,7 @@ _SIGS = {
     "msplat_cuda_num_isects": (i64, [vp]),
     "msplat_cuda_frame_pair_counts": (i32, [vp, vp]),
     "msplat_cuda_device_alloc": (i32, [sz, PP]),
+    "msplat_cuda_rasterizer_exp": (i32, [vp, vp, i64, vp]),
     "msplat_cuda_ctx_device_bytes": (i64, [vp]),
     "msplat_cuda_drain_stage_times": (i32, [vp, vp, vp, i32, C.POINTER(i32), vp]),
 }

@@ -1226,6 +1226,13 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss) {
 
 int64_t msplat_cuda_num_isects(msplat_cuda_ctx *ctx) { return ctx ? ctx->n_isect : -1; }
 
+int msplat_cuda_rasterizer_exp(msplat_cuda_ctx *ctx, const float *x, int64_t n, float *out) {
+    if (!ctx || (n > 0 && (!x || !out))) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    launch_exp_tab(x, n, out, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MSPLAT_CUDA_OK;
+}
+
 int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out) {
     if (!ctx || !out) return fail(MSPLAT_CUDA_EINVAL, "null argument");
     out[0] = out[1] = 0;

@@ -41,6 +41,40 @@ __host__ __device__ inline uint32_t num_sh_bases(uint32_t degree) {
 // exp in double, rounded once to float
 __device__ __forceinline__ float exp_ref(float x) { return (float)exp((double)x); }
 
+// The rasterizers' exponential, exp(x) rounded once to float for x = -sigma in
+// [-5.55, 0]: Tang's table-driven method (P. T. P. Tang, ACM TOMS 15(2), 1989) in
+// double precision. x = (64 m + j) ln2 / 64 + r with |r| <= ln2 / 128, so
+// exp(x) = 2^m 2^(j/64) exp(r); exp(r) is its Taylor polynomial of degree 5 (truncation
+// below 3.5e-17 on the interval) and 2^(j/64) comes from a 64-entry table that the
+// block fills once (exp_table_init). The double result is within a few ulps of exp(x),
+// so the float it rounds to equals exp_ref's unless exp(x) lies within about 1e-15 of
+// a float rounding boundary. Valid for x in [-700, 0].
+constexpr double EXP_INV_LN2_64 = 92.33248261689366;    // 64 / ln 2
+constexpr double EXP_LN2_64_HI = 0x1.62e42fefa2000p-7;  // ln 2 / 64 to 40 bits: k * HI is exact
+constexpr double EXP_LN2_64_LO = 0x1.9ef35793c7673p-47; // ln 2 / 64 - HI
+constexpr int EXP_TABLE = 64;
+
+// Every thread of the block calls it; the table is ready after the next barrier.
+__device__ __forceinline__ void exp_table_init(double *t) {
+    for (int j = threadIdx.x; j < EXP_TABLE; j += blockDim.x) t[j] = exp2((double)j * (1.0 / EXP_TABLE));
+}
+
+__device__ __forceinline__ float exp_tab(float xf, const double *t) {
+    const double x = (double)xf;
+    const double k = rint(x * EXP_INV_LN2_64);
+    const int ki = (int)k;
+    double r = fma(-k, EXP_LN2_64_HI, x);
+    r = fma(-k, EXP_LN2_64_LO, r);
+    double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const double v = t[ki & (EXP_TABLE - 1)] * p;
+    const int m = ki >> 6;  // floor(ki / 64): the power of two, added to the exponent field
+    return (float)__hiloint2double(__double2hiint(v) + m * (1 << 20), __double2loint(v));
+}
+
 // Two float32 values in one 64-bit register pair, for sm_100's packed FP32
 // instructions (PTX add / mul / fma .rn.f32x2): one instruction issues two IEEE
 // single-precision operations, each rounded exactly as its scalar form, so packing

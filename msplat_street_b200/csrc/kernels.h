@@ -100,6 +100,8 @@ void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
 // (pixel, Gaussian) pairs the reference's forward / backward loops evaluate over the
 // frame (out[0], out[1]; device counters)
 void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st);
+// the rasterizers' exponential (exp_tab) of n device inputs
+void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st);
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st);
 
 struct RasterBwdArgs;

@@ -100,8 +100,8 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4
 // write the piece's transmittance, colour and last contributor to item `item`.
 template <int FB, bool AUX = false, bool CHUNK = false>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
-                                                float4 *s1, float4 *s2, uint8_t *sm, const ChunkArgs *ck = nullptr,
-                                                int item = 0, int chunk = 0) {
+                                                float4 *s1, float4 *s2, uint8_t *sm, const double *etab,
+                                                const ChunkArgs *ck = nullptr, int item = 0, int chunk = 0) {
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
@@ -128,7 +128,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
             s0[threadIdx.x] = A;
             s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
             // z: the sigma above which alpha = o exp(-sigma) < 1/255 for certain,
-            // ln(255 o) plus a margin far above the roundings of logf, of exp_ref and
+            // ln(255 o) plus a margin far above the roundings of logf, of exp_tab and
             // of the product, so a pixel past it skips the exponential with the
             // decision the exact test would take
             s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, logf(255.f * B.y) + 1e-3f, C.w);
@@ -147,7 +147,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
                 const float dx = A.x - fpx, dy = A.y - fpy;
                 const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
                 if (sigma < 0.f || sigma >= 5.55f || sigma > C.z) continue;
-                const float alpha = fminf(0.999f, B.y * exp_ref(-sigma));
+                const float alpha = fminf(0.999f, B.y * exp_tab(-sigma, etab));
                 if (alpha < 1.f / 255.f) continue;
                 const float nT = T * (1.f - alpha);
                 if (nT <= 1e-4f) {
@@ -210,8 +210,10 @@ template <int FB, bool AUX = false>
 __global__ void __launch_bounds__(FWD_THREADS) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the tile's first barrier
     const int tile = blockIdx.x;
-    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm);
+    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
@@ -224,6 +226,8 @@ __global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_batch_kernel(const 
     __shared__ uint8_t sm[FB];
     __shared__ int s_tile, s_lt;
     __shared__ RasterArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the loop's first barrier
     const int total_tiles = d.tile_off[d.n_views];  // read on the device: the launch is graph-capturable
     for (;;) {
         __syncthreads();  // the previous tile's shared state is no longer read
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_batch_kernel(const 
         __syncthreads();
         const int t = s_tile, lt = s_lt;
         if (t >= total_tiles) break;
-        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2, sm);
+        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2, sm, etab);
     }
 }
 
@@ -346,8 +350,8 @@ __device__ __forceinline__ void bwd_warp_sums(const float *mypb, float *red, uin
 // colour cotangent, so one running scalar replaces the three-channel buffer.
 template <int BB, int SB, bool AUX = false, bool CHUNK = false, bool TS = false>
 __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile, int tx, int ty, float4 *smem4,
-                                                int &kmax, const ChunkArgs *ck = nullptr, int item = 0,
-                                                int chunk = 0) {
+                                                int &kmax, const double *etab, const ChunkArgs *ck = nullptr,
+                                                int item = 0, int chunk = 0) {
     constexpr int NG = AUX ? 10 : 9;
     constexpr int SUB = SB, SUB_OUT = SB * NG;
     static_assert(BB <= BWD_THREADS, "one staging thread per splat");
@@ -473,7 +477,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                         const float va_fast = B.y * __expf(-sigma);
                         float alpha = fminf(0.999f, va_fast);
                         if (fabsf(va_fast - 1.f / 255.f) <= 1e-5f * (1.f / 255.f) || fabsf(va_fast - 0.999f) <= 1e-5f)
-                            alpha = fminf(0.999f, B.y * exp_ref(-sigma));
+                            alpha = fminf(0.999f, B.y * exp_tab(-sigma, etab));
                         if (alpha >= 1.f / 255.f) {
                             hit[i] = true;
                             al[i] = alpha;
@@ -601,11 +605,13 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
 }
 
 template <int BB, int SB, bool AUX = false, bool TS = false>
-__global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_kernel(RasterBwdArgs a) {
+__global__ void __launch_bounds__(BWD_THREADS, BB <= 64 ? 6 : 5) raster_bwd_kernel(RasterBwdArgs a) {
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax;
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the tile's first barrier
     const int tile = blockIdx.x;
-    raster_bwd_tile<BB, SB, AUX, false, TS>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax);
+    raster_bwd_tile<BB, SB, AUX, false, TS>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax, etab);
 }
 
 // Persistent backward over the tiles of a batch of views, pulling global tile ids
@@ -617,6 +623,8 @@ __global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_batch_kernel(const 
     extern __shared__ __align__(16) float4 smem4[];
     __shared__ int kmax, s_tile, s_lt;
     __shared__ RasterBwdArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the loop's first barrier
     const int total_tiles = tile_off[n_views];
     for (;;) {
         if (threadIdx.x == 0) {
@@ -631,7 +639,7 @@ __global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_batch_kernel(const 
         __syncthreads();
         const int t = s_tile, lt = s_lt;
         if (t >= total_tiles) break;
-        raster_bwd_tile<BB, SB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, smem4, kmax);
+        raster_bwd_tile<BB, SB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, smem4, kmax, etab);
         __syncthreads();  // the tile's shared state is free before thread 0 claims the next tile
     }
 }
@@ -737,6 +745,9 @@ void launch_raster_bwd_batch(const RasterBwdArgs *d_views, const int *d_tile_off
 // list's end; rasterize_backward (:959-1031) walks from min(final_idx, end - 1) down
 // to the start. out[0] += forward pairs, out[1] += backward pairs.
 __global__ void __launch_bounds__(TILE_PIX) pair_count_kernel(RasterArgs a, unsigned long long *out) {
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);
+    __syncthreads();
     const int tile = blockIdx.x, tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     int lx, ly;
     tile_pixel(threadIdx.x, lx, ly);
@@ -754,7 +765,7 @@ __global__ void __launch_bounds__(TILE_PIX) pair_count_kernel(RasterArgs a, unsi
             const float dx = A.x - (float)px, dy = A.y - (float)py;
             const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
             if (sigma < 0.f || sigma >= 5.55f) continue;
-            if (fminf(0.999f, B.y * exp_ref(-sigma)) < 1.f / 255.f) continue;
+            if (fminf(0.999f, B.y * exp_tab(-sigma, etab)) < 1.f / 255.f) continue;
             stop = k + 1;
             break;
         }
@@ -769,6 +780,21 @@ __global__ void __launch_bounds__(TILE_PIX) pair_count_kernel(RasterArgs a, unsi
         atomicAdd(out, fwd);
         atomicAdd(out + 1, bwd);
     }
+}
+
+// The rasterizers' exponential over n inputs (test hook for exp_tab against exp_ref).
+__global__ void exp_tab_kernel(const float *x, int64_t n, float *out) {
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = exp_tab(x[i], etab);
+}
+
+void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st) {
+    if (n <= 0) return;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+    exp_tab_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, n, out);
 }
 
 void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st) {
@@ -816,7 +842,9 @@ __global__ void __launch_bounds__(FWD_THREADS) raster_fwd_chunk_kernel(RasterArg
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
     if (item >= c.first[T]) return;  // block-uniform
     const int tile = chunk_tile(c.first, T, item);
-    raster_fwd_tile<FB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, &c, item,
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the tile's first barrier
+    raster_fwd_tile<FB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab, &c, item,
                                      item - c.first[tile]);
 }
 
@@ -910,8 +938,10 @@ __global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_chunk_kernel(Raster
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
     if (item >= c.first[T]) return;  // block-uniform
     const int tile = chunk_tile(c.first, T, item);
-    raster_bwd_tile<BB, SB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax, &c, item,
-                                         item - c.first[tile]);
+    __shared__ double etab[EXP_TABLE];
+    exp_table_init(etab);  // ready after the tile's first barrier
+    raster_bwd_tile<BB, SB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, smem4, kmax, etab, &c,
+                                         item, item - c.first[tile]);
 }
 
 template <int BB, int SB>

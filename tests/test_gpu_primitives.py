@@ -183,3 +183,30 @@ def test_gpu_opacity_reset():
     Context().opacity_reset(to, ta, tb, 1000)
     assert np.array_equal(to.cpu().numpy(), oo)
     assert np.array_equal(ta.cpu().numpy(), aa) and np.array_equal(tb.cpu().numpy(), bb)
+
+
+def test_rasterizer_exponential_matches_double_exp():
+    """The rasterizers' exponential (Tang's table-driven method in double precision,
+    rounded once to float) against CUDA's double exp rounded once (the rounding the
+    kernels used before, which agrees with glibc's expf on 99.98 % of floats): over
+    every float in [-1, 0] and 16 M random ones in [-5.55, -1], equal except where
+    exp(x) sits within ~1e-15 of a float rounding boundary -- then by one ulp."""
+    import ctypes as C
+    from msplat_street_b200 import _lib
+    ctx = Context()
+    one = int(np.float32(1.0).view(np.int32))
+    chunks = [torch.arange(s, min(s + (1 << 26), one + 1), dtype=torch.int32, device="cuda").view(torch.float32).neg()
+              for s in range(0, one + 1, 1 << 26)]
+    chunks.append(torch.from_numpy(np.random.default_rng(0).uniform(-5.55, -1.0, 16 << 20).astype(np.float32)).cuda())
+    worst, differ, total = 0, 0, 0
+    for xt in chunks:
+        got = torch.empty_like(xt)
+        _lib.check(_lib.lib().msplat_cuda_rasterizer_exp(ctx.handle, C.c_void_p(xt.data_ptr()), xt.numel(),
+                                                          C.c_void_p(got.data_ptr())))
+        ref = torch.exp(xt.double()).float()
+        diff = (got.view(torch.int32).long() - ref.view(torch.int32).long()).abs()
+        worst = max(worst, int(diff.max()))
+        differ += int((diff > 0).sum())
+        total += xt.numel()
+    assert worst <= 1
+    assert differ <= max(4, total // 10_000_000), (differ, total)
