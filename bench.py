@@ -497,6 +497,12 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
             out[name]["wall_ms_per_view"] = dt / (steps * per) * 1e3
         if graph:
             out[name]["graph"] = ctx.graph_stats()
+            # the staging autotuner on this arm: every compiled rasterizer variant timed
+            # on the graph-replayed step, interleaved over rounds; the step keeps the best
+            from msplat_street_b200.autotune import tune_raster
+            tuned = tune_raster([ctx], tr.step, warmup=1, reps=4, rounds=2)
+            out[name]["autotune"] = {"best": tuned["best"], "best_staging": tuned["variants"][tuned["best"]],
+                                     "ms_per_step": {str(k): v for k, v in tuned["ms"].items()}}
         del tr
         ctx.close()
         torch.cuda.empty_cache()
@@ -736,7 +742,7 @@ def launches_per_step(n_isect: float, n_gauss: float = 1e5) -> float:
 # DRAM bytes read + written by one launch of the rasterizer backward, from an ncu
 # capture of the street step's first timed launch (1.86 M intersections), and the
 # intersections it processed; the run scales it by its own intersections.
-NCU_RAST_BWD = {"dram_bytes": 16.65e6 + 1.42e6, "isects": 1.86e6}
+NCU_RAST_BWD = {"dram_bytes": 16.66e6 + 0.87e6, "isects": 1.86e6}
 
 SM_COUNT, FP32_LANES = 148, 128
 NPIX = 1024 * 512

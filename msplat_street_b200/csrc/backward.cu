@@ -114,11 +114,16 @@ __device__ __forceinline__ void cov3d_vjp(V3 sc, float gs, Q4 q, const float *gc
 
 
 // Sums of the 9 raster-backward values over each visible Gaussian's intersection
-// slots, in sorted (tile) order. A Gaussian may cover hundreds of tiles, so the warp
-// sums each of its visible Gaussians together: lane l takes the intersections l,
-// l+32, ... and a fixed butterfly combines the lanes. g0 = index of the warp's first
-// Gaussian in offsets / n_tiles; s9 is zero for invisible Gaussians. With
-// slots_depth (aux mode) the depth slots are summed the same way into *sd.
+// slots, in sorted (tile) order. Most Gaussians cover a few tiles: each lane sums its
+// own Gaussian's slots one after another, so the lanes' independent loads overlap.
+// A Gaussian covering more than SLOT_LANE_MAX tiles (near the camera: hundreds) is
+// summed by the whole warp afterwards: lane l takes its intersections l, l+32, ... and
+// a fixed butterfly combines the lanes. Both orders are fixed, so the sums do not
+// depend on scheduling. g0 = index of the warp's first Gaussian in offsets / n_tiles;
+// s9 is zero for invisible Gaussians. With slots_depth (aux mode) the depth slots are
+// summed the same way into *sd.
+constexpr int SLOT_LANE_MAX = 64;
+
 __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64_t *offsets, const int32_t *n_tiles,
                                                const int32_t *inv, const float *slots, float s9[9],
                                                const float *slots_depth = nullptr, float *sd = nullptr) {
@@ -128,13 +133,22 @@ __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64
     if (sd) *sd = 0.f;
     long long my_e0 = 0;
     int my_cnt = 0;
-    if (vis) {  // each lane loads its own Gaussian's range once; the loop shuffles it
+    if (vis) {
         my_e0 = offsets[g0 + lane];
         my_cnt = n_tiles[g0 + lane];
     }
-    const unsigned vis_mask = __ballot_sync(0xffffffffu, vis);
-    for (int gl = 0; gl < 32; gl++) {
-        if (!((vis_mask >> gl) & 1u)) continue;  // warp-uniform
+    if (vis && my_cnt <= SLOT_LANE_MAX) {
+        for (int j = 0; j < my_cnt; j++) {
+            const int32_t k = inv[my_e0 + j];
+            const float *sl = slots + (size_t)k * 9;
+#pragma unroll
+            for (int c = 0; c < 9; c++) s9[c] += sl[c];
+            if (slots_depth) *sd += slots_depth[k];
+        }
+    }
+    const unsigned big = __ballot_sync(0xffffffffu, vis && my_cnt > SLOT_LANE_MAX);
+    for (unsigned bits = big; bits; bits &= bits - 1u) {  // warp-uniform
+        const int gl = __ffs(bits) - 1;
         const long long e0 = __shfl_sync(0xffffffffu, my_e0, gl);
         const int cnt = __shfl_sync(0xffffffffu, my_cnt, gl);
         float p[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, pd = 0.f;
