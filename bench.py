@@ -476,6 +476,13 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
         per = views_per_step if batched else 1
         for _ in range(max(warmup_views // per, 3)):
             tr.step()
+        tuned = None
+        if graph:
+            # the staging autotuner on this arm before it is timed: every compiled
+            # rasterizer variant timed on the graph-replayed step, interleaved over
+            # rounds; the step keeps the best
+            from msplat_street_b200.autotune import tune_raster
+            tuned = tune_raster([ctx], tr.step, warmup=1, reps=4, rounds=2)
         torch.cuda.synchronize()
         steps = views // per
         if not graph:  # the eager arms report per-view device time by stage (CUDA events)
@@ -497,10 +504,6 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
             out[name]["wall_ms_per_view"] = dt / (steps * per) * 1e3
         if graph:
             out[name]["graph"] = ctx.graph_stats()
-            # the staging autotuner on this arm: every compiled rasterizer variant timed
-            # on the graph-replayed step, interleaved over rounds; the step keeps the best
-            from msplat_street_b200.autotune import tune_raster
-            tuned = tune_raster([ctx], tr.step, warmup=1, reps=4, rounds=2)
             out[name]["autotune"] = {"best": tuned["best"], "best_staging": tuned["variants"][tuned["best"]],
                                      "ms_per_step": {str(k): v for k, v in tuned["ms"].items()}}
         del tr

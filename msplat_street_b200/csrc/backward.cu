@@ -193,7 +193,8 @@ __device__ __forceinline__ void projection_vjp(const CamParams &cam, const float
     float gc2[3];
     conic_vjp(V3{sp0.z, sp0.w, sp1.x}, V3{s9[2], s9[3], s9[4]}, gc2);
     V3 ls = ld3(scales, i);
-    V3 es{exp_ref(ls.x), exp_ref(ls.y), exp_ref(ls.z)};
+    // gradient arithmetic: single-precision exp (within 2 ulps) is enough here
+    V3 es{expf(ls.x), expf(ls.y), expf(ls.z)};
     const float4 qq = reinterpret_cast<const float4 *>(quats)[i];
     Q4 q{qq.x, qq.y, qq.z, qq.w};
     float cov[6];
@@ -237,7 +238,7 @@ __device__ __forceinline__ void sh_rest_basis(V3 d, float *bs) {
 constexpr int BWD_THREADS = 256;
 constexpr int MAX_REST = 15;  // SH bases beyond DC that the backward updates (degree <= 3)
 
-__global__ void __launch_bounds__(BWD_THREADS) backward_adam_kernel(BackwardArgs a) {
+__global__ void __launch_bounds__(BWD_THREADS, 4) backward_adam_kernel(BackwardArgs a) {
     __shared__ float s_basis[BWD_THREADS][MAX_REST + 1];
     __shared__ float s_vrgb[BWD_THREADS][3];
     __shared__ int s_vis[BWD_THREADS];

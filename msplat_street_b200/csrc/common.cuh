@@ -61,8 +61,11 @@ __device__ __forceinline__ void exp_table_init(double *t) {
 
 __device__ __forceinline__ float exp_tab(float xf, const double *t) {
     const double x = (double)xf;
-    const double k = rint(x * EXP_INV_LN2_64);
-    const int ki = (int)k;
+    // k = round(x 64 / ln 2): adding 1.5 * 2^52 leaves the rounded integer in the low
+    // word of the sum (exact for |k| < 2^31)
+    const double shifted = fma(x, EXP_INV_LN2_64, 0x1.8p52);
+    const int ki = __double2loint(shifted);
+    const double k = shifted - 0x1.8p52;
     double r = fma(-k, EXP_LN2_64_HI, x);
     r = fma(-k, EXP_LN2_64_LO, r);
     double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);

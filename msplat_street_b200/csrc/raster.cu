@@ -98,7 +98,7 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4
 // (rasterize_forward_aux, core/cpu/msplat_cpu.cpp:574-626 with f.aux).
 // CHUNK: composite only piece `chunk` of the list (ck->chunk_len long) from T = 1 and
 // write the piece's transmittance, colour and last contributor to item `item`.
-template <int FB, bool AUX = false, bool CHUNK = false>
+template <int FB, bool AUX = false, bool CHUNK = false, bool TS = false>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
                                                 float4 *s1, float4 *s2, uint8_t *sm, const double *etab,
                                                 const ChunkArgs *ck = nullptr, int item = 0, int chunk = 0) {
@@ -155,7 +155,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
                     done = true;
                     break;
                 }
-                if (a.tstore) {
+                if (TS) {
                     if (stored < a.tcap) a.tstore[(size_t)stored * npix + pid] = T;
                     stored++;
                 }
@@ -181,7 +181,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     }
     if (a.final_T) a.final_T[pid] = T;
     if (a.final_idx) a.final_idx[pid] = last;
-    if (a.tcount) a.tcount[pid] = stored <= a.tcap ? stored : -1;
+    if (TS) a.tcount[pid] = stored <= a.tcap ? stored : -1;
     float *o = a.out_img + 3 * (size_t)pid;
     if (AUX) {
         float *bp = a.bg_img + 3 * (size_t)pid;
@@ -206,14 +206,14 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     o[2] = clamp01(a.bg[2] * T + cb);
 }
 
-template <int FB, bool AUX = false>
-__global__ void __launch_bounds__(FWD_THREADS) raster_fwd_kernel(RasterArgs a) {
+template <int FB, bool AUX = false, bool TS = false>
+__global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_kernel(RasterArgs a) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     __shared__ double etab[EXP_TABLE];
     exp_table_init(etab);  // ready after the tile's first barrier
     const int tile = blockIdx.x;
-    raster_fwd_tile<FB, AUX>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab);
+    raster_fwd_tile<FB, AUX, false, TS>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
@@ -654,12 +654,17 @@ void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    raster_fwd_kernel<128, true><<<T, FWD_THREADS, 0, st>>>(a);
+    if (a.tstore) raster_fwd_kernel<128, true, true><<<T, FWD_THREADS, 0, st>>>(a);
+    else raster_fwd_kernel<128, true><<<T, FWD_THREADS, 0, st>>>(a);
 }
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
+    if (a.tstore) {  // stored-transmittance mode: the default staging only
+        raster_fwd_kernel<128, false, true><<<T, FWD_THREADS, 0, st>>>(a);
+        return;
+    }
     switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
         case 64: fwd_launch<64>(a, T, st); break;
         case 256: fwd_launch<256>(a, T, st); break;
@@ -836,7 +841,7 @@ __device__ __forceinline__ int chunk_tile(const int32_t *first, int T, int i) {
 }
 
 template <int FB>
-__global__ void __launch_bounds__(FWD_THREADS) raster_fwd_chunk_kernel(RasterArgs a, ChunkArgs c) {
+__global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_chunk_kernel(RasterArgs a, ChunkArgs c) {
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;

@@ -373,14 +373,17 @@ __device__ __forceinline__ unsigned digit_peers(int d) {
     return m;
 }
 
+// Counting needs no ranks: each warp adds its keys' digits to its own shared-memory
+// histogram with one atomic per key (lanes of a warp that share a digit are resolved
+// by the shared-memory atomic unit), and the block sums the warps' histograms.
 template <typename K, int SORT_ITEMS>
 __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shift, uint32_t mask, uint32_t *counts,
                                   int nb) {
-    __shared__ uint32_t h[RADIX];
+    __shared__ uint32_t h[SORT_WARPS][RADIX];
     if (d_n) n = min(n, *d_n);
-    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = 0;
+    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
     const int base = blockIdx.x * SORT_TILE;
     int dig[SORT_ITEMS];
@@ -390,13 +393,15 @@ __global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shif
         dig[j] = k < n ? (int)((keys[k] >> shift) & mask) : RADIX;
     }
 #pragma unroll
-    for (int j = 0; j < SORT_ITEMS; j++) {
-        const int d = dig[j];
-        const unsigned peers = digit_peers(d);
-        if (d < RADIX && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
-    }
+    for (int j = 0; j < SORT_ITEMS; j++)
+        if (dig[j] < RADIX) atomicAdd(&h[warp][dig[j]], 1u);
     __syncthreads();
-    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) counts[(size_t)i * nb + blockIdx.x] = h[i];
+    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int w = 0; w < SORT_WARPS; w++) s += h[w][i];
+        counts[(size_t)i * nb + blockIdx.x] = s;
+    }
 }
 
 // counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
