@@ -412,6 +412,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         if (inside[i]) atomicMax(&kmax, min(kf[i], end - 1));
     __syncthreads();
     const int kend = kmax + 1;  // nothing at or above kend contributes to any pixel
+    // nothing above wkf contributes to this warp's pixels: the warp skips those splats
+    const int wkf = __reduce_max_sync(0xffffffffu, max(inside[0] ? kf[0] : start - 1, inside[1] ? kf[1] : start - 1));
     // packed per-pixel state: (row y, row y + 4)
     f32x2 T2 = pack2(T[0], T[1]), bv2 = pack2(bv[0], bv[1]);
     const f32x2 tbv2 = pack2(tbv[0], tbv[1]), vr2 = pack2(vr[0], vr[1]), vg2 = pack2(vg[0], vg[1]),
@@ -449,7 +451,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
         uint32_t pend = 0;  // their staged indices, 8 bits each, the newest lowest
         for (int c32 = (cnt - 1) >> 5; c32 >= 0; c32--) {
             const int jl = (c32 << 5) + lane;
-            uint32_t bits = __ballot_sync(0xffffffffu, jl < cnt && ((sm[jl] >> warp) & 1u));
+            uint32_t bits = __ballot_sync(0xffffffffu, jl < cnt && b_start + jl <= wkf && ((sm[jl] >> warp) & 1u));
             while (bits) {
                 const int hb = 31 - __clz(bits);
                 bits &= ~(1u << hb);

@@ -32,3 +32,23 @@ def test_reference_gradcheck_passes_on_this_backend():
     for line in runs:
         got, total = line.split("gradients match")[0].split()[-1].split("/")
         assert got == total, line
+
+
+TRAIN_BIN = os.path.join(os.path.dirname(BIN), "train_bindings")
+
+
+@pytest.mark.skipif(not os.path.exists(TRAIN_BIN), reason="train_bindings not built (needs the reference headers)")
+def test_training_through_bindings_h_with_host_tensors():
+    """integration/train_bindings.cpp trains the small plain config through bindings.h
+    with host tensors, as the reference's Model / CLI hold them: every call stages its
+    tensors through the persistent device buffers and back. It must run, report its
+    throughput, and its loss must fall from the first steps to the last."""
+    import json
+    first = subprocess.run([TRAIN_BIN, "2", "0"], capture_output=True, text=True, timeout=300)
+    last = subprocess.run([TRAIN_BIN, "150", "0"], capture_output=True, text=True, timeout=300)
+    for r in (first, last):
+        assert r.returncode == 0, r.stdout + r.stderr
+    a = json.loads(first.stdout.strip().splitlines()[-1])
+    b = json.loads(last.stdout.strip().splitlines()[-1])
+    assert b["iters_per_s"] > 0 and b["steps"] == 150
+    assert b["final_loss"] < a["final_loss"], (a, b)
