@@ -421,20 +421,22 @@ def bindings_report(dev, steps: int = 300, warmup: int = 10) -> dict:
     """Training-step throughput on the small plain config (10k Gaussians, 256x256)
     through bindings.h with host tensors -- the path core/src/model.cpp and the CLI take
     (msplat_street_b200/_build/train_bindings, wall clock, every call staging its
-    tensors to the device and back) -- next to the same step through the Python API
-    with device-resident tensors (CUDA events)."""
+    tensors to the device and back) -- next to the same training from C++ straight
+    through the C-ABI with device-resident tensors (the same binary, mode c_abi, wall
+    clock) and through the Python API (CUDA events)."""
     import torch
     from msplat_street_b200 import build, scenes
     from msplat_street_b200.backend import AdamState, Context, GaussianParams
     from msplat_street_b200.trainer import LR_INIT
     out = {"config": "10k Gaussians, 256x256, SH degree 3, L1 + 0.2 SSIM, Adam"}
-    if os.path.exists(build.TRAIN_BINDINGS):
-        r = subprocess.run([build.TRAIN_BINDINGS, str(steps), str(warmup)], capture_output=True, text=True,
-                           timeout=300)
-        line = [x for x in r.stdout.splitlines() if x.startswith("{")]
-        out["bindings_h"] = json.loads(line[-1]) if r.returncode == 0 and line else {"error": r.stderr[-300:]}
-    else:
-        out["bindings_h"] = {"error": "train_bindings not built (needs the reference headers at build time)"}
+    for mode in ("bindings_h", "c_abi"):
+        if os.path.exists(build.TRAIN_BINDINGS):
+            r = subprocess.run([build.TRAIN_BINDINGS, str(steps), str(warmup), mode], capture_output=True, text=True,
+                               timeout=300)
+            line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out[mode] = json.loads(line[-1]) if r.returncode == 0 and line else {"error": r.stderr[-300:]}
+        else:
+            out[mode] = {"error": "train_bindings not built (needs the reference headers at build time)"}
     ctx = Context()
     cam = scenes.small_camera()
     bg = np.array([0.6130, 0.0101, 0.3984], np.float32)
@@ -909,10 +911,11 @@ def knn_rate(trainer, ctx, reps: int = 5) -> dict:
 PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")
 
 
-def profile_case(name: str, dev) -> dict:
-    """One stage at a size larger than the 126 MB L2, run twice (the second launch is
-    the one an ncu capture takes with -s 1 -c 1 on the stage's kernel), for the DRAM
-    traffic and achieved bandwidth of that kernel:
+def profile_case(name: str, dev, runs: int = 2) -> dict:
+    """One stage at a size larger than the 126 MB L2, run `runs` times (default twice:
+    the second launch is the one an ncu capture takes with -s 1 -c 1 on the stage's
+    kernel), for the DRAM traffic and achieved bandwidth of that kernel; "stage_ms" holds
+    the context's CUDA-event stage times per run over the runs after the first:
       sort     stable radix sort of 32 M (u64 key, i32 value) pairs, 40 key bits (5 passes)
       ssim     fused L1 + SSIM forward and backward of a 4096 x 4096 render
       adam     backward/Adam of a training step over 1 M Gaussians (SH degree 3)
@@ -926,18 +929,35 @@ def profile_case(name: str, dev) -> dict:
     ctx = Context()
     g = torch.Generator(device=dev).manual_seed(7)
     out = {"case": name}
+    runs = max(2, runs)
+
+    walls = []
+
+    def timed(it):  # stage timing from the second run on; wall time of each run
+        torch.cuda.synchronize()
+        if walls and walls[-1] < 0:
+            walls[-1] += time.perf_counter()
+        if it == 1:
+            ctx.enable_stage_timing(True)
+            ctx.drain_stage_times()
+        walls.append(-time.perf_counter())
+        return it
+
     if name == "sort":
         n = 32 << 20
-        for _ in range(2):
-            keys = torch.randint(0, 1 << 40, (n,), device=dev, dtype=torch.int64, generator=g)
+        src = torch.randint(0, 1 << 40, (n,), device=dev, dtype=torch.int64, generator=g)
+        for it in range(runs):
+            keys = src.clone()
             vals = torch.arange(n, device=dev, dtype=torch.int32)
+            timed(it)
             ctx.radix_sort(keys, vals, 40)
         out.update(pairs=n, key_bits=40, bytes_per_pair_pass=24)
     elif name == "ssim":
         h = w = 4096
         img = torch.rand((h, w, 3), device=dev, generator=g)
         gt = torch.rand((h, w, 3), device=dev, generator=g)
-        for _ in range(2):
+        for it in range(runs):
+            timed(it)
             loss = autograd.ssim_l1_loss(img.requires_grad_(), gt)
             loss.backward()
             img.grad = None
@@ -949,7 +969,8 @@ def profile_case(name: str, dev) -> dict:
         gt_img = torch.rand((512, 512, 3), device=dev, generator=g)
         adam = AdamState.zeros_like(p, [1.6e-4, 5e-3, 1e-3, 2.5e-3, 1.25e-4, 0.05])
         stats = tuple(torch.zeros(n, device=dev) for _ in range(3))
-        for _ in range(2):
+        for it in range(runs):
+            timed(it)
             ctx.train_step(p, adam, cam, np.zeros(3, np.float32), gt_img, stats)
         torch.cuda.synchronize()
         vis = int((ctx.frame("radii") > 0).sum())
@@ -959,7 +980,7 @@ def profile_case(name: str, dev) -> dict:
         n, cap = 500_000, 2_000_000  # room for every Gaussian to be split and cloned
         src = scenes.random_gaussians(n, 4, log_scale_mean=-4.0, log_scale_std=1.5)
         strides = [3, 3, 4, 3, 45, 1]
-        for _ in range(2):
+        for it in range(runs):
             bufs = []
             for a, st in zip(src.arrays(), strides):
                 b = torch.zeros((cap, st), device=dev)
@@ -970,6 +991,7 @@ def profile_case(name: str, dev) -> dict:
             gn = torch.rand(n, device=dev, generator=g) * 4e-3
             vc = torch.randint(1, 4, (n,), device=dev, generator=g).float()
             ms = torch.rand(n, device=dev, generator=g) * 0.3
+            timed(it)
             new_n = ctx.densify(n, bufs, m1, m2, gn, vc, ms, 512.0, 1234)
         out.update(gaussians=n, capacity=cap, new_gaussians=new_n, floats_per_gaussian=59, arrays=3)
     elif name == "render":
@@ -978,11 +1000,18 @@ def profile_case(name: str, dev) -> dict:
         from msplat_street_b200.workloads import BACKGROUND
         p = serving.random_scene_tensors(3_000_000, 7, device=dev)
         cam = scenes.sphere_camera(np.random.default_rng(3), 1920, 1080, radius=5.0)
-        for _ in range(2):
+        for it in range(runs):
+            timed(it)
             ctx.render_batch([BatchItem(p, cam, BACKGROUND)])
         torch.cuda.synchronize()
         out.update(gaussians=3_000_000, resolution="1920x1080", isects=ctx.num_isects())
     torch.cuda.synchronize()
+    if walls and walls[-1] < 0:
+        walls[-1] += time.perf_counter()
+    out["run_wall_ms"] = [round(1e3 * w, 3) for w in walls]
+    st = ctx.drain_stage_times()
+    ctx.enable_stage_timing(False)
+    out["stage_ms"] = {k: round(v[0] / max(1, runs - 1), 4) for k, v in st.items() if v[1] > 0}
     return out
 
 
@@ -998,10 +1027,11 @@ def main(argv=None):
     ap.add_argument("--no-batching", action="store_true", help="skip the batched-training report")
     ap.add_argument("--profile-case", choices=PROFILE_CASES,
                     help="run one stage at a size larger than L2 (for an ncu capture) and exit")
+    ap.add_argument("--case-runs", type=int, default=2, help="runs of the --profile-case stage (at least 2)")
     args = ap.parse_args(argv)
     if args.profile_case:
         import torch
-        print(json.dumps(profile_case(args.profile_case, torch.device("cuda", 0))))
+        print(json.dumps(profile_case(args.profile_case, torch.device("cuda", 0), args.case_runs)))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

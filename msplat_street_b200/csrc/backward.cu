@@ -233,6 +233,85 @@ __device__ __forceinline__ void sh_rest_basis(V3 d, float *bs) {
     bs[14] = SH_C3_6 * x * (xx - 3.f * yy);
 }
 
+// Adam over the SH-rest rows of a warp's Gaussians (rows of `stride` floats starting at
+// p, m1, m2), walked as one flat range of rows x stride floats: every access of the
+// warp covers 32 consecutive floats, and each lane loads its U elements before it
+// updates any, so the loads of a row block overlap instead of following one row at a
+// time. grad(r, e) is the gradient of float e of row r; rows with vis[r] == 0 and
+// floats e >= used keep their values. Each element gets the same adam_step as in the
+// row-by-row walk.
+template <int U, typename Grad>
+__device__ __forceinline__ void warp_rest_adam(float *__restrict__ p, float *__restrict__ m1,
+                                               float *__restrict__ m2, int rows, int stride, int used,
+                                               const int *vis, Grad grad, float ss, float b1, float b2, float bc2,
+                                               float eps) {
+    if (stride <= 0 || rows <= 0) return;
+    const int lane = threadIdx.x & 31;
+    const int total = rows * stride;
+    int r = 0, e = lane;  // row and float of this lane's next element
+    while (e >= stride) {
+        e -= stride;
+        r++;
+    }
+    for (int j0 = 0; j0 < total; j0 += 32 * U) {
+        float pv[U], v1[U], v2[U];
+        int rr[U], ee[U];
+        bool up[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int j = j0 + u * 32 + lane;
+            rr[u] = r;
+            ee[u] = e;
+            up[u] = j < total && e < used && vis[r] != 0;  // vis[r] read only for j < total
+            if (up[u]) {
+                pv[u] = p[j];
+                v1[u] = m1[j];
+                v2[u] = m2[j];
+            }
+            e += 32;
+            while (e >= stride) {
+                e -= stride;
+                r++;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (up[u]) {
+                const int j = j0 + u * 32 + lane;
+                adam_step(pv[u], v1[u], v2[u], grad(rr[u], ee[u]), ss, b1, b2, bc2, eps);
+                p[j] = pv[u];
+                m1[j] = v1[u];
+                m2[j] = v2[u];
+            }
+        }
+    }
+}
+
+// Writes a warp's SH-rest gradient rows (gradient-only mode) as one flat range:
+// grad(r, e) where e < used and row r is visible (every row when vis is null), else 0.
+template <typename Grad>
+__device__ __forceinline__ void warp_rest_grad(float *__restrict__ out, int rows, int stride, int used,
+                                               const int *vis, Grad grad) {
+    if (stride <= 0 || rows <= 0) return;
+    const int lane = threadIdx.x & 31;
+    const int total = rows * stride;
+    int r = 0, e = lane;
+    while (e >= stride) {
+        e -= stride;
+        r++;
+    }
+    for (int j = lane; j < total; j += 32) {
+        out[j] = (e < used && (vis == nullptr || vis[r] != 0)) ? grad(r, e) : 0.f;
+        e += 32;
+        while (e >= stride) {
+            e -= stride;
+            r++;
+        }
+    }
+}
+
+constexpr int REST_UNROLL = 4;
+
 }  // namespace
 
 constexpr int BWD_THREADS = 256;
@@ -355,29 +434,18 @@ __global__ void __launch_bounds__(BWD_THREADS, 4) backward_adam_kernel(BackwardA
     const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;  // its Gaussian
     const int stride = a.rest_stride;
     const int used = 3 * active;  // floats of each row that get a gradient
+    const int rows = (int)min((int64_t)32, (int64_t)a.n - g0);
+    const size_t off = (size_t)g0 * stride;
+    auto grad = [&](int r, int e) {
+        const int base = e / 3;
+        return s_basis[wbase_t + r][base] * s_vrgb[wbase_t + r][e - 3 * base];
+    };
     if (a.g_rest) {  // gradient-only mode: every row, zero where invisible or inactive
-        for (int gl = 0; gl < 32; gl++) {
-            if (g0 + gl >= a.n) break;
-            const bool gv = s_vis[wbase_t + gl] != 0;
-            float *gr = a.g_rest + (size_t)(g0 + gl) * stride;
-            const float *bs = s_basis[wbase_t + gl], *vc = s_vrgb[wbase_t + gl];
-            for (int j = lane; j < stride; j += 32) {
-                const int base = j / 3, c = j - base * 3;
-                gr[j] = (gv && j < used) ? bs[base] * vc[c] : 0.f;
-            }
-        }
+        warp_rest_grad(a.g_rest + off, rows, stride, used, s_vis + wbase_t, grad);
         return;
     }
-    for (int gl = 0; gl < 32; gl++) {  // one Gaussian's row at a time (warp-uniform)
-        if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
-        const size_t off = (size_t)(g0 + gl) * stride;
-        float *rest = a.p[4] + off, *r1 = a.m1[4] + off, *r2 = a.m2[4] + off;
-        const float *bs = s_basis[wbase_t + gl], *vc = s_vrgb[wbase_t + gl];
-        for (int j = lane; j < used; j += 32) {
-            const int base = j / 3, c = j - base * 3;
-            adam_step(rest[j], r1[j], r2[j], bs[base] * vc[c], a.ss[4], b1, b2, a.bc2[4], eps);
-        }
-    }
+    warp_rest_adam<REST_UNROLL>(a.p[4] + off, a.m1[4] + off, a.m2[4] + off, rows, stride, used, s_vis + wbase_t, grad,
+                                a.ss[4], b1, b2, a.bc2[4], eps);
 }
 
 void launch_backward_adam(const BackwardArgs &a, cudaStream_t st) {
@@ -495,22 +563,15 @@ __global__ void __launch_bounds__(BWD_THREADS) backward_adam_batch_kernel(Backwa
     const int wbase_t = threadIdx.x - lane;
     const int64_t g0 = (int64_t)blockIdx.x * BWD_THREADS + wbase_t;
     const int stride = a.rest_stride;
-    if (a.g[4]) {
-        for (int gl = 0; gl < 32; gl++) {
-            if (g0 + gl >= a.n) break;
-            float *gr = a.g[4] + (size_t)(g0 + gl) * stride;
-            const float *src = s_grest[wbase_t + gl];
-            for (int j = lane; j < stride; j += 32) gr[j] = j < used ? src[j] : 0.f;
-        }
+    const int rows = (int)min((int64_t)32, (int64_t)a.n - g0);
+    const size_t off = (size_t)g0 * stride;
+    auto grad = [&](int r, int e) { return s_grest[wbase_t + r][e]; };
+    if (a.g[4]) {  // every row: the summed gradient where used (zero where no view saw it)
+        warp_rest_grad(a.g[4] + off, rows, stride, used, nullptr, grad);
     }
     if (!a.do_adam || active == 0) return;
-    for (int gl = 0; gl < 32; gl++) {
-        if (g0 + gl >= a.n || !s_vis[wbase_t + gl]) continue;
-        const size_t off = (size_t)(g0 + gl) * stride;
-        float *rest = a.p[4] + off, *r1 = a.m1[4] + off, *r2 = a.m2[4] + off;
-        const float *src = s_grest[wbase_t + gl];
-        for (int j = lane; j < used; j += 32) adam_step(rest[j], r1[j], r2[j], src[j], ss[4], b1, b2, bc2[4], eps);
-    }
+    warp_rest_adam<REST_UNROLL>(a.p[4] + off, a.m1[4] + off, a.m2[4] + off, rows, stride, used, s_vis + wbase_t, grad,
+                                ss[4], b1, b2, bc2[4], eps);
 }
 
 void launch_backward_adam_batch(const BackwardBatchArgs &a, cudaStream_t st) {

@@ -339,33 +339,42 @@ void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const
 // 32- and 64-bit keys.
 
 constexpr int RADIX = 256;
-// Keys per block: SORT_THREADS x ITEMS. Large sorts take 16 items a thread (4096 keys
-// a block): each digit's run in a block then averages 16 entries, so the scatter's
-// stores come in runs of 64 bytes or more, and the per-block digit counts (256 per
-// block, scanned every pass) stay small next to the keys. Below LARGE_SORT keys, 8
-// items (2048 keys a block) keep enough blocks to fill the GPU; 64-bit keys always
-// take 8 (16 would need 48 KB of staging per block and halve the resident blocks).
-constexpr int SORT_THREADS = 256, SORT_WARPS = SORT_THREADS / 32;
+// Keys per block: THREADS x ITEMS. Large sorts of 32-bit keys take 256 threads x 16
+// items (4096 keys a block): each digit's run in a block then averages 16 entries, so
+// the scatter's stores come in runs of 64 bytes or more, and the per-block digit counts
+// (256 per block, scanned every pass) stay small next to the keys. Below LARGE_SORT
+// keys, 256 x 8 (2048 keys a block) keeps enough blocks to fill the GPU; 64-bit keys
+// take 2048-key blocks too (4096 would need 48 KB of staging per block). Measured and
+// not kept: 512 x 8 and 1024 x 4 blocks for the large 32-bit sort (two and one blocks
+// per SM: the 46 M-key tile sort of a 1080p frame 1.06 and 1.51 ms against 1.02), and
+// the largest shared-memory carveout (1.06 ms: the scatter's loads and stores want
+// the L1). The scatter is bound by its integer pipe (ALU 64 % of peak, issue 54 %):
+// the ranking's ballots, not DRAM, set its pace.
+constexpr int SORT_THREADS = 256;
 constexpr int LARGE_SORT = 4 << 20;
+constexpr int MAX_SORT_THREADS = 1024;
 
 // Up to this many blocks (131,072 keys at 2048 a block, the depth order of a training
 // view), each scatter block sums the per-block digit counts itself instead of a
 // separate scan launch over them.
 constexpr int DIRECT_SORT_BLOCKS = 64;
 
-int sort_items(int n, int key_bytes) { return key_bytes == 4 && n >= LARGE_SORT ? 16 : 8; }
-// The most blocks any sort of up to n keys uses (scratch sizing): 2048-key blocks.
-int radix_max_blocks(int n) { return (n + SORT_THREADS * 8 - 1) / (SORT_THREADS * 8); }
+// The most blocks any sort of up to n keys uses (scratch sizing): 2048-key blocks,
+// the smallest of every block shape below.
+int radix_max_blocks(int n) { return (n + 2047) / 2048; }
 
 // d_n (may be null): a device-side count that caps n (capacity-bounded launches)
 // The lanes of the warp whose digit equals this lane's (d in 0..RADIX, RADIX marking
 // a lane with no key): nine ballots, one per bit of d, each narrowing the set to the
 // lanes that agree on that bit. Constant cost whatever the number of distinct digits
 // in the warp (a warp of scattered tile ids holds up to 32).
-__device__ __forceinline__ unsigned digit_peers(int d) {
+// Only the bits a pass's digits can hold take a ballot (mask, uniform), and the no-key
+// bit only in a block that is not full (full: every lane holds a key).
+__device__ __forceinline__ unsigned digit_peers(int d, uint32_t mask, bool full) {
     unsigned m = 0xffffffffu;
 #pragma unroll
     for (int b = 0; b < 9; b++) {
+        if (b < 8 ? !((mask >> b) & 1u) : full) continue;  // uniform
         const bool on = (d >> b) & 1;
         const unsigned bal = __ballot_sync(0xffffffffu, on);
         m &= on ? bal : ~bal;
@@ -376,69 +385,77 @@ __device__ __forceinline__ unsigned digit_peers(int d) {
 // Counting needs no ranks: each warp adds its keys' digits to its own shared-memory
 // histogram with one atomic per key (lanes of a warp that share a digit are resolved
 // by the shared-memory atomic unit), and the block sums the warps' histograms.
-template <typename K, int SORT_ITEMS>
-__global__ void radix_hist_kernel(const K *keys, int n, const int *d_n, int shift, uint32_t mask, uint32_t *counts,
-                                  int nb) {
-    __shared__ uint32_t h[SORT_WARPS][RADIX];
+template <typename K, int THREADS, int SORT_ITEMS>
+__global__ void __launch_bounds__(THREADS) radix_hist_kernel(const K *keys, int n, const int *d_n, int shift,
+                                                             uint32_t mask, uint32_t *counts, int nb) {
+    constexpr int WARPS = THREADS / 32;
+    __shared__ uint32_t h[WARPS][RADIX];
     if (d_n) n = min(n, *d_n);
-    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&h[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < WARPS * RADIX; i += THREADS) (&h[0][0])[i] = 0;
     __syncthreads();
     const int warp = threadIdx.x >> 5;
-    constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
+    constexpr int SORT_TILE = THREADS * SORT_ITEMS;
     const int base = blockIdx.x * SORT_TILE;
     int dig[SORT_ITEMS];
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {  // independent loads first
-        const int k = base + j * SORT_THREADS + threadIdx.x;
+        const int k = base + j * THREADS + threadIdx.x;
         dig[j] = k < n ? (int)((keys[k] >> shift) & mask) : RADIX;
     }
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++)
         if (dig[j] < RADIX) atomicAdd(&h[warp][dig[j]], 1u);
     __syncthreads();
-    for (int i = threadIdx.x; i < RADIX; i += blockDim.x) {
+    for (int i = threadIdx.x; i < RADIX; i += THREADS) {
         uint32_t s = 0;
 #pragma unroll
-        for (int w = 0; w < SORT_WARPS; w++) s += h[w][i];
+        for (int w = 0; w < WARPS; w++) s += h[w][i];
         counts[(size_t)i * nb + blockIdx.x] = s;
     }
 }
 
-// counts -> exclusive digit-major offsets (uint32 scan over 256 * nb entries)
-template <typename K, int SORT_ITEMS>
 // offs: the exclusive digit-major scan of the per-block digit counts; or, with offs
 // null (a sort of at most DIRECT_SORT_BLOCKS blocks), counts: the per-block digit counts
 // themselves, from which each block forms its own digit starts (no scan launch).
-__global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout, uint32_t *vout, int n,
-                                     const int *d_n, int shift, uint32_t mask, const int32_t *offs,
-                                     const uint32_t *counts, int nb) {
+// The 64-bit-key scatter is held to 64 registers, four resident blocks per SM (32 M
+// pairs of 40 bits: 2.35 instead of 2.49 ms); the 32-bit ones to 128 (the depth order
+// of a street view's 100 k Gaussians ran 10 % slower at 64).
+template <typename K, int THREADS, int SORT_ITEMS>
+__global__ void __launch_bounds__(THREADS, sizeof(K) == 8 ? 1024 / THREADS : 512 / THREADS) radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
+                                                                uint32_t *vout, int n, const int *d_n, int shift,
+                                                                uint32_t mask, const int32_t *offs,
+                                                                const uint32_t *counts, int nb) {
     // The block's keys are first ranked and placed in shared memory in digit order
     // (a block-local stable multisplit), then written out so that consecutive threads
     // write consecutive entries of each digit's run: coalesced global stores.
-    __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
+    static_assert(THREADS >= RADIX && THREADS <= MAX_SORT_THREADS, "a thread per digit");
+    constexpr int WARPS = THREADS / 32;
+    __shared__ uint32_t wcnt[WARPS][RADIX];
     __shared__ uint32_t gbase[RADIX], bstart[RADIX + 1];
-    constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // keys per block
-    constexpr int WARP_KEYS = SORT_TILE / SORT_WARPS;     // contiguous keys per warp
+    constexpr int SORT_TILE = THREADS * SORT_ITEMS;  // keys per block
+    constexpr int WARP_KEYS = SORT_TILE / WARPS;     // contiguous keys per warp
     __shared__ uint32_t ws[33];
     extern __shared__ __align__(16) unsigned char sort_smem[];  // radix_scatter_smem<K, SORT_ITEMS>()
     K *skey = reinterpret_cast<K *>(sort_smem);
     uint32_t *sval = reinterpret_cast<uint32_t *>(skey + SORT_TILE);
     if (d_n) n = min(n, *d_n);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < WARPS * RADIX; i += THREADS) (&wcnt[0][0])[i] = 0;
     if (offs) {
-        for (int i = threadIdx.x; i < RADIX; i += blockDim.x) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
+        for (int i = threadIdx.x; i < RADIX; i += THREADS) gbase[i] = (uint32_t)offs[(size_t)i * nb + blockIdx.x];
     } else {  // thread d: digit d's count over all blocks and over the blocks before this one
-        static_assert(SORT_THREADS == RADIX, "one thread per digit");
-        const uint32_t *row = counts + (size_t)threadIdx.x * nb;
         uint32_t tot = 0u, before = 0u;
-        for (int b = 0; b < nb; b++) {
-            const uint32_t c = row[b];
-            tot += c;
-            if (b < (int)blockIdx.x) before += c;
+        if (threadIdx.x < RADIX) {
+            const uint32_t *row = counts + (size_t)threadIdx.x * nb;
+            for (int b = 0; b < nb; b++) {
+                const uint32_t c = row[b];
+                tot += c;
+                if (b < (int)blockIdx.x) before += c;
+            }
         }
         uint32_t all;
-        gbase[threadIdx.x] = block_exclusive_scan<uint32_t>(tot, ws, all) + before;
+        const uint32_t ex = block_exclusive_scan<uint32_t>(tot, ws, all) + before;
+        if (threadIdx.x < RADIX) gbase[threadIdx.x] = ex;
     }
     K key[SORT_ITEMS];
     uint32_t val[SORT_ITEMS], rank[SORT_ITEMS];
@@ -454,11 +471,12 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     }
     __syncthreads();
     const unsigned lt = (1u << lane) - 1u;
+    const bool full = (int64_t)blockIdx.x * SORT_TILE + SORT_TILE <= (int64_t)n;
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; r++) {
         const int d = dig[r];
         const bool ok = d < RADIX;
-        const unsigned peers = digit_peers(d);
+        const unsigned peers = digit_peers(d, mask, full);
         const uint32_t before = ok ? wcnt[warp][d] : 0u;
         rank[r] = before + (uint32_t)__popc(peers & lt);
         __syncwarp();
@@ -471,7 +489,7 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     if (threadIdx.x < RADIX) {
         const int d = threadIdx.x;
 #pragma unroll
-        for (int w = 0; w < SORT_WARPS; w++) {
+        for (int w = 0; w < WARPS; w++) {
             const uint32_t t = wcnt[w][d];
             wcnt[w][d] = tot;
             tot += t;
@@ -493,7 +511,7 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     }
     __syncthreads();
     const int valid = (int)bstart[RADIX];
-    for (int i = threadIdx.x; i < valid; i += blockDim.x) {
+    for (int i = threadIdx.x; i < valid; i += THREADS) {
         const K kk = skey[i];
         const int d = (int)((kk >> shift) & mask);
         const uint32_t pos = gbase[d] + ((uint32_t)i - bstart[d]);
@@ -502,9 +520,9 @@ __global__ void radix_scatter_kernel(const K *kin, const uint32_t *vin, K *kout,
     }
 }
 
-template <typename K, int ITEMS>
+template <typename K, int THREADS, int ITEMS>
 constexpr size_t radix_scatter_smem() {
-    return (size_t)SORT_THREADS * ITEMS * (sizeof(K) + sizeof(uint32_t));
+    return (size_t)THREADS * ITEMS * (sizeof(K) + sizeof(uint32_t));
 }
 
 size_t radix_scratch_bytes(int n) {
@@ -516,21 +534,22 @@ size_t radix_scratch_bytes(int n) {
 // Sorts (k[0], v[0]) using (k[1], v[1]) as the ping-pong buffers; returns the index
 // (0 or 1) of the buffer pair holding the result. With d_n, n is a capacity and the
 // count is read on the device (no host round trip; every pass runs).
-template <typename K, int ITEMS>
+template <typename K, int THREADS, int ITEMS>
 int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
-    const int nb = (n + SORT_THREADS * ITEMS - 1) / (SORT_THREADS * ITEMS);
+    const int nb = (n + THREADS * ITEMS - 1) / (THREADS * ITEMS);
     const size_t cnt = (size_t)RADIX * nb;
     int32_t *counts = reinterpret_cast<int32_t *>(scratch);
     int32_t *offs = counts + cnt;
     int32_t *partials = offs + cnt;
-    constexpr size_t smem = radix_scatter_smem<K, ITEMS>();
-    if (smem > 32 * 1024) {  // with the static arrays, above the 48 KB default: opt in once per device
+    constexpr size_t smem = radix_scatter_smem<K, THREADS, ITEMS>();
+    {  // once per device: the dynamic staging (with the static arrays it can pass the 48 KB
+       // default)
         static std::atomic<uint64_t> done{0};
         int dev = 0;
         cudaGetDevice(&dev);
         const uint64_t bit = 1ull << (dev & 63);
         if (!(done.load() & bit)) {
-            cudaFuncSetAttribute(radix_scatter_kernel<K, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(radix_scatter_kernel<K, THREADS, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
             done.fetch_or(bit);
         }
@@ -539,11 +558,11 @@ int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch,
     for (int shift = 0; shift < key_bits; shift += 8) {
         const int bits = key_bits - shift < 8 ? key_bits - shift : 8;  // digits above key_bits are ignored
         const uint32_t mask = (1u << bits) - 1u;
-        radix_hist_kernel<K, ITEMS><<<nb, SORT_THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
-                                                                 reinterpret_cast<uint32_t *>(counts), nb);
+        radix_hist_kernel<K, THREADS, ITEMS><<<nb, THREADS, 0, st>>>(k[cur], n, d_n, shift, mask,
+                                                                     reinterpret_cast<uint32_t *>(counts), nb);
         const bool direct = nb <= DIRECT_SORT_BLOCKS;
         if (!direct) scan_exclusive<int32_t>(counts, offs, (int)cnt, nullptr, partials, st);
-        radix_scatter_kernel<K, ITEMS><<<nb, SORT_THREADS, smem, st>>>(
+        radix_scatter_kernel<K, THREADS, ITEMS><<<nb, THREADS, smem, st>>>(
             k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n, d_n, shift, mask, direct ? nullptr : offs,
             reinterpret_cast<const uint32_t *>(counts), nb);
         cur ^= 1;
@@ -554,8 +573,10 @@ int radix_sort_impl(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch,
 template <typename K>
 int radix_sort_dispatch(K *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st, const int *d_n) {
     if ((!d_n && n <= 1) || n <= 0 || key_bits <= 0) return 0;
-    return sort_items(n, (int)sizeof(K)) == 16 ? radix_sort_impl<K, 16>(k, v, n, key_bits, scratch, st, d_n)
-                               : radix_sort_impl<K, 8>(k, v, n, key_bits, scratch, st, d_n);
+    if constexpr (sizeof(K) == 4) {
+        if (n >= LARGE_SORT) return radix_sort_impl<K, 256, 16>(k, v, n, key_bits, scratch, st, d_n);
+    }
+    return radix_sort_impl<K, 256, 8>(k, v, n, key_bits, scratch, st, d_n);
 }
 
 int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,

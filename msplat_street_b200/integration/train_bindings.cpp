@@ -9,12 +9,18 @@
 // callers hold them, and prints one JSON line: {"iters_per_s", "ms_per_step", "steps",
 // "warmup", "gaussians", "width", "height"}.
 //
-//     train_bindings [steps] [warmup]
+// With the mode "c_abi" the same training runs from C++ straight through the C-ABI
+// (include/msplat_cuda.h) with every tensor resident in device memory -- the form a
+// C++ host that owns its device buffers takes: no per-call staging, the loss read back
+// once at the end.
+//
+//     train_bindings [steps] [warmup] [bindings_h | c_abi]
 //
 // Built by msplat_street_b200.build.build_bindings_bench against the reference's
 // headers (core/metal/bindings.h, core/include/metal_tensor.hpp) and
 // integration/bindings_cuda.cpp; the binary runs without the reference tree.
 #include "bindings.h"
+#include "msplat_cuda.h"
 
 #include <chrono>
 #include <cmath>
@@ -97,9 +103,24 @@ void camera(float viewmat[16], float projmat[16], float cam_pos[3]) {
 
 }  // namespace
 
+void check(int status) {
+    if (status != MSPLAT_CUDA_OK) {
+        std::fprintf(stderr, "msplat_cuda: %s\n", msplat_cuda_last_error());
+        std::exit(2);
+    }
+}
+
+float *to_device(const MTensor &t) {
+    void *d = nullptr;
+    check(msplat_cuda_device_alloc(t.nbytes(), &d));
+    check(msplat_cuda_copy_buffer(msplat_cuda_default_ctx(), d, t.data_ptr(), t.nbytes()));
+    return static_cast<float *>(d);
+}
+
 int main(int argc, char **argv) {
     const int steps = argc > 1 ? std::atoi(argv[1]) : 200;
     const int warmup = argc > 2 ? std::atoi(argv[2]) : 10;
+    const bool c_abi = argc > 3 && std::strcmp(argv[3], "c_abi") == 0;
     float vmf[16], pmf[16], cam_pos[3];
     camera(vmf, pmf, cam_pos);
     MTensor viewmat = gpu_empty({4, 4}, DType::Float32), projmat = gpu_empty({4, 4}, DType::Float32);
@@ -131,6 +152,21 @@ int main(int argc, char **argv) {
     const float lr[6] = {0.00016f, 0.005f, 0.001f, 0.0025f, 0.000125f, 0.05f};  // model.cpp:100
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
 
+    // the c_abi mode's device copies of every tensor the step reads or updates
+    msplat_cuda_ctx *cx = msplat_cuda_default_ctx();
+    float *d_par[6] = {}, *d_m1[6] = {}, *d_m2[6] = {}, *d_gt = nullptr, *d_stat[3] = {};
+    if (c_abi) {
+        for (int g = 0; g < 6; g++) {
+            d_par[g] = to_device(params[g]);
+            d_m1[g] = to_device(m1[g]);
+            d_m2[g] = to_device(m2[g]);
+        }
+        d_gt = to_device(gt);
+        d_stat[0] = to_device(vis);
+        d_stat[1] = to_device(gn);
+        d_stat[2] = to_device(ms);
+        check(msplat_cuda_sync(cx));
+    }
     auto step = [&](int t) {
         // Model::fullIteration's bias-corrected scalars (core/src/model.cpp:638-651)
         const float bc1 = 1.0f - std::pow(beta1, t), bc2 = 1.0f - std::pow(beta2, t);
@@ -138,6 +174,14 @@ int main(int argc, char **argv) {
         for (int g = 0; g < 6; g++) {
             ss[g] = lr[g] / bc1;
             b2[g] = std::sqrt(bc2);
+        }
+        if (c_abi) {
+            check(msplat_cuda_train_step(cx, N, d_par[0], d_par[1], 1.f, d_par[2], vmf, pmf, F, F, W / 2.f, H / 2.f,
+                                         H, W, std::get<0>(tiles), std::get<1>(tiles), 0.01f, 3, 3, cam_pos, d_par[3],
+                                         d_par[4], d_par[5], bgv, d_gt, 0.2f, 1.f / (float)(H * W * 3), 6, d_m1, d_m2,
+                                         ss, b2, beta1, beta2, eps, d_stat[0], d_stat[1], d_stat[2],
+                                         1.f / (float)std::max(H, W), nullptr, nullptr));
+            return 0.f;
         }
         auto r = msplat_train_step(N, s.means, s.scales, 1.f, s.quats, viewmat, projmat, F, F, W / 2.f, H / 2.f, H, W,
                                    tiles, 0.01f, 3, 3, cam_pos, s.dc, s.rest, s.opac, bg, gt, window, 0.2f,
@@ -151,11 +195,23 @@ int main(int argc, char **argv) {
     const auto t0 = std::chrono::steady_clock::now();
     float loss = 0.f;
     for (int i = 0; i < steps; i++) loss = step(++t);
+    if (c_abi) {  // the last step's loss, read once after the timed loop
+        const float *dl = nullptr;
+        check(msplat_cuda_loss_device(cx, &dl));
+        check(msplat_cuda_copy_buffer(cx, &loss, dl, sizeof(float)));
+    }
     msplat_gpu_sync();
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    std::printf("{\"iters_per_s\": %.3f, \"ms_per_step\": %.4f, \"steps\": %d, \"warmup\": %d, \"gaussians\": %d, "
-                "\"width\": %d, \"height\": %d, \"final_loss\": %.6f}\n",
-                steps / sec, 1e3 * sec / steps, steps, warmup, N, W, H, loss);
+    std::printf("{\"mode\": \"%s\", \"iters_per_s\": %.3f, \"ms_per_step\": %.4f, \"steps\": %d, \"warmup\": %d, "
+                "\"gaussians\": %d, \"width\": %d, \"height\": %d, \"final_loss\": %.6f}\n",
+                c_abi ? "c_abi" : "bindings_h", steps / sec, 1e3 * sec / steps, steps, warmup, N, W, H, loss);
+    for (int g = 0; g < 6; g++) {
+        msplat_cuda_free(d_par[g]);
+        msplat_cuda_free(d_m1[g]);
+        msplat_cuda_free(d_m2[g]);
+    }
+    msplat_cuda_free(d_gt);
+    for (float *p : d_stat) msplat_cuda_free(p);
     cleanup_msplat_metal();
     return std::isfinite(loss) ? 0 : 1;
 }

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("n,bits,hi", [
     (1, 32, 10), (5, 32, 4), (1023, 32, 2 ** 30), (1024, 32, 2 ** 30), (1025, 32, 7),
     (70_000, 32, 2 ** 30), (5_000, 64, 2 ** 63), (2_049, 64, 3),
-    (1_000_003, 43, 2 ** 43), (300_000, 30, 2 ** 40), (2_500_000, 64, 2 ** 62),
+    (1_000_003, 43, 2 ** 43), (300_000, 30, 2 ** 40), (2_500_000, 64, 2 ** 62), (5_000_001, 40, 2 ** 40),
 ])
 def test_gpu_radix_sort_matches_numpy(n, bits, hi):
     rng = np.random.default_rng(n + bits)

@@ -42,13 +42,18 @@ def test_training_through_bindings_h_with_host_tensors():
     """integration/train_bindings.cpp trains the small plain config through bindings.h
     with host tensors, as the reference's Model / CLI hold them: every call stages its
     tensors through the persistent device buffers and back. It must run, report its
-    throughput, and its loss must fall from the first steps to the last."""
+    throughput, and its loss must fall from the first steps to the last. The same
+    training from C++ through the C-ABI with device-resident tensors (mode c_abi) ends
+    at the same loss: the staging only moves bytes."""
     import json
     first = subprocess.run([TRAIN_BIN, "2", "0"], capture_output=True, text=True, timeout=300)
     last = subprocess.run([TRAIN_BIN, "150", "0"], capture_output=True, text=True, timeout=300)
-    for r in (first, last):
+    direct = subprocess.run([TRAIN_BIN, "150", "0", "c_abi"], capture_output=True, text=True, timeout=300)
+    for r in (first, last, direct):
         assert r.returncode == 0, r.stdout + r.stderr
     a = json.loads(first.stdout.strip().splitlines()[-1])
     b = json.loads(last.stdout.strip().splitlines()[-1])
+    c = json.loads(direct.stdout.strip().splitlines()[-1])
     assert b["iters_per_s"] > 0 and b["steps"] == 150
     assert b["final_loss"] < a["final_loss"], (a, b)
+    assert c["mode"] == "c_abi" and c["final_loss"] == b["final_loss"], (b, c)
