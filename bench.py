@@ -241,6 +241,8 @@ def run_ours(args, world, rank, local):
 
     # ---- device-timed pass: targets resident in HBM ----
     ctx = Context()
+    if args.raster_shape is not None:
+        ctx.set_raster_shape(args.raster_shape)
     trainer, targets = workloads.street_plain(ctx, iterations=iters)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     for _ in range(args.warmup):
@@ -296,6 +298,8 @@ def run_ours(args, world, rank, local):
 
     # ---- end-to-end pass through the public API: host targets, loss read back ----
     ctx2 = Context()
+    if args.raster_shape is not None:
+        ctx2.set_raster_shape(args.raster_shape)
     trainer2, targets2 = workloads.street_plain(ctx2, iterations=iters)
     host_targets = [t.cpu().pin_memory() for t in targets2]
     del targets2
@@ -480,11 +484,11 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
             tr.step()
         tuned = None
         if graph:
-            # the staging autotuner on this arm before it is timed: every compiled
-            # rasterizer variant timed on the graph-replayed step, interleaved over
-            # rounds; the step keeps the best
+            # the autotuner on this arm before it is timed: every compiled rasterizer
+            # staging variant x batched-forward block shape (16x16, 16x8, 8x8) timed on
+            # the graph-replayed step, interleaved over rounds; the step keeps the best
             from msplat_street_b200.autotune import tune_raster
-            tuned = tune_raster([ctx], tr.step, warmup=1, reps=4, rounds=2)
+            tuned = tune_raster([ctx], tr.step, warmup=1, reps=4, rounds=2, shapes=[0, 1, 2])
         torch.cuda.synchronize()
         steps = views // per
         if not graph:  # the eager arms report per-view device time by stage (CUDA events)
@@ -507,7 +511,8 @@ def batching_report(dev, views: int = 480, warmup_views: int = 48, views_per_ste
         if graph:
             out[name]["graph"] = ctx.graph_stats()
             out[name]["autotune"] = {"best": tuned["best"], "best_staging": tuned["variants"][tuned["best"]],
-                                     "ms_per_step": {str(k): v for k, v in tuned["ms"].items()}}
+                                     "best_shape": tuned["shapes"][tuned["best_shape"]],
+                                     "ms_per_step_by_variant_shape": {str(k): v for k, v in tuned["ms"].items()}}
         del tr
         ctx.close()
         torch.cuda.empty_cache()
@@ -550,6 +555,10 @@ def small_batching_report(views_per_step: int = 8, views: int = 960):
         per = views_per_step if batched else 1
         for _ in range(max(32 // per, 3)):
             tr.step()
+        tuned = None
+        if graph:  # the same tuner as the street arm's, on this step
+            from msplat_street_b200.autotune import tune_raster
+            tuned = tune_raster([ctx], tr.step, warmup=1, reps=6, rounds=2, shapes=[0, 1, 2])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(views // per):
@@ -557,6 +566,9 @@ def small_batching_report(views_per_step: int = 8, views: int = 960):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         out[name] = {"views_per_s": (views // per) * per / dt}
+        if tuned:
+            out[name]["autotune"] = {"best_staging": tuned["variants"][tuned["best"]],
+                                     "best_shape": tuned["shapes"][tuned["best_shape"]]}
         ctx.close()
     out["batched_graph"]["views_per_s_vs_plain"] = out["batched_graph"]["views_per_s"] / out["plain"]["views_per_s"]
     return out
@@ -911,7 +923,7 @@ def knn_rate(trainer, ctx, reps: int = 5) -> dict:
 PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")
 
 
-def profile_case(name: str, dev, runs: int = 2) -> dict:
+def profile_case(name: str, dev, runs: int = 2, shape=None) -> dict:
     """One stage at a size larger than the 126 MB L2, run `runs` times (default twice:
     the second launch is the one an ncu capture takes with -s 1 -c 1 on the stage's
     kernel), for the DRAM traffic and achieved bandwidth of that kernel; "stage_ms" holds
@@ -927,6 +939,8 @@ def profile_case(name: str, dev, runs: int = 2) -> dict:
     from msplat_street_b200.backend import AdamState, Context, GaussianParams
 
     ctx = Context()
+    if shape is not None:
+        ctx.set_raster_shape(shape)
     g = torch.Generator(device=dev).manual_seed(7)
     out = {"case": name}
     runs = max(2, runs)
@@ -1028,10 +1042,12 @@ def main(argv=None):
     ap.add_argument("--profile-case", choices=PROFILE_CASES,
                     help="run one stage at a size larger than L2 (for an ncu capture) and exit")
     ap.add_argument("--case-runs", type=int, default=2, help="runs of the --profile-case stage (at least 2)")
+    ap.add_argument("--raster-shape", type=int, default=None,
+                    help="forward rasterizer block shape (0: 16x16, 1: 16x8, 2: 8x8; default: the library's)")
     args = ap.parse_args(argv)
     if args.profile_case:
         import torch
-        print(json.dumps(profile_case(args.profile_case, torch.device("cuda", 0), args.case_runs)))
+        print(json.dumps(profile_case(args.profile_case, torch.device("cuda", 0), args.case_runs, args.raster_shape)))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

@@ -56,6 +56,11 @@ int msplat_cuda_ctx_set_stream(msplat_cuda_ctx *ctx, void *stream);
  * "graph" (1 = msplat_cuda_train_batch replays a captured CUDA graph of its step);
  * "raster_variant" (0..7: the rasterizer's shared-memory staging sizes, see
  * msplat_cuda_raster_variant; results do not depend on it, speed does);
+ * "raster_shape" (0..2: the pixels a block of the batched forward composites --
+ * 16 x 16, 16 x 8 or 8 x 8 -- each block walking its 16 x 16 tile's whole list, so
+ * results do not depend on it; the reference's Metal rasterizer runs 8 x 8 thread
+ * groups in its 16 x 16 bins, core/metal/msplat_metal.mm:1187-1197; see
+ * msplat_cuda_raster_shape);
  * "stage_timing" (1 = time the stages, see msplat_cuda_drain_stage_times);
  * "store_transmittance" (K > 0: the forward stores each pixel's transmittance before
  * its first K contributions and the backward reads them instead of recovering T by
@@ -79,6 +84,9 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
 /* Staging sizes of rasterizer variant v (0..7): Gaussians per forward round, per
  * backward round, and the backward reduction's sub-batch. Returns the variant count. */
 int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, int32_t *bwd_sub);
+/* Block shape s (0..2) of the batched forward: width and height in pixels. Returns the
+ * shape count. */
+int msplat_cuda_raster_shape(int s, int32_t *w, int32_t *h);
 /* No counterpart in the reference (measurement). The (pixel, Gaussian) pairs the
  * reference's loops evaluate over the context's last single-view frame: out[0] for the
  * forward (core/cpu/msplat_cpu.cpp:574-626: each pixel walks its tile's list up to the

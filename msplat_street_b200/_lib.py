@@ -106,6 +106,7 @@ _SIGS["msplat_cuda_train_batch"] = (i32, [vp, i32, vp, vp, f32, vp, vp, vp, vp, 
 _SIGS["msplat_cuda_train_batch_stats"] = (i32, [vp, C.POINTER(i64)])
 _SIGS["msplat_cuda_raster_variant"] = (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32)])
+_SIGS["msplat_cuda_raster_shape"] = (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)])
 _SIGS["msplat_cuda_resize_area"] = (i32, [vp, vp, i32, i32, i32, vp, i32, i32])
 _SIGS["msplat_cuda_undistort"] = (i32, [vp, vp, i32, i32, vp, vp, i32, i32, vp, i32, i32])
 _SIGS["msplat_cuda_image_metrics"] = (i32, [vp, vp, vp, i32, i32, vp])

@@ -204,6 +204,8 @@ class Context:
         h = C.c_void_p()
         check(self._lib.msplat_cuda_ctx_create(C.byref(h)))
         self.handle = h
+        self.raster_variant = 0
+        self.raster_shape = 0
         self.keep_grads = keep_grads
         if keep_grads:
             check(self._lib.msplat_cuda_ctx_set_option(h, b"keep_grads", 1))
@@ -404,6 +406,12 @@ class Context:
         """Rasterizer staging variant (see raster_variants()); results do not depend on it."""
         check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"raster_variant", int(v)))
         self.raster_variant = int(v)
+
+    def set_raster_shape(self, s: int) -> None:
+        """Block shape of the batched forward rasterizer (see autotune.raster_shapes());
+        results do not depend on it."""
+        check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"raster_shape", int(s)))
+        self.raster_shape = int(s)
 
     def set_graph(self, on: bool = True) -> None:
         """Replay a captured CUDA graph of each batched training step (train_batch)."""

@@ -251,13 +251,13 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ctx->timer.mark(2, st);
     if (aux) {
         if (sky) launch_sky_background(sky_args(*pr, cam), (int)cam.width, (int)cam.height, bg_img, st);
-        launch_raster_fwd_aux(ra, st);
+        launch_raster_fwd_aux(ra, st, ctx->raster_shape);
     } else if (chunked) {
         launch_chunk_items(tile_start, tile_end, T, ck.chunk_len, reinterpret_cast<int32_t *>(ctx->ch[CH_COUNTS].ptr),
                            ck.first, reinterpret_cast<int32_t *>(ctx->ch[CH_PART].ptr), st);
         launch_raster_fwd_chunked(ra, ck, ctx->chunk_cap, st, ctx->raster_variant);
     } else {
-        launch_raster_fwd(ra, st, ctx->raster_variant);
+        launch_raster_fwd(ra, st, ctx->raster_variant, ctx->raster_shape);
     }
     ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
@@ -425,7 +425,7 @@ int forward_batch(msplat_cuda_ctx *ctx, int nv, const msplat_cuda_view *views) {
     CUDA_TRY(cudaEventRecord(ctx->bdesc_ev, st));
     ctx->bdesc_pending = true;
     ctx->timer.mark(2, st);
-    launch_raster_fwd_batch(d, T, d_counter, st, ctx->raster_variant);
+    launch_raster_fwd_batch(d, T, d_counter, st, ctx->raster_variant, ctx->raster_shape);
     ctx->timer.mark(3, st);
     CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
@@ -487,6 +487,12 @@ int msplat_cuda_ctx_set_option(msplat_cuda_ctx *ctx, const char *name, int64_t v
         if (value < 0 || value >= N_RASTER_VARIANTS)
             return fail(MSPLAT_CUDA_EINVAL, "raster_variant must be 0..%d", N_RASTER_VARIANTS - 1);
         ctx->raster_variant = (int)value;
+        return MSPLAT_CUDA_OK;
+    }
+    if (!std::strcmp(name, "raster_shape")) {
+        if (value < 0 || value >= N_RASTER_SHAPES)
+            return fail(MSPLAT_CUDA_EINVAL, "raster_shape must be 0..%d", N_RASTER_SHAPES - 1);
+        ctx->raster_shape = (int)value;
         return MSPLAT_CUDA_OK;
     }
     if (!std::strcmp(name, "graph")) {
@@ -1265,6 +1271,14 @@ int msplat_cuda_raster_variant(int v, int32_t *fwd_batch, int32_t *bwd_batch, in
         if (bwd_sub) *bwd_sub = RASTER_VARIANTS[v].bwd_sub;
     }
     return N_RASTER_VARIANTS;
+}
+
+int msplat_cuda_raster_shape(int s, int32_t *w, int32_t *h) {
+    if (s >= 0 && s < N_RASTER_SHAPES) {
+        if (w) *w = RASTER_SHAPES[s].w;
+        if (h) *h = RASTER_SHAPES[s].h;
+    }
+    return N_RASTER_SHAPES;
 }
 
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx) {

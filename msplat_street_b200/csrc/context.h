@@ -176,6 +176,7 @@ constexpr int CHUNK_AUTO_TILES = 400;  // core/metal/msplat_metal.mm:1103
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
     int raster_variant = 0;  // option "raster_variant": index into RASTER_VARIANTS
+    int raster_shape = 0;    // option "raster_shape": index into RASTER_SHAPES (batched forward)
     TrainBatchState tb;
     bool keep_grads = false;
     StageTimer timer;

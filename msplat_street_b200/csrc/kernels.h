@@ -96,13 +96,23 @@ constexpr RasterVariant RASTER_VARIANTS[N_RASTER_VARIANTS] = {
     {128, 128, 3}, {128, 64, 3}, {128, 64, 4}, {256, 128, 3}, {64, 128, 3}, {256, 64, 4}, {128, 32, 4}, {256, 128, 4}};
 inline int variant_index(int v) { return (v >= 0 && v < N_RASTER_VARIANTS) ? v : 0; }
 
-void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0);
+// Block shapes of the batched forward rasterizer (pixels a block composites; every
+// shape walks the 16 x 16 tile's list, so all give the same bits): 16 x 16 (the
+// default), 16 x 8 and 8 x 8 (the reference's Metal thread-group shape).
+struct RasterShape {
+    int w, h;
+};
+constexpr int N_RASTER_SHAPES = 3;
+constexpr RasterShape RASTER_SHAPES[N_RASTER_SHAPES] = {{16, 16}, {16, 8}, {8, 8}};
+inline int shape_index(int s) { return (s >= 0 && s < N_RASTER_SHAPES) ? s : 0; }
+
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0, int shape = 0);
 // (pixel, Gaussian) pairs the reference's forward / backward loops evaluate over the
 // frame (out[0], out[1]; device counters)
 void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st);
 // the rasterizers' exponential (exp_tab) of n device inputs
 void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st);
-void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st);
+void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st, int shape = 0);
 
 struct RasterBwdArgs;
 // Depth-chunked compositing (core/metal/msplat_metal.metal:2641-3030): every tile's
@@ -161,7 +171,8 @@ void launch_project_batch(const BatchDesc &d, int total, cudaStream_t st);
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,
                             const int64_t *offsets, const DepthScratch *ds, const BatchDesc &d, uint32_t *keys,
                             uint32_t *vals, int32_t *emit_gid, cudaStream_t st, int64_t cap = INT64_MAX);
-void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant = 0);
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant = 0,
+                             int shape = 0);
 
 struct RasterBwdArgs {
     int W, H, tiles_x, tiles_y;

@@ -91,19 +91,36 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 A, const float4
     return mask;
 }
 
+// The tile thread (0 .. TILE_PIX - 1, as tile_pixel maps it) that thread t of a block
+// of NT threads takes in sub-block q of the tile: NT = 256, the whole tile; 128, the
+// 16 x 8 half q (warps 4q .. 4q + 3); 64, the 8 x 8 quarter q = (qy, qx) (warps
+// 4 qy + qx and 4 qy + 2 + qx: column half qx, rows 8 qy .. 8 qy + 7).
+template <int NT>
+__device__ __forceinline__ int sub_tile_thread(int t, int q) {
+    if (NT == TILE_PIX) return t;
+    if (NT == TILE_PIX / 2) return q * NT + t;
+    return ((4 * (q >> 1) + (q & 1) + 2 * (t >> 5)) << 5) + (t & 31);
+}
+
 // One 16x16 tile: `tile` indexes tile_start / tile_end (a global tile id in a batch),
 // (tx, ty) is its position in its view. Every thread of the block must call it.
-// FB: Gaussians staged in shared memory per round (at most one per thread).
+// NT, q: the block runs sub-block q of the tile with NT threads (sub_tile_thread), each
+// pixel walking the tile's whole list with the same decisions and sums as in a
+// whole-tile block, so its results do not depend on the shape.
+// FB: Gaussians staged in shared memory per round.
 // AUX: also the expected-depth numerator and a per-pixel background
 // (rasterize_forward_aux, core/cpu/msplat_cpu.cpp:574-626 with f.aux).
 // CHUNK: composite only piece `chunk` of the list (ck->chunk_len long) from T = 1 and
 // write the piece's transmittance, colour and last contributor to item `item`.
-template <int FB, bool AUX = false, bool CHUNK = false, bool TS = false>
+template <int FB, bool AUX = false, bool CHUNK = false, bool TS = false, int NT = FWD_THREADS>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
                                                 float4 *s1, float4 *s2, uint8_t *sm, const double *etab,
-                                                const ChunkArgs *ck = nullptr, int item = 0, int chunk = 0) {
+                                                const ChunkArgs *ck = nullptr, int item = 0, int chunk = 0,
+                                                int q = 0) {
+    static_assert(!CHUNK || NT == FWD_THREADS, "depth pieces are composited by whole-tile blocks");
+    const int g = sub_tile_thread<NT>(threadIdx.x, q);  // this thread's place in the tile
     int lx, ly;
-    tile_pixel(threadIdx.x, lx, ly);
+    tile_pixel(g, lx, ly);
     const int px = tx * TILE + lx, py = ty * TILE + ly;
     const bool inside = px < a.W && py < a.H;
     int start = a.tile_start[tile], end = a.tile_end[tile];
@@ -112,7 +129,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
         end = min(end, start + ck->chunk_len);
     }
     const float fpx = (float)px, fpy = (float)py;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = g >> 5, lane = threadIdx.x & 31;  // w: the warp's block of the tile
     float T = 1.f, cr = 0.f, cg = 0.f, cb = 0.f, depth = 0.f;
     int last = start - 1;
     bool done = !inside;
@@ -120,19 +137,20 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     const size_t pid = inside ? (size_t)py * a.W + px : 0;
     int stored = 0;  // contributions seen (stored-transmittance mode)
     for (int b0 = start; b0 < end; b0 += FB) {
-        if (__syncthreads_count(done) == TILE_PIX) break;
-        const int k = b0 + threadIdx.x;
-        if (threadIdx.x < FB && k < end) {
+        if (__syncthreads_count(done) == NT) break;
+        for (int si = threadIdx.x; si < FB; si += NT) {
+            const int k = b0 + si;
+            if (k >= end) break;
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
             const float4 A = rec[0], B = rec[1], C = rec[2];
-            s0[threadIdx.x] = A;
-            s1[threadIdx.x] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
+            s0[si] = A;
+            s1[si] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
             // z: the sigma above which alpha = o exp(-sigma) < 1/255 for certain,
             // ln(255 o) plus a margin far above the roundings of logf, of exp_tab and
             // of the product, so a pixel past it skips the exponential with the
             // decision the exact test would take
-            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, logf(255.f * B.y) + 1e-3f, C.w);
-            sm[threadIdx.x] = (uint8_t)warp_block_mask(A, C, tx, ty);
+            s2[si] = make_float4(staged_colour(C.x), C.y, logf(255.f * B.y) + 1e-3f, C.w);
+            sm[si] = (uint8_t)warp_block_mask(A, C, tx, ty);
         }
         __syncthreads();
         const int cnt = min(FB, end - b0);
@@ -171,7 +189,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     }
     if (!inside) return;
     if (CHUNK) {
-        const size_t o = (size_t)item * TILE_PIX + threadIdx.x, o3 = (size_t)item * 3 * TILE_PIX + threadIdx.x;
+        const size_t o = (size_t)item * TILE_PIX + g, o3 = (size_t)item * 3 * TILE_PIX + g;
         ck->cT[o] = T;
         ck->cC[o3] = cr;
         ck->cC[o3 + TILE_PIX] = cg;
@@ -206,44 +224,54 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
     o[2] = clamp01(a.bg[2] * T + cb);
 }
 
-template <int FB, bool AUX = false, bool TS = false>
-__global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_kernel(RasterArgs a) {
+// One block per sub-block of a tile (NT threads: the whole 16 x 16 tile, a 16 x 8
+// half or an 8 x 8 quarter; blocks SUB * t .. SUB * t + SUB - 1 share tile t's list).
+template <int FB, bool AUX = false, bool TS = false, int NT = FWD_THREADS>
+__global__ void __launch_bounds__(NT, 4 * FWD_THREADS / NT) raster_fwd_kernel(RasterArgs a) {
+    constexpr int SUB = FWD_THREADS / NT;
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
     __shared__ double etab[EXP_TABLE];
     exp_table_init(etab);  // ready after the tile's first barrier
-    const int tile = blockIdx.x;
-    raster_fwd_tile<FB, AUX, false, TS>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab);
+    const int tile = blockIdx.x / SUB;
+    raster_fwd_tile<FB, AUX, false, TS, NT>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab,
+                                            nullptr, 0, 0, blockIdx.x % SUB);
 }
 
 // Persistent forward over the tiles of a batch of views (each with its own scene,
-// camera, resolution and output): every block pulls global tile ids from a counter
-// until none are left. A tile's image equals what the per-view kernel renders: the
-// same list (the batch sort keeps each tile's order) and the same code.
-template <int FB>
-__global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
+// camera, resolution and output): every block pulls work items from a counter until
+// none are left. An item is one of a tile's 256 / NT sub-blocks (the tile shape of the
+// launch: 16 x 16, 16 x 8 or 8 x 8 pixels, each walking its tile's whole list -- the
+// reference's Metal rasterizer runs 8 x 8 thread groups inside its 16 x 16 bins). A
+// tile's image equals what the per-view kernel renders: the same list (the batch sort
+// keeps each tile's order) and the same per-pixel code.
+template <int FB, int NT>
+__global__ void __launch_bounds__(NT, 4 * FWD_THREADS / NT) raster_fwd_batch_kernel(const BatchDesc d, int *counter) {
+    constexpr int SUB = FWD_THREADS / NT;
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
-    __shared__ int s_tile, s_lt;
+    __shared__ int s_item, s_lt;
     __shared__ RasterArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
     __shared__ double etab[EXP_TABLE];
     exp_table_init(etab);  // ready after the loop's first barrier
-    const int total_tiles = d.tile_off[d.n_views];  // read on the device: the launch is graph-capturable
+    const int total_items = d.tile_off[d.n_views] * SUB;  // read on the device: the launch is graph-capturable
     for (;;) {
-        __syncthreads();  // the previous tile's shared state is no longer read
+        __syncthreads();  // the previous item's shared state is no longer read
         if (threadIdx.x == 0) {
-            const int t = atomicAdd(counter, 1);
-            s_tile = t;
-            if (t < total_tiles) {
+            const int it = atomicAdd(counter, 1);
+            s_item = it;
+            if (it < total_items) {
+                const int t = it / SUB;
                 const int v = find_view(d.tile_off, d.n_views, t);
                 s_args = d.raster[v];
                 s_lt = t - d.tile_off[v];
             }
         }
         __syncthreads();
-        const int t = s_tile, lt = s_lt;
-        if (t >= total_tiles) break;
-        raster_fwd_tile<FB>(s_args, t, lt % s_args.tiles_x, lt / s_args.tiles_x, s0, s1, s2, sm, etab);
+        const int it = s_item, lt = s_lt;
+        if (it >= total_items) break;
+        raster_fwd_tile<FB, false, false, false, NT>(s_args, it / SUB, lt % s_args.tiles_x, lt / s_args.tiles_x, s0,
+                                                     s1, s2, sm, etab, nullptr, 0, 0, it % SUB);
     }
 }
 
@@ -257,21 +285,33 @@ int resident_grid(K kernel, size_t smem, int threads = TILE_PIX) {
     return std::max(1, sms * std::max(per_sm, 1));
 }
 
-template <int FB>
+template <int FB, int NT>
 void fwd_batch_launch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st) {
-    // once per variant, thread-safe
-    static const int grid = resident_grid(raster_fwd_batch_kernel<FB>, 0, FWD_THREADS);
-    const int g = tiles_hint > 0 ? std::min(grid, tiles_hint) : grid;
-    raster_fwd_batch_kernel<FB><<<g, FWD_THREADS, 0, st>>>(d, d_counter);
+    // once per variant and shape, thread-safe
+    static const int grid = resident_grid(raster_fwd_batch_kernel<FB, NT>, 0, NT);
+    const int items = tiles_hint * (FWD_THREADS / NT);
+    const int g = tiles_hint > 0 ? std::min(grid, items) : grid;
+    raster_fwd_batch_kernel<FB, NT><<<g, NT, 0, st>>>(d, d_counter);
 }
 
-// tiles_hint: the batch's tile count when the host knows it (caps the grid), else 0
-void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant) {
-    cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+template <int NT>
+void fwd_batch_staging(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant) {
     switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
-        case 64: fwd_batch_launch<64>(d, tiles_hint, d_counter, st); break;
-        case 256: fwd_batch_launch<256>(d, tiles_hint, d_counter, st); break;
-        default: fwd_batch_launch<128>(d, tiles_hint, d_counter, st); break;
+        case 64: fwd_batch_launch<64, NT>(d, tiles_hint, d_counter, st); break;
+        case 256: fwd_batch_launch<256, NT>(d, tiles_hint, d_counter, st); break;
+        default: fwd_batch_launch<128, NT>(d, tiles_hint, d_counter, st); break;
+    }
+}
+
+// tiles_hint: the batch's tile count when the host knows it (caps the grid), else 0;
+// shape: RASTER_SHAPES index (16 x 16, 16 x 8 or 8 x 8 pixels a block)
+void launch_raster_fwd_batch(const BatchDesc &d, int tiles_hint, int *d_counter, cudaStream_t st, int variant,
+                             int shape) {
+    cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+    switch (shape_index(shape)) {
+        case 1: fwd_batch_staging<FWD_THREADS / 2>(d, tiles_hint, d_counter, st, variant); break;
+        case 2: fwd_batch_staging<FWD_THREADS / 4>(d, tiles_hint, d_counter, st, variant); break;
+        default: fwd_batch_staging<FWD_THREADS>(d, tiles_hint, d_counter, st, variant); break;
     }
 }
 
@@ -646,31 +686,40 @@ __global__ void __launch_bounds__(BWD_THREADS, 5) raster_bwd_batch_kernel(const 
     }
 }
 
-template <int FB>
+template <int FB, bool AUX, bool TS, int NT>
 void fwd_launch(const RasterArgs &a, int T, cudaStream_t st) {
-    raster_fwd_kernel<FB><<<T, FWD_THREADS, 0, st>>>(a);
+    raster_fwd_kernel<FB, AUX, TS, NT><<<T * (FWD_THREADS / NT), NT, 0, st>>>(a);
+}
+
+template <int FB, bool AUX, bool TS>
+void fwd_launch_shape(const RasterArgs &a, int T, cudaStream_t st, int shape) {
+    switch (shape_index(shape)) {
+        case 1: fwd_launch<FB, AUX, TS, FWD_THREADS / 2>(a, T, st); break;
+        case 2: fwd_launch<FB, AUX, TS, FWD_THREADS / 4>(a, T, st); break;
+        default: fwd_launch<FB, AUX, TS, FWD_THREADS>(a, T, st); break;
+    }
 }
 
 // The aux forward runs the default staging only (the reference too forces one
 // rasterizer in this mode, core/metal/bindings.h:44-46).
-void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st) {
+void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st, int shape) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
-    if (a.tstore) raster_fwd_kernel<128, true, true><<<T, FWD_THREADS, 0, st>>>(a);
-    else raster_fwd_kernel<128, true><<<T, FWD_THREADS, 0, st>>>(a);
+    if (a.tstore) fwd_launch_shape<128, true, true>(a, T, st, shape);
+    else fwd_launch_shape<128, true, false>(a, T, st, shape);
 }
 
-void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant) {
+void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant, int shape) {
     const int T = a.tiles_x * a.tiles_y;
     if (T <= 0) return;
     if (a.tstore) {  // stored-transmittance mode: the default staging only
-        raster_fwd_kernel<128, false, true><<<T, FWD_THREADS, 0, st>>>(a);
+        fwd_launch_shape<128, false, true>(a, T, st, shape);
         return;
     }
     switch (RASTER_VARIANTS[variant_index(variant)].fwd_batch) {
-        case 64: fwd_launch<64>(a, T, st); break;
-        case 256: fwd_launch<256>(a, T, st); break;
-        default: fwd_launch<128>(a, T, st); break;
+        case 64: fwd_launch_shape<64, false, false>(a, T, st, shape); break;
+        case 256: fwd_launch_shape<256, false, false>(a, T, st, shape); break;
+        default: fwd_launch_shape<128, false, false>(a, T, st, shape); break;
     }
 }
 

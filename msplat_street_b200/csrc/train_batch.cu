@@ -72,6 +72,7 @@ struct StepArgs {
     float *vis, *gn, *ms;
     float *const *grads;
     int variant;  // rasterizer staging variant
+    int shape;    // batched forward's block shape (RASTER_SHAPES)
 };
 
 // Device pointers of one step, derived from the context's buffers.
@@ -330,7 +331,7 @@ void enqueue_rest(const StepArgs &a, const StepPtrs &P, int64_t isect_cap, int t
     launch_tile_ranges(kk[cur], cap, tile_cap, P.tile_start, P.tile_end, st, d_n, d.tile_off + a.nv);
     launch_isect_map(vv[cur], cap, P.emit_gid, P.isect_gid, P.inv, st, d_n);
     if (tm) tm->mark(2, st);
-    launch_raster_fwd_batch(d, tiles_hint, P.counters + C_RAS, st, a.variant);
+    launch_raster_fwd_batch(d, tiles_hint, P.counters + C_RAS, st, a.variant, a.shape);
     if (tm) tm->mark(3, st);
     launch_ssim_loss_batch(reinterpret_cast<const SsimArgs *>(P.desc + L.ssim),
                            reinterpret_cast<const int *>(P.desc + L.boff), a.nv, P.counters + C_SSIM, st);
@@ -383,7 +384,7 @@ std::vector<uint64_t> graph_key(const StepArgs &a, const StepPtrs &P, int64_t is
         std::memcpy(&b, &x, 4);
         k.push_back(b);
     };
-    u(a.n), u(a.nv), u(a.degree), u(a.dtu), u(a.adam_groups), u(isect_cap), u(tile_cap), u(a.variant);
+    u(a.n), u(a.nv), u(a.degree), u(a.dtu), u(a.adam_groups), u(isect_cap), u(tile_cap), u(a.variant), u(a.shape);
     f(a.glob_scale), f(a.beta1), f(a.beta2), f(a.eps);
     for (int g = 0; g < 6; g++) {
         u((uintptr_t)a.p[g]);
@@ -579,6 +580,7 @@ extern "C" int msplat_cuda_train_batch(msplat_cuda_ctx *ctx, int num_points, flo
     a.ms = max_2d_size;
     a.grads = grads_out;
     a.variant = ctx->raster_variant;
+    a.shape = ctx->raster_shape;
     if (int r = check_step(a)) return r;
     const Sizes sz = sizes_of(a);
     if (sz.inst >= (int64_t)INT32_MAX || sz.tiles >= (int64_t)INT32_MAX || sz.pix >= (int64_t)INT32_MAX)
