@@ -251,7 +251,8 @@ def run_ours(args, world, rank, local):
     ctx.enable_stage_timing(True)
     ctx.drain_stage_times()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    n_isects, pairs, n_gauss = [], [], []
+    n_isects, n_gauss = [], []
+    pair_sum = torch.zeros(2, dtype=torch.int64, device=dev)
     window = {"first": trainer.iteration + 1, "sh_first": trainer.degrees_to_use(trainer.iteration + 1),
               "gaussians_first": trainer.splat_count, "densify": []}
     barrier(world, dev)
@@ -263,12 +264,13 @@ def run_ours(args, world, rank, local):
             evs[i][0].record()
             st = trainer.step()
             evs[i][1].record()
-            n_isects.append(ctx.num_isects())
-            pairs.append(ctx.pair_counts())  # outside the events: a counting kernel and a readback
+            n_isects.append(ctx.num_isects())  # known on the host since the step's binning
+            ctx.add_pair_counts(pair_sum)  # outside the events: a counting kernel, no readback
             if st.splat_count != n_gauss[-1]:
                 window["densify"].append(st.iteration)
         torch.cuda.synchronize()
     barrier(world, dev)
+    pairs = [tuple(float(x) / args.steps for x in pair_sum.cpu().tolist())]  # per-step means
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(sum(step_ms), world, dev)
     stages = ctx.drain_stage_times()

@@ -93,6 +93,10 @@ int msplat_cuda_raster_shape(int s, int32_t *w, int32_t *h);
  * entry that ends it, or to the end), out[1] for the backward (:959-1031: from the
  * pixel's last contributor down). Synchronises the context's stream. */
 int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out);
+/* The same counts added into d_sum[0..1] (device memory, two uint64) on the
+ * context's stream, without synchronising: a training loop sums its steps' pairs and
+ * reads them once. */
+int msplat_cuda_frame_pair_counts_device(msplat_cuda_ctx *ctx, uint64_t *d_sum);
 /* No counterpart in the reference (test hook). The rasterizers' exponential -- exp(x)
  * for x in [-700, 0], Tang's table-driven method in double precision, rounded once to
  * float -- of n device inputs into out, on the context's stream. */

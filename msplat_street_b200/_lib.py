@@ -62,6 +62,7 @@ _SIGS = {
     "msplat_cuda_frame": (i32, [vp, C.c_char_p, PP, C.POINTER(i64)]),
     "msplat_cuda_num_isects": (i64, [vp]),
     "msplat_cuda_frame_pair_counts": (i32, [vp, vp]),
+    "msplat_cuda_frame_pair_counts_device": (i32, [vp, vp]),
     "msplat_cuda_device_alloc": (i32, [sz, PP]),
     "msplat_cuda_rasterizer_exp": (i32, [vp, vp, i64, vp]),
     "msplat_cuda_ctx_device_bytes": (i64, [vp]),

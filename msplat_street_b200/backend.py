@@ -605,6 +605,14 @@ class Context:
         check(self._lib.msplat_cuda_frame_pair_counts(self.handle, C.c_void_p(out.ctypes.data)))
         return int(out[0]), int(out[1])
 
+    def add_pair_counts(self, acc: torch.Tensor) -> None:
+        """Adds the last single-view frame's (forward, backward) pair counts into
+        ``acc`` (a CUDA int64 tensor of 2) on the context's stream, without
+        synchronising."""
+        if acc.dtype != torch.int64 or not acc.is_cuda or acc.numel() < 2 or not acc.is_contiguous():
+            raise ValueError("acc must be a contiguous CUDA int64 tensor of at least 2 elements")
+        check(self._lib.msplat_cuda_frame_pair_counts_device(self.handle, ptr(acc)))
+
     def enable_stage_timing(self, on: bool = True) -> None:
         check(self._lib.msplat_cuda_ctx_set_option(self.handle, b"stage_timing", int(on)))
 

@@ -185,12 +185,26 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     launch_project(pa, st);
     launch_depth_offsets(n, splats, n_tiles, ds, offsets, d_total, scan_part, st);
     CUDA_TRY(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    if (!ctx->total_ev) CUDA_TRY(cudaEventCreateWithFlags(&ctx->total_ev, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(ctx->total_ev, st));
+    // The key emission needs the count only for its buffers' size: it is queued before
+    // the host waits for the count, into the buffers as they are (entries past their
+    // capacity dropped), so the device runs it while the host reads the count and
+    // queues the rest; when the buffers were too small it runs again below.
+    ctx->timer.mark(1, st);
+    const int64_t cap0 = (int64_t)std::min({ctx->keys[0].bytes, ctx->vals[0].bytes, ctx->emit_gid.bytes}) / 4;
+    if (cap0 > 0 && n > 0)
+        launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y,
+                         reinterpret_cast<uint32_t *>(ctx->keys[0].ptr), reinterpret_cast<uint32_t *>(ctx->vals[0].ptr),
+                         reinterpret_cast<int32_t *>(ctx->emit_gid.ptr), st, cap0);
+    CUDA_TRY(cudaEventSynchronize(ctx->total_ev));
     const int64_t n_isect = *ctx->h_total;
     if (n_isect > (int64_t)INT32_MAX)
         return fail(MSPLAT_CUDA_EOVERFLOW, "more than 2^31 tile intersections (%lld); lower the resolution",
                     (long long)n_isect);
     ctx->n_isect = n_isect;
+    const bool emitted = cap0 > 0 && n_isect <= cap0;
+    if (!emitted) CUDA_TRY(cudaStreamSynchronize(st));  // the early emission is done before buffers move
     ENSURE(ctx->keys[0], n_isect, uint32_t, k0);
     ENSURE(ctx->keys[1], n_isect, uint32_t, k1);
     ENSURE(ctx->vals[0], n_isect, uint32_t, v0);
@@ -200,8 +214,8 @@ int forward(msplat_cuda_ctx *ctx, int n, const float *means, const float *scales
     ENSURE(ctx->inv, n_isect, int32_t, inv);
     ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n_isect), unsigned char, rscratch);
 
-    ctx->timer.mark(1, st);
-    launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y, k0, v0, emit_gid, st);
+    if (!emitted)
+        launch_emit_keys(n, splats, aabb, n_tiles, offsets, cam.tiles_x, cam.tiles_y, k0, v0, emit_gid, st);
     uint32_t *kk[2] = {k0, k1};
     uint32_t *vv[2] = {v0, v1};
     const int cur = radix_sort_pairs32(kk, vv, (int)n_isect, ceil_log2(std::max(T, 1)), rscratch, st);
@@ -1239,12 +1253,9 @@ int msplat_cuda_rasterizer_exp(msplat_cuda_ctx *ctx, const float *x, int64_t n, 
     return MSPLAT_CUDA_OK;
 }
 
-int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out) {
-    if (!ctx || !out) return fail(MSPLAT_CUDA_EINVAL, "null argument");
-    out[0] = out[1] = 0;
-    if (ctx->tiles_x <= 0 || ctx->tiles_y <= 0 || !ctx->tile_start.ptr || !ctx->final_idx.ptr) return MSPLAT_CUDA_OK;
-    if (ctx->gid_in_vals) return fail(MSPLAT_CUDA_EINVAL, "the last frame was a batched render");
-    ENSURE(ctx->pairs, 2, unsigned long long, d);
+namespace {
+// The pair counter's view of the context's last single-view frame.
+RasterArgs pair_count_args(const msplat_cuda_ctx *ctx) {
     RasterArgs a{};
     a.W = ctx->W;
     a.H = ctx->H;
@@ -1255,12 +1266,31 @@ int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out) {
     a.isect_gid = reinterpret_cast<const int32_t *>(ctx->isect_gid.ptr);
     a.splats = reinterpret_cast<const Splat *>(ctx->splats.ptr);
     a.final_idx = reinterpret_cast<int32_t *>(ctx->final_idx.ptr);
-    launch_pair_counts(a, d, ctx->stream);
+    return a;
+}
+}  // namespace
+
+int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out) {
+    if (!ctx || !out) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    out[0] = out[1] = 0;
+    if (ctx->tiles_x <= 0 || ctx->tiles_y <= 0 || !ctx->tile_start.ptr || !ctx->final_idx.ptr) return MSPLAT_CUDA_OK;
+    if (ctx->gid_in_vals) return fail(MSPLAT_CUDA_EINVAL, "the last frame was a batched render");
+    ENSURE(ctx->pairs, 2, unsigned long long, d);
+    launch_pair_counts(pair_count_args(ctx), d, ctx->stream);
     unsigned long long h[2] = {0, 0};
     CUDA_TRY(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     out[0] = (int64_t)h[0];
     out[1] = (int64_t)h[1];
+    return MSPLAT_CUDA_OK;
+}
+
+int msplat_cuda_frame_pair_counts_device(msplat_cuda_ctx *ctx, uint64_t *d_sum) {
+    if (!ctx || !d_sum) return fail(MSPLAT_CUDA_EINVAL, "null argument");
+    if (ctx->tiles_x <= 0 || ctx->tiles_y <= 0 || !ctx->tile_start.ptr || !ctx->final_idx.ptr) return MSPLAT_CUDA_OK;
+    if (ctx->gid_in_vals) return fail(MSPLAT_CUDA_EINVAL, "the last frame was a batched render");
+    launch_pair_counts(pair_count_args(ctx), reinterpret_cast<unsigned long long *>(d_sum), ctx->stream, true);
+    CUDA_TRY(cudaGetLastError());
     return MSPLAT_CUDA_OK;
 }
 

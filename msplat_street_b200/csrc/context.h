@@ -176,7 +176,7 @@ constexpr int CHUNK_AUTO_TILES = 400;  // core/metal/msplat_metal.mm:1103
 struct msplat_cuda_ctx {
     cudaStream_t stream = nullptr;
     int raster_variant = 0;  // option "raster_variant": index into RASTER_VARIANTS
-    int raster_shape = 0;    // option "raster_shape": index into RASTER_SHAPES (batched forward)
+    int raster_shape = 0;    // option "raster_shape": index into RASTER_SHAPES (forward rasterizers)
     TrainBatchState tb;
     bool keep_grads = false;
     StageTimer timer;
@@ -215,6 +215,7 @@ struct msplat_cuda_ctx {
     msplat_cuda_prior prior{};
     Buf pri[PB_COUNT];
     int64_t *h_total = nullptr;  // pinned readback of the intersection count
+    cudaEvent_t total_ev = nullptr;  // recorded after that readback
     int32_t *h_count = nullptr;  // pinned readback of the densified count
     // batched render: device view descriptors, their pinned staging copy, the
     // persistent rasterizer's work counter, and an event after the last upload
@@ -255,6 +256,8 @@ struct msplat_cuda_ctx {
         tb.release();  // its graph refers to the buffers just freed
         if (h_total) cudaFreeHost(h_total);
         h_total = nullptr;
+        if (total_ev) cudaEventDestroy(total_ev);
+        total_ev = nullptr;
         if (h_count) cudaFreeHost(h_count);
         h_count = nullptr;
         if (h_bdesc) cudaFreeHost(h_bdesc);

@@ -52,8 +52,10 @@ void launch_depth_offsets(int n, const Splat *splats, const int32_t *n_tiles, De
                           int64_t *d_total, int64_t *scan_part, cudaStream_t st);
 // Emission: key = tile id (global tile id in a batch), value = emission index, or
 // the Gaussian id when emit_gid is null (render only: no backward needs the map).
+// cap: entries at or past it are not written (the buffers' capacity)
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
-                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st);
+                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st,
+                      int64_t cap = INT64_MAX);
 size_t radix_scratch_bytes(int n);
 // d_n / d_T (optional): device-side counts capping the host-side capacities n / T
 int radix_sort_pairs(uint64_t *k[2], uint32_t *v[2], int n, int key_bits, void *scratch, cudaStream_t st,
@@ -108,8 +110,8 @@ inline int shape_index(int s) { return (s >= 0 && s < N_RASTER_SHAPES) ? s : 0; 
 
 void launch_raster_fwd(const RasterArgs &a, cudaStream_t st, int variant = 0, int shape = 0);
 // (pixel, Gaussian) pairs the reference's forward / backward loops evaluate over the
-// frame (out[0], out[1]; device counters)
-void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st);
+// frame (out[0], out[1]; device counters, zeroed first unless accumulate)
+void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st, bool accumulate = false);
 // the rasterizers' exponential (exp_tab) of n device inputs
 void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st);
 void launch_raster_fwd_aux(const RasterArgs &a, cudaStream_t st, int shape = 0);

@@ -853,9 +853,9 @@ void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st) {
     exp_tab_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, n, out);
 }
 
-void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st) {
+void launch_pair_counts(const RasterArgs &a, unsigned long long *d_out, cudaStream_t st, bool accumulate) {
     const int T = a.tiles_x * a.tiles_y;
-    cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), st);
+    if (!accumulate) cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), st);
     if (T > 0) pair_count_kernel<<<T, TILE_PIX, 0, st>>>(a, d_out);
 }
 

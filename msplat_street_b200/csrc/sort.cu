@@ -314,11 +314,12 @@ EmitSrc emit_src(const int32_t *n_tiles, const int64_t *offsets, const DepthScra
 }  // namespace
 
 void launch_emit_keys(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles, const int64_t *offsets,
-                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st) {
-    if (n <= 0) return;
+                      int tiles_x, int tiles_y, uint32_t *keys, uint32_t *vals, int32_t *emit_gid, cudaStream_t st,
+                      int64_t cap) {
+    if (n <= 0 || cap <= 0) return;
     emit_keys_kernel<false, false><<<(n + 127) / 128, 128, 0, st>>>(
         n, splats, aabb, emit_src(n_tiles, offsets, nullptr), tiles_x, tiles_y, BatchDesc{}, keys, vals, emit_gid,
-        INT64_MAX);
+        cap);
 }
 
 void launch_emit_keys_batch(int n, const Splat *splats, const float *aabb, const int32_t *n_tiles,

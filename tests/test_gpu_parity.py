@@ -272,3 +272,8 @@ def test_pair_counts_follow_the_reference_loops(oracle):
             fwd += max(0, stop - s)
     assert got == (fwd, bwd), (got, fwd, bwd)
     assert fwd >= bwd > 0
+    # the device-side form adds into a running sum without synchronising
+    acc = torch.tensor([5, 7], dtype=torch.int64, device="cuda")
+    ctx.add_pair_counts(acc)
+    ctx.add_pair_counts(acc)
+    assert acc.tolist() == [5 + 2 * fwd, 7 + 2 * bwd]
