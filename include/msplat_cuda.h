@@ -99,7 +99,10 @@ int msplat_cuda_frame_pair_counts(msplat_cuda_ctx *ctx, int64_t *out);
 int msplat_cuda_frame_pair_counts_device(msplat_cuda_ctx *ctx, uint64_t *d_sum);
 /* No counterpart in the reference (test hook). The rasterizers' exponential -- exp(x)
  * for x in [-700, 0], Tang's table-driven method in double precision, rounded once to
- * float -- of n device inputs into out, on the context's stream. */
+ * float -- of n device inputs into out, on the context's stream. Over [-5.55, 0] it
+ * runs both forms the kernels use (the forward's table of 2^(k/64) spanning the range
+ * and the backward's 64-entry table with the power of two applied to the exponent)
+ * and writes NaN wherever they differ. */
 int msplat_cuda_rasterizer_exp(msplat_cuda_ctx *ctx, const float *x, int64_t n, float *out);
 /* Bytes of device memory the context's caches hold. */
 int64_t msplat_cuda_ctx_device_bytes(msplat_cuda_ctx *ctx);

@@ -78,6 +78,38 @@ __device__ __forceinline__ float exp_tab(float xf, const double *t) {
     return (float)__hiloint2double(__double2hiint(v) + m * (1 << 20), __double2loint(v));
 }
 
+// The same exponential with the power of two folded into the table, for x in
+// [-5.55, 0] (-sigma over the rasterizers' range): entry i = 2^m 2^(j/64) for
+// ki = -i = 64 m + j, the old table's entry scaled exactly, so v = entry * p is the
+// old t[j] * p scaled by 2^m -- the same double, rounded to the same float -- with the
+// exponent-field arithmetic gone. Indices past the span are clamped (not reached for
+// x >= -5.55). The block fills the table in two steps with one barrier between
+// (exp_span_init_a, __syncthreads, exp_span_init_b).
+constexpr int EXP_SPAN = 520;  // covers ki = round(x 64 / ln 2) down to -519 (x >= -5.62)
+
+__device__ __forceinline__ void exp_span_init_a(double *t64) { exp_table_init(t64); }
+__device__ __forceinline__ void exp_span_init_b(double *span, const double *t64) {
+    for (int i = threadIdx.x; i < EXP_SPAN; i += blockDim.x) {
+        const int ki = -i;
+        span[i] = scalbn(t64[ki & (EXP_TABLE - 1)], ki >> 6);
+    }
+}
+
+__device__ __forceinline__ float exp_span(float xf, const double *span) {
+    const double x = (double)xf;
+    const double shifted = fma(x, EXP_INV_LN2_64, 0x1.8p52);
+    const int ki = __double2loint(shifted);
+    const double k = shifted - 0x1.8p52;
+    double r = fma(-k, EXP_LN2_64_HI, x);
+    r = fma(-k, EXP_LN2_64_LO, r);
+    double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    return (float)(span[min(-ki, EXP_SPAN - 1)] * p);
+}
+
 // Two float32 values in one 64-bit register pair, for sm_100's packed FP32
 // instructions (PTX add / mul / fma .rn.f32x2): one instruction issues two IEEE
 // single-precision operations, each rounded exactly as its scalar form, so packing

@@ -114,7 +114,7 @@ __device__ __forceinline__ int sub_tile_thread(int t, int q) {
 // write the piece's transmittance, colour and last contributor to item `item`.
 template <int FB, bool AUX = false, bool CHUNK = false, bool TS = false, int NT = FWD_THREADS>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, int tx, int ty, float4 *s0,
-                                                float4 *s1, float4 *s2, uint8_t *sm, const double *etab,
+                                                float4 *s1, float4 *s2, uint8_t *sm, const double *espan,
                                                 const ChunkArgs *ck = nullptr, int item = 0, int chunk = 0,
                                                 int q = 0) {
     static_assert(!CHUNK || NT == FWD_THREADS, "depth pieces are composited by whole-tile blocks");
@@ -165,7 +165,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
                 const float dx = A.x - fpx, dy = A.y - fpy;
                 const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
                 if (sigma < 0.f || sigma >= 5.55f || sigma > C.z) continue;
-                const float alpha = fminf(0.999f, B.y * exp_tab(-sigma, etab));
+                const float alpha = fminf(0.999f, B.y * exp_span(-sigma, espan));
                 if (alpha < 1.f / 255.f) continue;
                 const float nT = T * (1.f - alpha);
                 if (nT <= 1e-4f) {
@@ -231,10 +231,12 @@ __global__ void __launch_bounds__(NT, 4 * FWD_THREADS / NT) raster_fwd_kernel(Ra
     constexpr int SUB = FWD_THREADS / NT;
     __shared__ float4 s0[FB], s1[FB], s2[FB];
     __shared__ uint8_t sm[FB];
-    __shared__ double etab[EXP_TABLE];
-    exp_table_init(etab);  // ready after the tile's first barrier
+    __shared__ double et64[EXP_TABLE], espan[EXP_SPAN];
+    exp_span_init_a(et64);
+    __syncthreads();
+    exp_span_init_b(espan, et64);  // ready after the tile's first barrier
     const int tile = blockIdx.x / SUB;
-    raster_fwd_tile<FB, AUX, false, TS, NT>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab,
+    raster_fwd_tile<FB, AUX, false, TS, NT>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, espan,
                                             nullptr, 0, 0, blockIdx.x % SUB);
 }
 
@@ -252,8 +254,10 @@ __global__ void __launch_bounds__(NT, 4 * FWD_THREADS / NT) raster_fwd_batch_ker
     __shared__ uint8_t sm[FB];
     __shared__ int s_item, s_lt;
     __shared__ RasterArgs s_args;  // the tile's view, read from shared memory (keeps registers down)
-    __shared__ double etab[EXP_TABLE];
-    exp_table_init(etab);  // ready after the loop's first barrier
+    __shared__ double et64[EXP_TABLE], espan[EXP_SPAN];
+    exp_span_init_a(et64);
+    __syncthreads();
+    exp_span_init_b(espan, et64);  // ready after the loop's first barrier
     const int total_items = d.tile_off[d.n_views] * SUB;  // read on the device: the launch is graph-capturable
     for (;;) {
         __syncthreads();  // the previous item's shared state is no longer read
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(NT, 4 * FWD_THREADS / NT) raster_fwd_batch_ker
         const int it = s_item, lt = s_lt;
         if (it >= total_items) break;
         raster_fwd_tile<FB, false, false, false, NT>(s_args, it / SUB, lt % s_args.tiles_x, lt / s_args.tiles_x, s0,
-                                                     s1, s2, sm, etab, nullptr, 0, 0, it % SUB);
+                                                     s1, s2, sm, espan, nullptr, 0, 0, it % SUB);
     }
 }
 
@@ -838,13 +842,21 @@ __global__ void __launch_bounds__(TILE_PIX) pair_count_kernel(RasterArgs a, unsi
     }
 }
 
-// The rasterizers' exponential over n inputs (test hook for exp_tab against exp_ref).
+// The rasterizers' exponential over n inputs (test hook for exp_span / exp_tab
+// against exp_ref).
 __global__ void exp_tab_kernel(const float *x, int64_t n, float *out) {
-    __shared__ double etab[EXP_TABLE];
-    exp_table_init(etab);
+    __shared__ double etab[EXP_TABLE], espan[EXP_SPAN];
+    exp_span_init_a(etab);
     __syncthreads();
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = exp_tab(x[i], etab);
+    exp_span_init_b(espan, etab);
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        // over the rasterizers' range [-5.55, 0] the forward's span-table form, NaN
+        // wherever it differs from the 64-entry form the backward uses (the two are the
+        // same function by construction); below it the 64-entry form
+        const float xi = x[i], v = exp_tab(xi, etab);
+        out[i] = xi < -5.55f ? v : (exp_span(xi, espan) == v ? v : __int_as_float(0x7fc00000));
+    }
 }
 
 void launch_exp_tab(const float *x, int64_t n, float *out, cudaStream_t st) {
@@ -898,9 +910,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 4) raster_fwd_chunk_kernel(Raster
     const int T = a.tiles_x * a.tiles_y, item = blockIdx.x;
     if (item >= c.first[T]) return;  // block-uniform
     const int tile = chunk_tile(c.first, T, item);
-    __shared__ double etab[EXP_TABLE];
-    exp_table_init(etab);  // ready after the tile's first barrier
-    raster_fwd_tile<FB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, etab, &c, item,
+    __shared__ double et64[EXP_TABLE], espan[EXP_SPAN];
+    exp_span_init_a(et64);
+    __syncthreads();
+    exp_span_init_b(espan, et64);  // ready after the tile's first barrier
+    raster_fwd_tile<FB, false, true>(a, tile, tile % a.tiles_x, tile / a.tiles_x, s0, s1, s2, sm, espan, &c, item,
                                      item - c.first[tile]);
 }
 
