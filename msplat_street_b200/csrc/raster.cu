@@ -41,6 +41,10 @@
 
 namespace msplat {
 
+// The float just below 5.55: sigma >= 5.55f is sigma > SIGMA_SKIP.
+constexpr float SIGMA_SKIP = 0x1.633332p+2f;  // 5.5499997
+static_assert(SIGMA_SKIP < 5.55f && SIGMA_SKIP + 0x1p-21f == 5.55f, "the float below 5.55f (ulp 2^-21 there)");
+
 // the forward's block: one thread per pixel (8 x 4 pixels per warp); the backward's:
 // 128 threads, two pixels each (8 x 8 pixels per warp)
 constexpr int FWD_THREADS = TILE_PIX;
@@ -143,13 +147,16 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
             if (k >= end) break;
             const float4 *rec = reinterpret_cast<const float4 *>(a.splats + a.isect_gid[k]);
             const float4 A = rec[0], B = rec[1], C = rec[2];
-            s0[si] = A;
-            s1[si] = make_float4(B.x, B.y, staged_colour(B.z), staged_colour(B.w));
-            // z: the sigma above which alpha = o exp(-sigma) < 1/255 for certain,
-            // ln(255 o) plus a margin far above the roundings of logf, of exp_tab and
-            // of the product, so a pixel past it skips the exponential with the
-            // decision the exact test would take
-            s2[si] = make_float4(staged_colour(C.x), C.y, logf(255.f * B.y) + 1e-3f, C.w);
+            // the conic's diagonal halved: 0.5 (a dx dx + c dy dy) == (a/2) dx dx +
+            // (c/2) dy dy bit for bit (scaling by 2^-1 commutes with each rounding)
+            s0[si] = make_float4(A.x, A.y, 0.5f * A.z, A.w);
+            s1[si] = make_float4(0.5f * B.x, B.y, staged_colour(B.z), staged_colour(B.w));
+            // z: the sigma above which the pixel skips the splat -- the smaller of the
+            // float below 5.55 (sigma >= 5.55 is sigma > that float) and the sigma above
+            // which alpha = o exp(-sigma) < 1/255 for certain, ln(255 o) plus a margin
+            // far above the roundings of logf, of the exponential and of the product --
+            // so one compare takes both decisions the exact tests would take
+            s2[si] = make_float4(staged_colour(C.x), C.y, fminf(logf(255.f * B.y) + 1e-3f, SIGMA_SKIP), C.w);
             sm[si] = (uint8_t)warp_block_mask(A, C, tx, ty);
         }
         __syncthreads();
@@ -163,8 +170,8 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs &a, int tile, i
                 bits &= bits - 1u;
                 const float4 A = s0[j], B = s1[j], C = s2[j];
                 const float dx = A.x - fpx, dy = A.y - fpy;
-                const float sigma = 0.5f * (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;
-                if (sigma < 0.f || sigma >= 5.55f || sigma > C.z) continue;
+                const float sigma = (A.z * dx * dx + B.x * dy * dy) + A.w * dx * dy;  // A.z, B.x halved
+                if (sigma < 0.f || sigma > C.z) continue;
                 const float alpha = fminf(0.999f, B.y * exp_span(-sigma, espan));
                 if (alpha < 1.f / 255.f) continue;
                 const float nT = T * (1.f - alpha);
@@ -478,10 +485,12 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
             const uint32_t m8 = warp_block_mask(A, C, tx, ty);
             sm[threadIdx.x] = (uint8_t)(((m8 | (m8 >> 2)) & 3u) | ((((m8 >> 4) | (m8 >> 6)) & 3u) << 2));
             hitw[threadIdx.x] = 0u;
-            // staged: (x, y, conic a, conic c), (conic b, opacity, colour r, g), (colour b, depth)
-            s0[threadIdx.x] = make_float4(A.x, A.y, A.z, B.x);
+            // staged: (x, y, a / 2, c / 2), (conic b, opacity, colour r, g), (colour b,
+            // depth, a, c) -- the halved diagonal for sigma (0.5 (a dx dx + c dy dy) ==
+            // (a/2) dx dx + (c/2) dy dy bit for bit), the whole one for the gradients
+            s0[threadIdx.x] = make_float4(A.x, A.y, 0.5f * A.z, 0.5f * B.x);
             s1[threadIdx.x] = make_float4(A.w, B.y, staged_colour(B.z), staged_colour(B.w));
-            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, C.z, C.w);
+            s2[threadIdx.x] = make_float4(staged_colour(C.x), C.y, A.z, B.x);
         }
         __syncthreads();
         // This warp's reachable splats, back to front, 32 mask bits per ballot. Splats
@@ -508,12 +517,12 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                 // following packed add (dx is the pixels' shared column)
                 const float dx = A.x - fpx;
                 const float dy[2] = {A.y - fpy[0], A.y - fpy[1]};
-                const float adx = A.z * dx, bdx = B.x * dx;
+                const float hadx2 = A.z * dx * dx, bdx = B.x * dx;  // A.z, A.w: a / 2, c / 2
                 float al[2];
                 bool hit[2];
 #pragma unroll
                 for (int i = 0; i < 2; i++) {
-                    const float sigma = 0.5f * (A.z * dx * dx + A.w * dy[i] * dy[i]) + B.x * dx * dy[i];
+                    const float sigma = (hadx2 + A.w * dy[i] * dy[i]) + bdx * dy[i];
                     hit[i] = false;
                     al[i] = 0.f;
                     if (inside[i] && k <= kf[i] && sigma >= 0.f && sigma < 5.55f) {
@@ -590,7 +599,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterBwdArgs &a, int tile
                     const f32x2 nal2 = pack2(hit[0] && al[0] < 0.999f ? -al[0] : 0.f,
                                              hit[1] && al[1] < 0.999f ? -al[1] : 0.f);
                     const f32x2 vs2 = mul2(nal2, va2), dx2 = pack2(dx, dx), dy2 = pack2(dy[0], dy[1]);
-                    const f32x2 cdy2 = mul2(pack2(A.w, A.w), dy2);
+                    const float adx = C.z * dx;  // the whole conic: C.z = a, C.w = c
+                    const f32x2 cdy2 = mul2(pack2(C.w, C.w), dy2);
                     const f32x2 m0 = mul2(vs2, dx2), m1 = mul2(vs2, dy2);
                     const float2 e0 = unpack2(mul2(vs2, fma2(pack2(B.x, B.x), dy2, pack2(adx, adx)))),
                                  e1 = unpack2(mul2(vs2, add2(pack2(bdx, bdx), cdy2))), e2 = unpack2(mul2(m0, dx2)),
