@@ -896,10 +896,13 @@ def schedule_sample(trainer, ctx, flush, dev, windows=SCHEDULE_WINDOWS) -> list:
                 dens.append(st.iteration)
             ms.append((e0, e1))
         torch.cuda.synchronize()
-        t = sum(x.elapsed_time(y) for x, y in ms)
+        per = [x.elapsed_time(y) for x, y in ms]
+        t = sum(per)
+        slow = int(np.argmax(per))
         out.append({"iterations": [a, b], "ms_per_step": t / len(ms), "iters_per_s": len(ms) / (t / 1e3),
                     "gaussians": [n0, trainer.splat_count], "sh_degree": trainer.degrees_to_use(),
-                    "densify_steps": dens, "isects_mean": float(np.mean(isects))})
+                    "densify_steps": dens, "isects_mean": float(np.mean(isects)),
+                    "slowest_step": {"iteration": a + slow, "ms": per[slow]}})
     return out
 
 
