@@ -138,26 +138,7 @@ __device__ __forceinline__ void warp_slot_sums(bool vis, int64_t g0, const int64
         my_cnt = n_tiles[g0 + lane];
     }
     if (vis && my_cnt <= SLOT_LANE_MAX) {
-        // two slots a step, both loaded before either is added (the adds keep slot
-        // order), so each step waits on one round of loads instead of two
-        int j = 0;
-        for (; j + 2 <= my_cnt; j += 2) {
-            const int32_t k0 = inv[my_e0 + j], k1 = inv[my_e0 + j + 1];
-            const float *a0 = slots + (size_t)k0 * 9, *a1 = slots + (size_t)k1 * 9;
-            float v0[9], v1[9];
-#pragma unroll
-            for (int c = 0; c < 9; c++) {
-                v0[c] = a0[c];
-                v1[c] = a1[c];
-            }
-#pragma unroll
-            for (int c = 0; c < 9; c++) s9[c] = (s9[c] + v0[c]) + v1[c];
-            if (slots_depth) {
-                const float d0 = slots_depth[k0], d1 = slots_depth[k1];
-                *sd = (*sd + d0) + d1;
-            }
-        }
-        if (j < my_cnt) {
+        for (int j = 0; j < my_cnt; j++) {
             const int32_t k = inv[my_e0 + j];
             const float *sl = slots + (size_t)k * 9;
 #pragma unroll
