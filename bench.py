@@ -908,7 +908,8 @@ def schedule_sample(trainer, ctx, flush, dev, windows=SCHEDULE_WINDOWS) -> list:
 
 def knn_rate(trainer, ctx, reps: int = 5) -> dict:
     """Exact 3-NN mean distance (the scale init) over the workload's initial point
-    cloud: points/s, CUDA events around each call."""
+    cloud: points/s and point-distance evaluations/s (counted on the device), CUDA
+    events around each call."""
     import torch
     pts = torch.from_numpy(trainer.ds.points).cuda()
     ctx.knn3_mean_dist(pts)
@@ -922,7 +923,9 @@ def knn_rate(trainer, ctx, reps: int = 5) -> dict:
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1))
     ms = statistics.median(ts)
-    return {"points": int(pts.shape[0]), "ms": ms, "points_per_s": pts.shape[0] / (ms * 1e-3)}
+    evals = int(ctx.frame("knn_evals").view(torch.int64)[0])  # the last call's (every call's) count
+    return {"points": int(pts.shape[0]), "ms": ms, "points_per_s": pts.shape[0] / (ms * 1e-3),
+            "distance_evals": evals, "distance_evals_per_s": evals / (ms * 1e-3)}
 
 
 PROFILE_CASES = ("sort", "ssim", "adam", "densify", "render")

@@ -366,7 +366,9 @@ int msplat_cuda_loss_device(msplat_cuda_ctx *ctx, const float **loss);
  * with option keep_grads, v_xy v_conic v_rgb v_opacity v_mean3d v_scale v_quat; with a
  * prior (msplat_cuda_set_prior): out_depth bg_img v_aux (dL/d depth numerator, dL/d
  * alpha per pixel) out_adj v_adj (exposure-adjusted render and its gradient) and,
- * with keep_grads, v_depth. *count is the element count (floats or int32). Device
+ * with keep_grads, v_depth; and knn_evals (one uint64 as two int32 words: the point
+ * distances the last msplat_cuda_knn3_mean_dist computed, 32 per query per candidate
+ * box its bounds test kept). *count is the element count (floats or int32). Device
  * pointers. */
 int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_ptr, int64_t *count);
 /* Number of tile intersections of the last frame. */

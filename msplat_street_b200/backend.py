@@ -18,7 +18,7 @@ from .camera import CameraSetup, logf
 from ._lib import check, lib
 
 PARAM_NAMES = ("means", "scales", "quats", "features_dc", "features_rest", "opacities")
-_FRAME_INT = {"radii", "tile_start", "tile_end", "isect_gid", "final_idx", "chunk_first"}
+_FRAME_INT = {"radii", "tile_start", "tile_end", "isect_gid", "final_idx", "chunk_first", "knn_evals"}
 
 
 def ptr(t: Optional[torch.Tensor]):

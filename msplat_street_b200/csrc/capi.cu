@@ -1140,7 +1140,9 @@ int msplat_cuda_knn3_mean_dist(msplat_cuda_ctx *ctx, const float *points, uint32
     ENSURE(ctx->radix_scratch, radix_scratch_bytes((int)n), unsigned char, rs);
     ENSURE(ctx->k_sorted, n, float4, sorted);
     ENSURE(ctx->k_box, 2 * (size_t)nb, float4, boxes);
+    ENSURE(ctx->k_evals, 1, unsigned long long, evals);
     KnnScratch s;
+    s.evals = evals;
     s.bounds = bounds;
     s.keys[0] = k0;
     s.keys[1] = k1;
@@ -1383,6 +1385,7 @@ int msplat_cuda_frame(msplat_cuda_ctx *ctx, const char *name, const void **dev_p
         {"out_adj", &ctx->pri[PB_ADJ], npix * 3},
         {"v_adj", &ctx->pri[PB_VADJ], npix * 3},
         {"chunk_first", &ctx->ch[CH_FIRST], ctx->chunk_frame ? T + 1 : 0},
+        {"knn_evals", &ctx->k_evals, 2},  // one uint64: the last kNN call's point distances
     };
     if (ctx->gid_in_vals && !std::strcmp(name, "isect_gid")) {  // a batched render's ids: the sorted values
         if (!ctx->vals[ctx->sorted].ptr) return fail(MSPLAT_CUDA_EINVAL, "frame buffer 'isect_gid' has not been produced");

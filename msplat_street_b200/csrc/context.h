@@ -193,7 +193,7 @@ struct msplat_cuda_ctx {
     // per tile / pixel
     Buf tile_start, tile_end, out_img, final_T, final_idx, v_rendered, loss_part, loss;
     // densification and primitive scratch
-    Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md;
+    Buf d_flags, d_counts, d_scratch, k_bounds, k_sorted, k_box, k_md, k_evals;
     // stored-transmittance mode (option "store_transmittance" = per-pixel capacity)
     int tstore_cap = 0;
     Buf tstore, tcount;
@@ -234,7 +234,7 @@ struct msplat_cuda_ctx {
                       &v_opacity, &v_mean3d, &v_scale, &v_quat, &keys[0], &keys[1], &vals[0], &vals[1], &emit_gid,
                       &isect_gid, &inv, &slots, &radix_scratch, &tile_start, &tile_end, &out_img, &final_T,
                       &final_idx, &v_rendered, &loss_part, &loss, &d_flags, &d_counts, &d_scratch, &k_bounds,
-                      &k_sorted, &k_box, &k_md, &tstore, &tcount, &pairs, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
+                      &k_sorted, &k_box, &k_md, &k_evals, &tstore, &tcount, &pairs, &bdesc, &bcounter, &dkeys[0], &dkeys[1],
                       &dvals[0], &dvals[1], &dcounts, &doff, &img[0], &img[1], &img[2], &img[3], &img[4], &img[5]};
         for (Buf *b : all) {
             if (b->ptr) cudaFree(b->ptr);

@@ -350,6 +350,7 @@ struct KnnScratch {
     uint32_t *vals[2];
     void *radix_scratch;
     float4 *sorted, *bmin, *bmax;
+    unsigned long long *evals;  // (may be null) point distances the search computed
 };
 int knn_boxes(int n);
 int launch_knn3(const float *pts, int n, float *out, KnnScratch &s, cudaStream_t st);

@@ -123,8 +123,10 @@ __device__ __forceinline__ float gap(float qlo, float qhi, float blo, float bhi)
     return fmaxf(fmaxf(blo - qhi, qlo - bhi), 0.f);
 }
 
+// evals (may be null): adds the point distances the warp computes (32 per query per
+// surviving box) -- the search's work, for throughput reports.
 __global__ void knn_query_kernel(const float4 *sp, int n, int nboxes, const float4 *bmin, const float4 *bmax,
-                                 float *out) {
+                                 float *out, unsigned long long *evals) {
     const int lane = threadIdx.x & 31;
     const int own = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (own >= nboxes) return;  // warp-uniform
@@ -144,6 +146,7 @@ __global__ void knn_query_kernel(const float4 *sp, int n, int nboxes, const floa
             qh[a] = fmaxf(qh[a], __shfl_xor_sync(0xffffffffu, qh[a], o));
         }
     float b0 = INFINITY, b1 = INFINITY, b2 = INFINITY;
+    const unsigned nq = __popc(__ballot_sync(0xffffffffu, fin));  // queries with a finite point
     // candidate t visits own, own+1, own-1, own+2, own-2, ...
     const int span = 2 * nboxes;
     for (int t0 = 0; t0 < span; t0 += 32) {
@@ -160,6 +163,7 @@ __global__ void knn_query_kernel(const float4 *sp, int n, int nboxes, const floa
             pass = gx * gx + gy * gy + gz * gz < thr && lo.x <= hi.x;
         }
         unsigned m = __ballot_sync(0xffffffffu, pass);
+        if (evals && lane == 0 && m) atomicAdd(evals, (unsigned long long)__popc(m) * nq * KNN_BOX);
         while (m) {
             const int src = __ffs(m) - 1;
             m &= m - 1;
@@ -190,13 +194,14 @@ int launch_knn3(const float *pts, int n, float *out, KnnScratch &s, cudaStream_t
     if (n <= 0) return 0;
     const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     cudaMemcpyAsync(s.bounds, init, sizeof init, cudaMemcpyHostToDevice, st);
+    if (s.evals) cudaMemsetAsync(s.evals, 0, sizeof(unsigned long long), st);
     knn_bounds_kernel<<<std::min((n + 255) / 256, 1184), 256, 0, st>>>(pts, n, s.bounds);
     knn_morton_kernel<<<(n + 255) / 256, 256, 0, st>>>(pts, n, s.bounds, s.keys[0], s.vals[0]);
     const int cur = radix_sort_pairs(s.keys, s.vals, n, 30, s.radix_scratch, st);
     knn_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pts, n, s.vals[cur], s.sorted);
     const int nb = knn_boxes(n);
     knn_boxes_kernel<<<(nb + 127) / 128, 128, 0, st>>>(s.sorted, n, nb, s.bmin, s.bmax);
-    knn_query_kernel<<<(nb * 32 + 127) / 128, 128, 0, st>>>(s.sorted, n, nb, s.bmin, s.bmax, out);
+    knn_query_kernel<<<(nb * 32 + 127) / 128, 128, 0, st>>>(s.sorted, n, nb, s.bmin, s.bmax, out, s.evals);
     return 0;
 }
 

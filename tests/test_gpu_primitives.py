@@ -69,6 +69,16 @@ def test_gpu_knn_sizes(n):
     np.testing.assert_array_equal(_core._gpu_knn3_mean_dist(pts), Oracle("restatement").knn3_mean_dist(pts))
 
 
+def test_gpu_knn_counts_its_distance_evaluations():
+    """33 points make two boxes of the Morton order, and with no neighbours found yet
+    every box passes its bounds test: box 0's 32 queries and box 1's single query each
+    compute 32 distances per box, 2 x (32 + 1) x 32 in all."""
+    pts = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, (33, 3)).astype(np.float32)).cuda()
+    ctx = Context()
+    ctx.knn3_mean_dist(pts)
+    assert int(ctx.frame("knn_evals").view(torch.int64)[0]) == 2 * 33 * 32
+
+
 def _f32_ulps(a, b):
     ia = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
     ib = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
