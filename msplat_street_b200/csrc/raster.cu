@@ -1,7 +1,9 @@
 // 16x16-tile front-to-back alpha compositing, forward and backward.
 //
-// One CTA per tile. The tile's depth-sorted list is walked in batches whose splat
-// records are staged in shared memory; every thread reads each record as a broadcast.
+// One CTA per tile (the forward may also split a tile into 16 x 8 or 8 x 8 pixel
+// blocks, each walking the tile's whole list: the block shape changes no result). The
+// tile's depth-sorted list is walked in batches whose splat records are staged in
+// shared memory; every thread reads each record as a broadcast.
 // Staging also clamps the colours once and marks which of the tile's warp blocks the
 // splat can reach at all (its box and its ellipse's diagonal extents, tested on 8 x 4
 // pixel blocks), so a warp passes over the splats that miss its pixels with one bit
