@@ -231,3 +231,42 @@ def test_batch_entry_points_refuse_a_prior():
         ctx.render_batch([BatchItem(p, cam, BACKGROUND)])
     ctx.set_prior(None)
     assert len(ctx.render_batch([BatchItem(p, cam, BACKGROUND)])) == 1
+
+
+@pytest.mark.parametrize("shape", [1, 2], ids=["16x8", "8x8"])
+def test_block_shapes_with_prior_and_stored_transmittance(shape):
+    """The forward's block shapes (raster_shape) in the aux rasterizer (a prior with the
+    sky, the depth prior and the exposure) and with stored transmittance: the same
+    render, aux outputs, loss and updated parameters, bit for bit, as whole-tile blocks."""
+    g, cam = _scene(), _camera()
+    results = []
+    for s in (0, shape):
+        out = []
+        # aux render and training step with the full prior
+        ctx = Context()
+        ctx.set_raster_shape(s)
+        pr = to_gpu(make_prior(cam.width, cam.height, 8, ALL))
+        ctx.set_prior(pr)
+        p = GaussianParams.from_numpy(g)
+        out.append(ctx.render(p, cam, BACKGROUND).clone())
+        out.extend(t.clone() for t in ctx.render_aux_outputs())
+        tgt = out[0].clone()
+        adam = AdamState.zeros_like(p, C1_LRS)
+        st = tuple(torch.zeros(p.n, device="cuda") for _ in range(3))
+        out.append(torch.tensor([ctx.train_step(p, adam, cam, BACKGROUND, tgt.flip(0).contiguous(), st,
+                                                sync_loss=True)]))
+        out.extend(t.clone() for t in p.tensors())
+        ctx.set_prior(None)
+        # plain step with stored transmittance
+        ctx2 = Context(store_transmittance=16)
+        ctx2.set_raster_shape(s)
+        q = GaussianParams.from_numpy(g)
+        adam2 = AdamState.zeros_like(q, C1_LRS)
+        st2 = tuple(torch.zeros(q.n, device="cuda") for _ in range(3))
+        out.append(torch.tensor([ctx2.train_step(q, adam2, cam, BACKGROUND, tgt.flip(0).contiguous(), st2,
+                                                 sync_loss=True)]))
+        out.extend(t.clone() for t in q.tensors())
+        out.append(ctx2.frame("final_idx").clone())
+        results.append([t.cpu() for t in out])
+    for a, b in zip(*results):
+        assert torch.equal(a, b)
